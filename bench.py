@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""LS-MPS per-step path on B200: particle-steps/s and PPE solve time at 1M particles.
+
+Workload (one "step" = the whole per-step path on one particle set):
+  1,000,000 particles, case `mixed` (80 % jittered bulk lattice +-0.1 l0, 20 % rain on a
+  20-degree plate: 3 wall layers, 4-layer film, radius-3 droplets 10-40 l0 above it),
+  l0 = 1, re = 2.1 l0, max_neighbors 128; neighbor build + 14-direction classification,
+  batched WLS over every particle, WLS-Laplacian PPE over all Interior / NearWall
+  particles with p* = sin(0.3x) cos(0.2y) + 0.1z and b = A p*, solved to relative residual
+  1e-10 (PPE relative L2 against p* <= 1e-8 is checked).
+  Synthetic data, seeded; matrices are larger than L2 (126 MB) so no flush is needed.
+
+`value` = particles x GPUs / (device step time, CUDA events on the library's stream, max
+over ranks) with the headline solver (mixed precision: FP32 Jacobi-BiCGStab inner solves,
+FP64 residual refinement). `e2e` = the same through the C ABI with host buffers: upload
+from pinned memory, the step, and the download of the pressure inside the timed region.
+The plain FP64 GPU BiCGStab (the reference iteration) is timed on the same system beside
+it. `--impl reference` times the reference's own CPU implementation of the path.
+
+Multi-GPU: replicas only (one independent particle set per rank), `scaling: weak`.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ls-mps_b200"))
+
+METRIC = "PPE solve ms & particle-steps/s at 1M, learned+mixed vs plain FP64 @ L2<=1e-8"
+UNIT = "particle-steps/s"
+L0, RE_RATIO, MAXN = 1.0, 2.1, 128
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--particles", type=int, default=1_000_000)
+    ap.add_argument("--case", default="mixed")
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "learned", "jacobi", "fp64"])
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--max-iter", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 comparison solves")
+    ap.add_argument("--cpu-sample-s", type=float, default=8.0, help="CPU BiCGStab sample budget (s)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self, want_gpu: bool):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            backend = "nccl" if (want_gpu and torch.cuda.is_available()) else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+            self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def reduce(self, value: float, op: str) -> float:
+        if not self.pg:
+            return value
+        import torch
+
+        dev = f"cuda:{self.local_rank}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([value], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX if op == "max" else self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 10:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        load = [r for r in rows if (num(r[4]) or 0) >= 50] or rows
+        sm = [num(r[1]) for r in load if num(r[1]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in load:
+            for k, name in enumerate(names):
+                if r[6 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(load),
+                "power_w_max": max((num(r[3]) or 0) for r in rows)}
+
+
+# ---------------------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------------------
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the SpMV kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def step(ctx, solver, tol, max_iter, timings):
+    """One pass of the per-step path on the resident particle set."""
+    import lsmps_b200 as lib
+
+    re = RE_RATIO * L0
+    nst = ctx.build_neighbors(re, MAXN, L0)
+    ctx.wls(re, L0, mode=1)
+    pst = ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
+    s = ctx.ppe_solve(solver, max_iter, tol)
+    t = ctx.timings()
+    timings.append({"neighbor_ms": t[1], "wls_ms": t[3], "assembly_ms": t[4], "solve_ms": s.solve_ms,
+                    "iterations": s.iterations, "outer": s.outer_iterations})
+    return nst, pst, s, lib
+
+
+def run_mine(args, dist):
+    import torch
+
+    import lsmps_b200 as lib
+
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    xyz, types, _ = lib.generate(None, case=args.case, particles=args.particles, l0=L0,
+                                 seed=args.seed + dist.rank)
+    n = len(types)
+    ctx = lib.Context(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    ctx.upload(xyz, types)
+    timings = []
+    for _ in range(args.warmup):
+        nst, pst, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings)
+    timings.clear()
+
+    # ---- device-timed steps (inputs resident) ----
+    clocks = ClockSampler(dev)
+    launches0 = lib.load().lsmps_launch_count()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        nst, pst, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    launches = lib.load().lsmps_launch_count() - launches0
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    ms_step_max = dist.reduce(ms_step, "max")
+    launches_total = int(dist.reduce(float(launches), "sum"))
+    rel_l2 = s.relative_l2_error
+
+    # ---- end to end through the C ABI with host buffers ----
+    pin_xyz = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pin_typ = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
+    pin_xyz[:] = xyz
+    pin_typ[:] = types
+    U = int(pst.unknowns)
+    pin_p = torch.empty(U, dtype=torch.float64, pin_memory=True).numpy()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.upload(pin_xyz, pin_typ)
+        step(ctx, args.solver, args.tol, args.max_iter, [])
+        ctx.pressure_into(pin_p)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    e2e_ms_max = dist.reduce(e2e_ms, "max")
+
+    result = {
+        "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step_max,
+        "value": n * dist.world / (ms_step_max * 1e-3),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (mixed)" if args.solver == "mixed" else args.solver,
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}",
+                   "particles": n, "case": args.case, "l0": L0, "re": RE_RATIO * L0, "max_neighbors": MAXN,
+                   "solver": args.solver, "ppe_unknowns": U, "ppe_nnz": int(pst.nnz), "pairs": int(nst.pairs),
+                   "parallelism": f"replicas x{dist.world}", "l2_flush": "inputs larger than L2 (matrix > 126 MB)"},
+        "e2e": {"value": n * dist.world / (e2e_ms_max * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": int(pin_xyz.nbytes + pin_typ.nbytes), "d2h_bytes_per_step": int(pin_p.nbytes),
+                "ms_per_step": e2e_ms_max},
+        "gpu_launches": launches_total,
+        "clocks": clk,
+        "phases_ms": {k: statistics.median(t[k] for t in timings) for k in timings[0]},
+        "ppe": {"relative_l2_error": rel_l2, "relative_residual": s.relative_residual,
+                "iterations": s.iterations, "outer_iterations": s.outer_iterations, "converged": bool(s.converged),
+                "solve_ms": statistics.median(t["solve_ms"] for t in timings)},
+    }
+
+    # ---- the plain FP64 GPU BiCGStab (and the stages between) on the same system ----
+    if not args.no_compare:
+        cmp = {}
+        for name in ("fp64", "jacobi", "mixed"):
+            r = ctx.ppe_solve(name, args.max_iter, args.tol)
+            cmp[name] = {"solve_ms": r.solve_ms, "iterations": r.iterations, "converged": bool(r.converged),
+                         "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual}
+        result["ppe_compare"] = cmp
+        result["speedup_vs_plain_fp64"] = cmp["fp64"]["solve_ms"] / result["ppe"]["solve_ms"]
+
+    # ---- roofline of the dominant kernel (the solver's SpMV) and the other kernels ----
+    peak, peak_kind = measured_hbm_peak()
+    kern = {}
+    for name, kid in (("spmv32", lib.KB_SPMV32), ("spmv64", lib.KB_SPMV64), ("nbr_count", lib.KB_NBR_COUNT),
+                      ("nbr_fill", lib.KB_NBR_FILL), ("wls", lib.KB_WLS)):
+        ms, nbytes = ctx.kernel_bench(kid, 20)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        kern[name] = {"ms": ms, "alg_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    dom = "spmv32" if args.solver in ("mixed", "learned") else "spmv64"
+    traffic = committed_traffic().get(dom)
+    result["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"], "peak": peak,
+                          "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,
+                          "traffic": traffic, "kernels": kern}
+
+    # ---- CPU baseline: the reference's own code on a bounded sample (rank 0, N = 1) ----
+    if dist.world == 1 and dist.rank == 0 and not args.no_cpu_baseline:
+        try:
+            result["cpu_baseline"] = cpu_baseline(ctx, xyz, types, cmp["fp64"]["iterations"] if not args.no_compare
+                                                  else s.iterations, args.cpu_sample_s)
+        except Exception as e:  # the reference build may be absent on a machine without its sources
+            result["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    ctx.close()
+    return result
+
+
+def _ref_case(xyz, types):
+    """A reference handle on this particle set with the bench's parameters."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Ref
+
+    fd, path = tempfile.mkstemp(suffix=".cfg")
+    with os.fdopen(fd, "w") as f:
+        f.write(f"case=bench\nparticles={len(types)}\nl0={L0}\nre_ratio={RE_RATIO}\nmax_neighbors={MAXN}\n"
+                f"wls_samples=4096\nppe_max_unknowns={len(types)}\nppe_max_iter=0\nppe_tol=1e-10\n")
+    r = Ref(path)
+    os.unlink(path)
+    r.set_particles(xyz, types)
+    return r
+
+
+def cpu_baseline(ctx, xyz, types, plain_iterations, sample_s):
+    """The reference (oracle/_ref, single-threaded as the reference is) on a bounded sample
+    of the same step: its neighbors + classify in full, wls_test on 4096 particles
+    extrapolated to all, its assemble_ppe in full, and its BiCGStab iteration on this step's
+    WLS matrix for a bounded number of iterations, extrapolated to the iteration count the
+    identical FP64 iteration needed on the GPU."""
+    from oracle import Ref
+
+    r = _ref_case(xyz, types)
+    n = len(types)
+    t0 = time.perf_counter()
+    r.neighbors()
+    t1 = time.perf_counter()
+    r.classify()
+    t2 = time.perf_counter()
+    w = r.wls_test()
+    t3 = time.perf_counter()
+    _, _, _, _, _, st = r.assemble_ppe()
+    t4 = time.perf_counter()
+    row, col, val, b, xe, _ = ctx.ppe_reference_numbering()
+    # bounded sample of the reference's BiCGStab iteration on this matrix
+    probe_x, probe = Ref.bicgstab_csr(row, col, val, b, xe, 3, 0.0)
+    per_iter = probe["solve_ms"] / 3.0
+    k = int(max(5, min(500, sample_s * 1e3 / max(per_iter, 1e-3))))
+    _, info = Ref.bicgstab_csr(row, col, val, b, xe, k, 0.0)
+    ms_iter = info["solve_ms"] / max(1, info["iterations"])
+    wls_all_ms = (t3 - t2) * 1e3 * n / max(1.0, w["sampled"] + w["failed"])
+    step_ms = (t1 - t0) * 1e3 + (t2 - t1) * 1e3 + wls_all_ms + (t4 - t3) * 1e3 + ms_iter * plain_iterations
+    return {
+        "value": n / (step_ms * 1e-3), "unit": UNIT, "cores": 1, "kind": "reference",
+        "sample": (f"reference neighbors+classify+assemble_ppe on all {n} particles, wls_test on "
+                   f"{int(w['sampled'])} sampled particles extrapolated to all, and {info['iterations']} "
+                   f"reference BiCGStab iterations on this WLS-Laplacian matrix extrapolated to the "
+                   f"{plain_iterations} the same FP64 iteration needed"),
+        "ms_per_step": step_ms, "bicgstab_ms_per_iteration": ms_iter,
+        "phases_ms": {"neighbors": (t1 - t0) * 1e3, "classify": (t2 - t1) * 1e3, "wls_all_est": wls_all_ms,
+                      "assemble": (t4 - t3) * 1e3, "solve_est": ms_iter * plain_iterations},
+        "host_nproc": os.cpu_count(),
+    }
+
+
+# ---------------------------------------------------------------------------------------
+# the reference arm: the reference's CPU implementation of the path
+# ---------------------------------------------------------------------------------------
+def run_reference(args, dist):
+    """Times the reference's own CPU implementation (oracle/_ref) of this step. Where the
+    reference lacks a piece (all-particle WLS, the WLS-Laplacian rows) the oracle's CPU
+    restatement stands in; BiCGStab runs the reference's iteration for a bounded sample and
+    is extrapolated to the iteration count that the same FP64 iteration (run once, in the
+    warm-up, multi-threaded) needs to reach the tolerance."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lsmps_b200 as lib
+    from oracle import Oracle, Ref
+
+    xyz, types, _ = lib.generate(None, case=args.case, particles=args.particles, l0=L0, seed=args.seed)
+    n = len(types)
+    nt = os.cpu_count() or 1
+    re = RE_RATIO * L0
+    # warm-up: the oracle's WLS-Laplacian system and the iteration count to the tolerance
+    r = _ref_case(xyz, types)
+    row, col, _ = r.neighbors()
+    cls = r.classify()
+    _, wst, z, ws = Oracle.wls(xyz, cls, row, col, re, L0)
+    prow, pcol, pval, pb, pxe, _, _ = Oracle.ppe_assemble(2, xyz, cls, row, col, re, L0, n, 0.0, z, ws, wst)
+    _, info = Oracle.bicgstab(prow, pcol, pval, pb, args.max_iter, args.tol, nthreads=nt)
+    iters = info["iterations"]
+    samples = []
+    for k in range(args.warmup + args.steps):
+        r = _ref_case(xyz, types)
+        t0 = time.perf_counter()
+        r.neighbors()
+        r.classify()
+        t1 = time.perf_counter()
+        w = r.wls_test()
+        t2 = time.perf_counter()
+        r.assemble_ppe()
+        t3 = time.perf_counter()
+        _, si = Ref.bicgstab_csr(prow, pcol, pval, pb, pxe, 20, 0.0)
+        # wls_test runs on a strided sample: its time is scaled to every particle
+        wls_ms = (t2 - t1) * 1e3 * n / max(1.0, w["sampled"] + w["failed"])
+        step_ms = (t1 - t0) * 1e3 + wls_ms + (t3 - t2) * 1e3 + si["solve_ms"] / max(1, si["iterations"]) * iters
+        if k >= args.warmup:
+            samples.append(step_ms)
+    ms = statistics.median(samples)
+    value = n / (ms * 1e-3)
+    return {
+        "impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "value": value, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}", "particles": n,
+                   "solver": "reference FP64 BiCGStab (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"per step: reference neighbors+classify+assemble_ppe on all {n} particles, "
+                                   f"wls_test on its 4096-particle sample scaled to all, and 20 reference BiCGStab "
+                                   f"iterations on the WLS-Laplacian matrix extrapolated to the {iters} iterations "
+                                   f"the same FP64 iteration needs ({nt} threads, once, in the warm-up)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        # the reference arm is CPU only: rank 0 measures, the other ranks exit at once
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        os.environ["WORLD_SIZE"] = "1"
+    dist = Dist(want_gpu=args.impl == "mine")
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, dist)
+        else:
+            out = run_mine(args, dist)
+        if dist.rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

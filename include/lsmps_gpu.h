@@ -1,0 +1,227 @@
+/* LS-MPS per-step path on an sm_100a GPU — C ABI.
+ *
+ * Plain C types only (pointers, sizes, PODs); no C++ exceptions cross it. One context
+ * owns the device buffers and one CUDA stream; calls on one context are not
+ * thread-safe, separate contexts are independent. Every function returns an
+ * lsmps_status; lsmps_last_error() gives the message of the last failure.
+ *
+ * Each entry point replaces one internal function of the reference benchmark
+ * (lilux618/LS-MPS src/lsmps.cpp, which has no FFI of its own: these are the
+ * functions its run_benchmark, src/lsmps.cpp:73, calls). The reference citation is
+ * given beside each. Particle indices in and out are the caller's (original) order;
+ * internally the library works in cell-sorted order.
+ */
+#ifndef LSMPS_GPU_H
+#define LSMPS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSMPS_ABI_VERSION 1
+
+typedef struct lsmps_ctx lsmps_ctx;
+
+typedef enum lsmps_status {
+    LSMPS_OK = 0,
+    LSMPS_ERR_ARG = 1,        /* invalid argument or size */
+    LSMPS_ERR_CUDA = 2,       /* CUDA runtime error (message in lsmps_last_error) */
+    LSMPS_ERR_ALLOC = 3,      /* device or pinned allocation failed */
+    LSMPS_ERR_STATE = 4,      /* call order: a prerequisite step has not run */
+    LSMPS_ERR_GRID = 5,       /* cell grid or cell occupancy beyond the supported limits */
+    LSMPS_ERR_OVERFLOW = 6,   /* a 32-bit index would overflow */
+    LSMPS_ERR_NONFINITE = 7,  /* non-finite particle position or solver value */
+    LSMPS_ERR_TIMEOUT = 8,    /* a bounded device-side wait expired */
+    LSMPS_ERR_IO = 9          /* file read/write (weights) */
+} lsmps_status;
+
+/* Particle classes, numbered as the reference's ParticleType (include/lsmps.hpp:8). */
+enum { LSMPS_INTERIOR = 0, LSMPS_FREE_SURFACE = 1, LSMPS_SPLASH = 2, LSMPS_NEAR_WALL = 3, LSMPS_WALL = 4 };
+
+/* ---- context ---------------------------------------------------------------------- */
+int lsmps_ctx_create(int device, lsmps_ctx** out);
+void lsmps_ctx_destroy(lsmps_ctx* ctx);
+const char* lsmps_last_error(const lsmps_ctx* ctx);
+int lsmps_abi_version(void);
+/* Device time (ms, CUDA events on the context stream) of the phases of the last calls:
+ * [0] upload, [1] neighbor build (+classification when fused), [2] classification,
+ * [3] WLS, [4] PPE assembly, [5] PPE solve, [6] last download. */
+int lsmps_get_timings(lsmps_ctx* ctx, double out[8]);
+/* Block until all work queued on the context stream has finished. */
+int lsmps_sync(lsmps_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+void* lsmps_stream(lsmps_ctx* ctx);
+/* Kernel launches this library has issued in this process (graph replays count every
+ * kernel node they run). */
+uint64_t lsmps_launch_count(void);
+
+/* Profiling hook: launches one kernel of the path `reps` times on the context stream on
+ * the current data and returns its mean duration (CUDA events around the launches) and
+ * its algorithmic bytes per launch (the traffic a perfect kernel would move):
+ *   LSMPS_KB_SPMV64  FP64 CSR SpMV + fused dot   12 nnz + 20 U
+ *   LSMPS_KB_SPMV32  FP32 CSR SpMV + fused dot    8 nnz + 16 U
+ *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL neighbor passes   24 N + 4 N (+ 4 P + 1 N fill)
+ *   LSMPS_KB_WLS     all-particle WLS            24 N + 4 P + 80 N (z, sum w, status)
+ * No reference counterpart (the reference has no GPU path). */
+enum { LSMPS_KB_SPMV64 = 0, LSMPS_KB_SPMV32 = 1, LSMPS_KB_NBR_COUNT = 2, LSMPS_KB_NBR_FILL = 3, LSMPS_KB_WLS = 4 };
+int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
+
+/* ---- particles -------------------------------------------------------------------- */
+/* xyz: n x 3 doubles (x, y, z interleaved, as the reference's Particle::r); type: n
+ * class bytes (only Wall is read by classification, src/lsmps.cpp:27). Host memory. */
+int lsmps_upload_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n);
+/* Same from device pointers already on the context's device (no host copy). */
+int lsmps_upload_particles_device(lsmps_ctx* ctx, const double* d_xyz, const uint8_t* d_type, size_t n);
+
+/* ---- neighbor build + classification ---------------------------------------------- */
+typedef struct lsmps_neighbor_stats {
+    uint64_t pairs;          /* kept directed pairs (reference NeighborData::pairs) */
+    uint64_t truncated;      /* dropped pairs beyond max_neighbors (NeighborData::truncated) */
+    double mean;             /* mean kept count over all particles (Metrics::neighbor_mean) */
+    int32_t p50, p90, p99;   /* percentiles cnt[(size_t)(q (N-1))] of the sorted counts */
+    int32_t max_count;
+    uint64_t type_count[5];  /* particles per class after classification */
+    int64_t grid_cells;      /* cells in the dense grid */
+    int32_t max_cell_occupancy;
+    int32_t reserved;
+} lsmps_neighbor_stats;
+
+#define LSMPS_NBR_CLASSIFY 1  /* fuse the 14-direction classification into the fill pass */
+
+/* Uniform-grid neighbor lists, bit-exact with the reference's neighbors()
+ * (src/lsmps.cpp:16-18,26): cell = floor(r / re) per axis, 27 cells dz, dy, dx from -1
+ * to 1, ascending index within a cell, |rj - ri|^2 < re^2 without FMA contraction, first
+ * max_neighbors kept. With LSMPS_NBR_CLASSIFY also classify() (src/lsmps.cpp:27) with l0.
+ * re must be the caller's re_ratio * l0 product, as run_benchmark (src/lsmps.cpp:73). */
+int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l0, int flags,
+                          lsmps_neighbor_stats* out);
+/* classify() (src/lsmps.cpp:27) over the current neighbor lists, standalone. */
+int lsmps_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
+
+/* ---- WLS -------------------------------------------------------------------------- */
+typedef struct lsmps_wls_opts {
+    double re, l0;
+    double regularization;   /* reference Config::wls_regularization (1e-8) */
+    int32_t mode;            /* 0: reference wls_test sample (src/lsmps.cpp:28), bit-exact;
+                                1: every particle, nrhs quadratic fields */
+    int32_t wls_samples;     /* mode 0: reference Config::wls_samples */
+    int32_t nrhs;            /* mode 1: 1..3 fields */
+    int32_t precision;       /* mode 1: 0 FP64; 1 FP32 Cholesky + FP64 refinement */
+    const double* quad_coef; /* mode 1: nrhs x 10 coefficients of
+                                c0 + c1 x + c2 y + c3 z + c4 x^2 + c5 y^2 + c6 z^2 + c7 xy + c8 xz + c9 yz */
+    int32_t store_solutions; /* mode 1: keep the n x nrhs x 9 solutions for download */
+    int32_t reserved;
+} lsmps_wls_opts;
+
+typedef struct lsmps_wls_stats {
+    /* reference WlsStats (include/lsmps.hpp:20); mode 1 fills them over all particles
+     * and all fields (errors against each field's analytic gradient / Laplacian) */
+    uint64_t sampled, ok, regularized, failed, virtual_points;
+    double max_gradient_error, rms_gradient_error, max_laplacian_error, rms_laplacian_error;
+    uint64_t skipped;        /* Wall / Splash particles */
+    uint64_t fp64_fallback;  /* precision 1: systems refactored in FP64 */
+} lsmps_wls_stats;
+
+/* wls_test (mode 0) or the all-particle batched WLS (mode 1). Mode 1 also keeps each
+ * particle's Laplacian vector z = M^-1 (e3+e4+e5) and sum of weights for the WLS PPE. */
+int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
+
+/* ---- PPE assembly ----------------------------------------------------------------- */
+enum { LSMPS_PPE_REFERENCE = 0, LSMPS_PPE_SHIFTED = 1, LSMPS_PPE_WLS = 2 };
+
+typedef struct lsmps_ppe_opts {
+    int32_t variant;         /* LSMPS_PPE_* */
+    int32_t reserved;
+    int64_t max_unknowns;    /* reference Config::ppe_max_unknowns */
+    double re, l0;
+    double diag_shift;       /* SHIFTED / WLS: diagonal times (1 + diag_shift) */
+} lsmps_ppe_opts;
+
+typedef struct lsmps_ppe_stats {
+    /* reference PpeStats (include/lsmps.hpp:21) */
+    uint64_t unknowns, nnz, dirichlet, neumann, failed_rows;
+    int32_t iterations, converged;
+    double initial_residual, final_residual, relative_l2_error, max_error, assembly_ms, solve_ms;
+    /* extensions */
+    int32_t outer_iterations;   /* FP64 refinement sweeps (mixed / learned) */
+    int32_t fallback;           /* learned: 1 when the stall rule switched to Jacobi */
+    double relative_residual;   /* |b - Ax| / |b| at exit (FP64) */
+} lsmps_ppe_stats;
+
+/* assemble_ppe (src/lsmps.cpp:30-64) and its variants; keeps A, b = A p*, p* on the device. */
+int lsmps_ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);
+
+/* ---- PPE solve -------------------------------------------------------------------- */
+enum {
+    LSMPS_SOLVER_REFERENCE = 0, /* bit-identical to the reference's FP64 BiCGStab (src/lsmps.cpp:67):
+                                   sequential-order dot products; for small systems */
+    LSMPS_SOLVER_FP64 = 1,      /* the reference iteration in FP64, GPU reductions */
+    LSMPS_SOLVER_JACOBI = 2,    /* FP64, Jacobi right preconditioning */
+    LSMPS_SOLVER_MIXED = 3,     /* FP32 Jacobi BiCGStab inner solves + FP64 residual refinement */
+    LSMPS_SOLVER_LEARNED = 4    /* MIXED with the message-passing network as warm start of each
+                                   refinement sweep; Jacobi fallback when the residual stalls */
+};
+
+typedef struct lsmps_solver_opts {
+    int32_t solver;          /* LSMPS_SOLVER_* */
+    int32_t max_iter;        /* total BiCGStab iterations (inner ones for MIXED / LEARNED) */
+    double tol;              /* converged when |r| <= tol * max(1, |b|) (src/lsmps.cpp:67) */
+    int32_t warm_start;      /* start from the last solution held by the context */
+    int32_t use_graph;       /* capture the iteration in a CUDA graph (FP64 / JACOBI / MIXED) */
+    double inner_tol;        /* MIXED: relative reduction per FP32 inner solve (default 1e-4) */
+    int32_t inner_max_iter;  /* MIXED: inner iteration cap per sweep (default 200) */
+    int32_t stall_window;    /* LEARNED: iterations without progress before fallback (20) */
+    int32_t check_every;     /* iterations between host convergence checks (default 8) */
+    int32_t reserved;
+} lsmps_solver_opts;
+
+int lsmps_ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out);
+
+/* ---- downloads (host buffers, caller's particle / unknown order) ------------------- */
+int lsmps_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);
+/* row_ptr: n + 1; col: pairs entries (original particle indices, reference order). */
+int lsmps_download_neighbors(lsmps_ctx* ctx, int32_t* row_ptr, int32_t* col, size_t col_cap);
+/* mode-1 WLS: x (n x nrhs x 9, if stored), status (n: 0 ok, 1 regularised, 2 skipped,
+ * 3 sum w <= 0, 4 Cholesky failed), z (n x 9), wsum (n). Any pointer may be NULL. */
+int lsmps_download_wls(lsmps_ctx* ctx, double* x, int32_t* status, double* z, double* wsum);
+/* PPE in the reference's numbering (unknown rank in particle order): row (U+1), col, val
+ * (nnz), b, p* (U), unknown_particle (U). Any pointer may be NULL. */
+int lsmps_download_ppe(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, double* b,
+                       double* x_exact, int32_t* unknown_particle);
+/* Solution of the last solve (U, reference numbering). */
+int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+
+/* ---- learned preconditioner (message-passing network over the neighbor graph) ----- */
+typedef struct lsmps_mpnn_train_opts {
+    int32_t steps;           /* optimiser steps on the samples added so far */
+    int32_t batch;           /* samples per step */
+    float lr;                /* Adam learning rate */
+    float weight_decay;
+    uint32_t seed;
+    int32_t reserved;
+} lsmps_mpnn_train_opts;
+
+/* Initialise the network (3 layers, hidden 64, BF16 weights) from a seed. */
+int lsmps_mpnn_init(lsmps_ctx* ctx, uint32_t seed);
+/* Add the current assembled system's (residual -> correction) training pair, using the
+ * current solution as the target. */
+int lsmps_mpnn_add_sample(lsmps_ctx* ctx);
+/* Train on the stored samples; loss_out gets the final mean loss. */
+int lsmps_mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss_out);
+int lsmps_mpnn_save(lsmps_ctx* ctx, const char* path);
+int lsmps_mpnn_load(lsmps_ctx* ctx, const char* path);
+
+/* ---- host helpers (no GPU) --------------------------------------------------------- */
+/* Parse a .cfg file and generate its particle set with the library's generate_case
+ * (bit-identical to the reference's for the reference's cases). Two calls: first with
+ * xyz == NULL for *n, then with buffers of n. Extra key=value overrides ("k=v;k=v"). */
+int lsmps_host_generate(const char* cfg_path, const char* overrides, double* xyz, uint8_t* type,
+                        double* uvw, size_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSMPS_GPU_H */

@@ -1,0 +1,307 @@
+// The C ABI of lsmps_gpu.h: argument checks, exception-to-status translation, context
+// lifetime, uploads and phase timing. The phases live in neighbors.cu, wls.cu, ppe.cu,
+// solver.cu and mpnn.cu.
+#include <atomic>
+#include <cstring>
+#include <new>
+
+#include "ops.cuh"
+
+namespace lsmps_gpu {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void* pinned_ensure(lsmps_ctx* ctx, size_t bytes) {
+    if (bytes > ctx->pinned_bytes) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        if (cudaMallocHost(&ctx->pinned, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{LSMPS_ERR_ALLOC, "pinned host allocation failed"};
+        }
+        ctx->pinned_bytes = bytes;
+    }
+    return ctx->pinned;
+}
+
+void check_device_flags(lsmps_ctx* ctx, const char* where) {
+    int f = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&f, ctx->dflags.get<int>(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (!f) return;
+    LSMPS_CUDA(cudaMemsetAsync(ctx->dflags.get<int>(), 0, sizeof(int), ctx->stream));
+    std::string w(where);
+    if (f & DFLAG_NONFINITE) throw Error{LSMPS_ERR_NONFINITE, w + ": non-finite particle position"};
+    if (f & DFLAG_CELL_OVERFLOW) throw Error{LSMPS_ERR_GRID, w + ": a cell holds more than 8192 particles"};
+    if (f & DFLAG_INDEX) throw Error{LSMPS_ERR_OVERFLOW, w + ": a count exceeds the int32 range"};
+    if (f & DFLAG_TIMEOUT) throw Error{LSMPS_ERR_TIMEOUT, w + ": a bounded device wait expired"};
+    throw Error{LSMPS_ERR_CUDA, w + ": device error flag " + std::to_string(f)};
+}
+
+void ev_record(lsmps_ctx* ctx, int slot) { LSMPS_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream)); }
+
+double ev_elapsed(lsmps_ctx* ctx, int a, int b) {
+    LSMPS_CUDA(cudaEventSynchronize(ctx->ev[b]));
+    float ms = 0;
+    LSMPS_CUDA(cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]));
+    return ms;
+}
+
+namespace {
+__global__ void k_pack_particles(const double* __restrict__ xyz, size_t n, double* __restrict__ pos) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < 3 * n) pos[i] = xyz[i];
+}
+}  // namespace
+
+}  // namespace lsmps_gpu
+
+using namespace lsmps_gpu;
+
+namespace {
+template <class F>
+int guarded(lsmps_ctx* ctx, F&& f) {
+    if (!ctx) return LSMPS_ERR_ARG;
+    try {
+        LSMPS_CUDA(cudaSetDevice(ctx->device));
+        f();
+        ctx->last_error.clear();
+        return LSMPS_OK;
+    } catch (const Error& e) {
+        ctx->last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->last_error = "host allocation failed";
+        return LSMPS_ERR_ALLOC;
+    } catch (const std::exception& e) {
+        ctx->last_error = e.what();
+        return LSMPS_ERR_ARG;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int lsmps_abi_version(void) { return LSMPS_ABI_VERSION; }
+
+int lsmps_ctx_create(int device, lsmps_ctx** out) {
+    if (!out) return LSMPS_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return LSMPS_ERR_CUDA;
+    }
+    lsmps_ctx* ctx = new (std::nothrow) lsmps_ctx();
+    if (!ctx) return LSMPS_ERR_ALLOC;
+    ctx->device = device;
+    int rc = guarded(ctx, [&] {
+        LSMPS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        for (auto& e : ctx->ev) LSMPS_CUDA(cudaEventCreate(&e));
+        int* f = ctx->dflags.ensure<int>(16);
+        LSMPS_CUDA(cudaMemsetAsync(f, 0, 16 * sizeof(int), ctx->stream));
+        ctx->scratch.ensure<int>(256);
+        LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+    if (rc != LSMPS_OK) {
+        lsmps_ctx_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return LSMPS_OK;
+}
+
+void lsmps_ctx_destroy(lsmps_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    lsmps_gpu::DevBuf* bufs[] = {&ctx->dflags, &ctx->scratch, &ctx->scan_tmp, &ctx->host_dummy, &ctx->pos,
+                                 &ctx->type_in, &ctx->cell_of, &ctx->slot, &ctx->cell_count, &ctx->cell_start,
+                                 &ctx->perm, &ctx->iperm, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->stype,
+                                 &ctx->scell, &ctx->cls, &ctx->nbr_cnt, &ctx->nbr_row, &ctx->nbr_col,
+                                 &ctx->nbr_stats, &ctx->wls_status, &ctx->wls_z, &ctx->wls_wsum, &ctx->wls_x,
+                                 &ctx->wls_stats, &ctx->wls_sample, &ctx->ref_rank, &ctx->u_of_sorted,
+                                 &ctx->sorted_of_u, &ctx->ref_of_u, &ctx->u_of_ref, &ctx->A_row, &ctx->A_col,
+                                 &ctx->A_val, &ctx->A_valf, &ctx->A_b, &ctx->A_xexact, &ctx->A_dinv,
+                                 &ctx->A_dinvf, &ctx->A_cnt, &ctx->vx, &ctx->vr, &ctx->vr0, &ctx->vp, &ctx->vv,
+                                 &ctx->vs, &ctx->vt, &ctx->vph, &ctx->vsh, &ctx->vtmp, &ctx->fx, &ctx->fr,
+                                 &ctx->fr0, &ctx->fp, &ctx->fv, &ctx->fs, &ctx->ft, &ctx->fph, &ctx->fsh,
+                                 &ctx->red, &ctx->mpnn_w, &ctx->mpnn_m, &ctx->mpnn_v, &ctx->mpnn_g,
+                                 &ctx->mpnn_act, &ctx->mpnn_samples};
+    for (auto* b : bufs) b->release();
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* lsmps_last_error(const lsmps_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int lsmps_get_timings(lsmps_ctx* ctx, double out[8]) {
+    if (!ctx || !out) return LSMPS_ERR_ARG;
+    std::memcpy(out, ctx->timings, sizeof(ctx->timings));
+    return LSMPS_OK;
+}
+
+int lsmps_sync(lsmps_ctx* ctx) {
+    return guarded(ctx, [&] { LSMPS_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+void* lsmps_stream(lsmps_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+uint64_t lsmps_launch_count(void) { return g_launches.load(); }
+
+int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(ms_per_launch && bytes_per_launch && reps > 0, LSMPS_ERR_ARG, "kernel bench arguments");
+        if (kernel == LSMPS_KB_SPMV64 || kernel == LSMPS_KB_SPMV32)
+            solver_kernel_bench(ctx, kernel, reps, ms_per_launch, bytes_per_launch);
+        else if (kernel == LSMPS_KB_NBR_COUNT || kernel == LSMPS_KB_NBR_FILL)
+            nb_kernel_bench(ctx, kernel, reps, ms_per_launch, bytes_per_launch);
+        else if (kernel == LSMPS_KB_WLS)
+            wls_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
+        else
+            throw Error{LSMPS_ERR_ARG, "unknown kernel id"};
+    });
+}
+
+int lsmps_upload_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(n == 0 || (xyz && type), LSMPS_ERR_ARG, "null particle buffers");
+        LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
+        ev_record(ctx, 0);
+        double* pos = ctx->pos.ensure<double>(3 * n + 1);
+        uint8_t* t = ctx->type_in.ensure<uint8_t>(n + 1);
+        if (n) {
+            LSMPS_CUDA(cudaMemcpyAsync(pos, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            LSMPS_CUDA(cudaMemcpyAsync(t, type, n, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        ev_record(ctx, 1);
+        ctx->n = n;
+        ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+        ctx->timings[0] = ev_elapsed(ctx, 0, 1);
+    });
+}
+
+int lsmps_upload_particles_device(lsmps_ctx* ctx, const double* d_xyz, const uint8_t* d_type, size_t n) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(n == 0 || (d_xyz && d_type), LSMPS_ERR_ARG, "null particle buffers");
+        LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
+        ev_record(ctx, 0);
+        double* pos = ctx->pos.ensure<double>(3 * n + 1);
+        uint8_t* t = ctx->type_in.ensure<uint8_t>(n + 1);
+        if (n) {
+            k_pack_particles<<<blocks_for(3 * n, 256), 256, 0, ctx->stream>>>(d_xyz, n, pos);
+            LSMPS_CHECK_LAUNCH();
+            LSMPS_CUDA(cudaMemcpyAsync(t, d_type, n, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        ev_record(ctx, 1);
+        ctx->n = n;
+        ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+        ctx->timings[0] = ev_elapsed(ctx, 0, 1);
+    });
+}
+
+int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l0, int flags,
+                          lsmps_neighbor_stats* out) {
+    return guarded(ctx, [&] {
+        ev_record(ctx, 2);
+        nb_build(ctx, re, max_neighbors, l0, flags, out);
+        ev_record(ctx, 3);
+        ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+    });
+}
+
+int lsmps_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out) {
+    return guarded(ctx, [&] {
+        ev_record(ctx, 4);
+        nb_classify(ctx, l0, out);
+        ev_record(ctx, 5);
+        ctx->timings[2] = ev_elapsed(ctx, 4, 5);
+    });
+}
+
+int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null WLS options");
+        ev_record(ctx, 6);
+        wls_run(ctx, opts, out);
+        ev_record(ctx, 7);
+        ctx->timings[3] = ev_elapsed(ctx, 6, 7);
+    });
+}
+
+int lsmps_ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null PPE options");
+        ppe_assemble(ctx, opts, out);
+        ctx->timings[4] = ctx->ppe_assembly.assembly_ms;
+    });
+}
+
+int lsmps_ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null solver options");
+        ppe_solve(ctx, opts, out);
+    });
+}
+
+int lsmps_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(type || n == 0, LSMPS_ERR_ARG, "null type buffer");
+        nb_download_types(ctx, type, n);
+    });
+}
+
+int lsmps_download_neighbors(lsmps_ctx* ctx, int32_t* row_ptr, int32_t* col, size_t col_cap) {
+    return guarded(ctx, [&] { nb_download(ctx, row_ptr, col, col_cap); });
+}
+
+int lsmps_download_wls(lsmps_ctx* ctx, double* x, int32_t* status, double* z, double* wsum) {
+    return guarded(ctx, [&] { wls_download(ctx, x, status, z, wsum); });
+}
+
+int lsmps_download_ppe(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, double* b, double* x_exact,
+                       int32_t* unknown_particle) {
+    return guarded(ctx, [&] { ppe_download(ctx, row, col, val, b, x_exact, unknown_particle); });
+}
+
+int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(p || u == 0, LSMPS_ERR_ARG, "null pressure buffer");
+        ev_record(ctx, 12);
+        ppe_download_pressure(ctx, p, u);
+        ev_record(ctx, 13);
+        ctx->timings[6] = ev_elapsed(ctx, 12, 13);
+    });
+}
+
+int lsmps_mpnn_init(lsmps_ctx* ctx, uint32_t seed) {
+    return guarded(ctx, [&] { mpnn_init(ctx, seed); });
+}
+int lsmps_mpnn_add_sample(lsmps_ctx* ctx) {
+    return guarded(ctx, [&] { mpnn_add_sample(ctx); });
+}
+int lsmps_mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss_out) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null training options");
+        mpnn_train(ctx, opts, loss_out);
+    });
+}
+int lsmps_mpnn_save(lsmps_ctx* ctx, const char* path) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(path, LSMPS_ERR_ARG, "null path");
+        mpnn_save(ctx, path);
+    });
+}
+int lsmps_mpnn_load(lsmps_ctx* ctx, const char* path) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(path, LSMPS_ERR_ARG, "null path");
+        mpnn_load(ctx, path);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+// The opaque lsmps_ctx: device buffers and state of one particle set on one GPU.
+//
+// HBM layout (n particles, P kept pairs, U unknowns, Z nonzeros):
+//   particles (caller order)   pos: n x double3 AoS (24 B), type_in: n x u8
+//   cell-sorted copies         perm/iperm: n x i32, sx/sy/sz: 3 x n x f64 (SoA), stype, cls:
+//                              n x u8, scell: n x i32
+//   dense cell grid            cell_start: cells + 1 x i32
+//   neighbor CSR (sorted)      nbr_row: n + 1 x i32, nbr_col: P x i32 (sorted indices; the
+//                              reference's row order is ascending sorted index)
+//   WLS                        wls_status: n x i32, wls_z: n x 9 f64, wls_wsum: n x f64
+//   PPE (unknowns in sorted    A_row: U + 1 x i32, A_col: Z x i32, A_val: Z x f64, A_valf:
+//   order)                     Z x f32, b, x*, diag_inv: U x f64, u_of_sorted: n x i32,
+//                              sorted_of_u / ref_of_u / u_of_ref: U x i32
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct lsmps_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    cudaEvent_t ev[16] = {};
+    double timings[8] = {};
+
+    lsmps_gpu::DevBuf dflags;      // int device error flags
+    lsmps_gpu::DevBuf scratch;     // general reduction scratch
+    lsmps_gpu::DevBuf scan_tmp;    // block sums of scans
+    lsmps_gpu::DevBuf host_dummy;
+
+    // ---- particles ----
+    size_t n = 0;
+    lsmps_gpu::DevBuf pos, type_in;
+
+    // ---- grid + neighbors ----
+    double re = 0, re2 = 0, l0 = 0;
+    int maxn = 0;
+    int gmin[3] = {0, 0, 0};
+    int gdim[3] = {0, 0, 0};
+    long long ncells = 0;
+    bool have_neighbors = false, have_classes = false;
+    uint64_t pairs = 0, truncated = 0;
+    int max_cell_occupancy = 0;
+    lsmps_gpu::DevBuf cell_of, slot, cell_count, cell_start, perm, iperm;
+    lsmps_gpu::DevBuf sx, sy, sz, stype, scell, cls;
+    lsmps_gpu::DevBuf nbr_cnt, nbr_row, nbr_col, nbr_stats;
+
+    // ---- WLS ----
+    bool have_wls = false;
+    int wls_nrhs = 0;
+    bool wls_stored = false;
+    lsmps_gpu::DevBuf wls_status, wls_z, wls_wsum, wls_x, wls_stats, wls_sample;
+
+    // ---- PPE ----
+    bool have_ppe = false;
+    int ppe_variant = 0;
+    long long U = 0, nnz = 0;
+    lsmps_gpu::DevBuf ref_rank, u_of_sorted, sorted_of_u, ref_of_u, u_of_ref;
+    lsmps_gpu::DevBuf A_row, A_col, A_val, A_valf, A_b, A_xexact, A_dinv, A_dinvf, A_cnt;
+    lsmps_ppe_stats ppe_assembly{};
+
+    // ---- solver state ----
+    bool have_solution = false;
+    lsmps_gpu::DevBuf vx, vr, vr0, vp, vv, vs, vt, vph, vsh, vtmp;   // FP64 vectors
+    lsmps_gpu::DevBuf fx, fr, fr0, fp, fv, fs, ft, fph, fsh;         // FP32 vectors
+    lsmps_gpu::DevBuf red;                                           // reduction partials + scalars
+
+    // ---- learned preconditioner ----
+    lsmps_gpu::DevBuf mpnn_w, mpnn_m, mpnn_v, mpnn_g, mpnn_act, mpnn_samples;
+    bool have_mpnn = false;
+    int mpnn_nsamples = 0;
+    std::vector<float> mpnn_host_samples_meta;
+
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+namespace lsmps_gpu {
+// Pinned host staging buffer of the context (grow-only).
+void* pinned_ensure(lsmps_ctx* ctx, size_t bytes);
+// Read device int flags, clear them, and throw on any set flag.
+void check_device_flags(lsmps_ctx* ctx, const char* where);
+}  // namespace lsmps_gpu

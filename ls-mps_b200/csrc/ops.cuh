@@ -1,0 +1,43 @@
+// Internal entry points of the library's phases (called by the C ABI in capi.cu).
+#pragma once
+#include "ctx.cuh"
+
+namespace lsmps_gpu {
+
+// neighbors.cu
+void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_neighbor_stats* out);
+void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
+void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out);
+void nb_download(lsmps_ctx* ctx, int32_t* row_ptr, int32_t* col, size_t col_cap);
+void nb_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);
+
+// wls.cu
+void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
+void wls_download(lsmps_ctx* ctx, double* x, int32_t* status, double* z, double* wsum);
+
+// ppe.cu
+void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);
+void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, double* b, double* xe,
+                  int32_t* unknown_particle);
+
+// solver.cu
+void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out);
+void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+
+// mpnn.cu
+void mpnn_init(lsmps_ctx* ctx, uint32_t seed);
+void mpnn_add_sample(lsmps_ctx* ctx);
+void mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss);
+void mpnn_save(lsmps_ctx* ctx, const char* path);
+void mpnn_load(lsmps_ctx* ctx, const char* path);
+
+// Profiling hooks behind lsmps_kernel_bench (mean ms per launch, algorithmic bytes).
+void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
+void wls_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
+void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
+
+// Timing helpers: record event `slot` on the context stream.
+void ev_record(lsmps_ctx* ctx, int slot);
+double ev_elapsed(lsmps_ctx* ctx, int a, int b);
+
+}  // namespace lsmps_gpu

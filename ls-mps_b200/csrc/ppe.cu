@@ -1,0 +1,381 @@
+// Pressure-Poisson (PPE) CSR assembly on sm_100a.
+//
+// Unknowns are the Interior / NearWall particles ranked in caller order and capped at
+// max_unknowns, as the reference's assemble_ppe (src/lsmps.cpp:33-36). Internally they
+// are numbered in cell-sorted order (unknown u = rank among unknowns in the sorted
+// arrays), so a row's column indices ascend and its x-gathers fall in a few contiguous
+// ranges; lsmps_download_ppe maps rows and columns back to the reference's numbering.
+// Each row holds its neighbors that are unknowns in neighbor-list order and the
+// diagonal last, like the reference (src/lsmps.cpp:40-57).
+//
+// Two passes, one thread per row: count (row lengths, scan -> row pointers), then fill
+// (columns, values, p*, and b = A p* in entry order). The reference variant uses exactly
+// rounded FP64 operations in the reference's order, so its CSR values and b are
+// bit-identical to the reference.
+#include <cmath>
+
+#include "ops.cuh"
+#include "scan.cuh"
+
+namespace lsmps_gpu {
+namespace {
+
+struct PpeParams {
+    int variant;
+    double re, l0, shift;
+    int pinned_ref;  // reference variant: the unknown of rank 0 is an identity row
+};
+
+__global__ void k_elig_orig(const int* __restrict__ iperm, const uint8_t* __restrict__ cls, size_t n,
+                            uint8_t* __restrict__ elig) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint8_t t = cls[iperm[i]];
+    elig[i] = (t == LSMPS_INTERIOR || t == LSMPS_NEAR_WALL) ? 1 : 0;
+}
+
+__global__ void k_is_unknown(const int* __restrict__ perm, const uint8_t* __restrict__ elig_orig,
+                             const int* __restrict__ rank_orig, long long cap, size_t n,
+                             uint8_t* __restrict__ isu) {
+    size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int i = perm[k];
+    isu[k] = (elig_orig[i] && rank_orig[i] < cap) ? 1 : 0;
+}
+
+__global__ void k_number_unknowns(const int* __restrict__ perm, const uint8_t* __restrict__ isu,
+                                  const int* __restrict__ rank_orig, size_t n, int* __restrict__ uidx,
+                                  int* __restrict__ sorted_of_u, int* __restrict__ ref_of_u,
+                                  int* __restrict__ u_of_ref) {
+    size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int u = uidx[k];  // exclusive scan of isu
+    if (isu[k]) {
+        int rr = rank_orig[perm[k]];
+        sorted_of_u[u] = (int)k;
+        ref_of_u[u] = rr;
+        u_of_ref[rr] = u;
+    } else {
+        uidx[k] = -1;
+    }
+}
+
+// Off-diagonal coefficient a_ij (> 0 means the row gets -a_ij at column j) of row k for
+// neighbor m; returns false when the pair contributes nothing.
+__device__ __forceinline__ bool row_coeff(const PpeParams& P, double xi, double yi, double zi, double xm,
+                                          double ym, double zm, const double* zk, double ws, double& a) {
+    double dx = xsub(xm, xi), dy = xsub(ym, yi), dz = xsub(zm, zi);
+    double r = __dsqrt_rn(xnorm2(dx, dy, dz));
+    double w = xweight(r, P.re);
+    if (w <= 0) return false;
+    if (P.variant == LSMPS_PPE_REFERENCE) {
+        a = xdiv(w, xmul(r, r));  // src/lsmps.cpp:48
+        return true;
+    }
+    if (P.variant == LSMPS_PPE_SHIFTED) {
+        a = w;
+        return true;
+    }
+    // WLS Laplacian: c = w (q . z) / (r sum_w l0), clipped: only c > 0 contributes.
+    double ir = 1.0 / r;
+    double s = ir / P.l0;
+    double hs = 0.5 * s;
+    double qz = dx * ir * zk[0] + dy * ir * zk[1] + dz * ir * zk[2] + dx * dx * hs * zk[3] + dy * dy * hs * zk[4] +
+                dz * dz * hs * zk[5] + dx * dy * s * zk[6] + dx * dz * s * zk[7] + dy * dz * s * zk[8];
+    a = w * qz / (r * ws * P.l0);
+    return a > 0;
+}
+
+__device__ __forceinline__ bool wls_row_valid(int st) { return st == 0 || st == 1; }
+
+// Count pass: entries per row (diagonal included).
+__global__ void k_ppe_count(PpeParams P, long long U, const int* __restrict__ sorted_of_u,
+                            const int* __restrict__ ref_of_u, const int* __restrict__ uidx,
+                            const double* __restrict__ sx, const double* __restrict__ sy,
+                            const double* __restrict__ sz, const int* __restrict__ row,
+                            const int* __restrict__ col, const int* __restrict__ wst,
+                            const double* __restrict__ wz, const double* __restrict__ wws,
+                            int* __restrict__ cnt) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    int k = sorted_of_u[u];
+    if (P.variant == LSMPS_PPE_REFERENCE && ref_of_u[u] == P.pinned_ref) { cnt[u] = 1; return; }
+    if (P.variant == LSMPS_PPE_WLS && !wls_row_valid(wst[k])) { cnt[u] = 1; return; }
+    double xi = sx[k], yi = sy[k], zi = sz[k];
+    double zk[K];
+    double ws = 0;
+    if (P.variant == LSMPS_PPE_WLS) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a];
+        ws = wws[k];
+    }
+    int c = 0;
+    double diag = 0.0;
+    for (int e = row[k]; e < row[k + 1]; ++e) {
+        int m = col[e];
+        bool is_u = uidx[m] >= 0;
+        if (P.variant != LSMPS_PPE_WLS && !is_u) continue;
+        double a;
+        if (!row_coeff(P, xi, yi, zi, sx[m], sy[m], sz[m], zk, ws, a)) continue;
+        diag = xadd(diag, a);
+        if (is_u) ++c;
+    }
+    // WLS rows without a positive, finite diagonal become identity rows (same test in fill)
+    if (P.variant == LSMPS_PPE_WLS && !(diag > 0 && isfinite(diag))) c = 0;
+    cnt[u] = c + 1;
+}
+
+// Fill pass. stats (u64): [0] neumann, [1] failed rows.
+__global__ void k_ppe_fill(PpeParams P, long long U, const int* __restrict__ sorted_of_u,
+                           const int* __restrict__ ref_of_u, const int* __restrict__ uidx,
+                           const double* __restrict__ sx, const double* __restrict__ sy,
+                           const double* __restrict__ sz, const uint8_t* __restrict__ cls,
+                           const int* __restrict__ row, const int* __restrict__ col,
+                           const int* __restrict__ wst, const double* __restrict__ wz,
+                           const double* __restrict__ wws, const int* __restrict__ arow,
+                           int* __restrict__ acol, double* __restrict__ aval, double* __restrict__ xexact,
+                           unsigned long long* stats) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int neumann = 0, failed = 0;
+    if (u < U) {
+        int k = sorted_of_u[u];
+        double xi = sx[k], yi = sy[k], zi = sz[k];
+        xexact[u] = P.variant == LSMPS_PPE_REFERENCE ? xadd(xmul(xi, xi), xmul(yi, yi))
+                                                     : sin(0.3 * xi) * cos(0.2 * yi) + 0.1 * zi;
+        int o = arow[u], oe = arow[u + 1];
+        bool pinned = P.variant == LSMPS_PPE_REFERENCE && ref_of_u[u] == P.pinned_ref;
+        if (pinned) {
+            acol[o] = (int)u;
+            aval[o] = 1.0;
+        } else {
+            double diag = 0.0;
+            bool identity = P.variant == LSMPS_PPE_WLS && !wls_row_valid(wst[k]);
+            if (!identity) {
+                double zk[K];
+                double ws = 0;
+                if (P.variant == LSMPS_PPE_WLS) {
+#pragma unroll
+                    for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a];
+                    ws = wws[k];
+                }
+                int p = o;
+                for (int e = row[k]; e < row[k + 1]; ++e) {
+                    int m = col[e];
+                    int cj = uidx[m];
+                    if (P.variant != LSMPS_PPE_WLS && cj < 0) continue;
+                    double a;
+                    if (!row_coeff(P, xi, yi, zi, sx[m], sy[m], sz[m], zk, ws, a)) continue;
+                    diag = xadd(diag, a);
+                    if (cj >= 0 && p < oe - 1) {  // the count pass sized the row
+                        acol[p] = cj;
+                        aval[p] = -a;
+                        ++p;
+                    }
+                }
+                if (P.variant == LSMPS_PPE_WLS && oe - o == 1) {
+                    // count pass found no positive finite diagonal, or only Dirichlet neighbors
+                    if (!(diag > 0 && isfinite(diag))) identity = true;
+                }
+                if (P.variant != LSMPS_PPE_REFERENCE) diag = diag * (1.0 + P.shift);
+            }
+            if (identity) {
+                failed = 1;
+                diag = 1.0;
+            } else if (diag <= 0 || !isfinite(diag)) {  // src/lsmps.cpp:52
+                failed = 1;
+                diag = 1.0;
+            }
+            acol[oe - 1] = (int)u;
+            aval[oe - 1] = diag;
+            if (cls[k] == LSMPS_NEAR_WALL) neumann = 1;
+        }
+    }
+    neumann = __reduce_add_sync(0xffffffffu, neumann);
+    failed = __reduce_add_sync(0xffffffffu, failed);
+    if ((threadIdx.x & 31) == 0) {
+        if (neumann) atomicAdd(&stats[0], (unsigned long long)neumann);
+        if (failed) atomicAdd(&stats[1], (unsigned long long)failed);
+    }
+}
+
+// b = A p* in entry order (src/lsmps.cpp:59-61); also the inverse diagonal for Jacobi.
+__global__ void k_ppe_rhs(long long U, const int* __restrict__ arow, const int* __restrict__ acol,
+                          const double* __restrict__ aval, const double* __restrict__ xexact,
+                          double* __restrict__ b, double* __restrict__ dinv) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    double s = 0;
+    int e0 = arow[u], e1 = arow[u + 1];
+    for (int e = e0; e < e1; ++e) s = xadd(s, xmul(aval[e], xexact[acol[e]]));
+    b[u] = s;
+    double d = aval[e1 - 1];
+    dinv[u] = d != 0.0 ? 1.0 / d : 1.0;
+}
+
+// ---- download in the reference numbering ----
+__global__ void k_ref_counts(const int* __restrict__ u_of_ref, const int* __restrict__ arow, long long U,
+                             int* __restrict__ cnt) {
+    long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (rr >= U) return;
+    int u = u_of_ref[rr];
+    cnt[rr] = arow[u + 1] - arow[u];
+}
+
+__global__ void k_ref_fill(const int* __restrict__ u_of_ref, const int* __restrict__ ref_of_u,
+                           const int* __restrict__ arow, const int* __restrict__ acol,
+                           const double* __restrict__ aval, const double* __restrict__ b,
+                           const double* __restrict__ xe, const int* __restrict__ sorted_of_u,
+                           const int* __restrict__ perm, long long U, const int* __restrict__ orow,
+                           int* __restrict__ ocol, double* __restrict__ oval, double* __restrict__ ob,
+                           double* __restrict__ oxe, int* __restrict__ opart) {
+    long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (rr >= U) return;
+    int u = u_of_ref[rr];
+    int o = orow[rr];
+    for (int e = arow[u]; e < arow[u + 1]; ++e, ++o) {
+        ocol[o] = ref_of_u[acol[e]];
+        oval[o] = aval[e];
+    }
+    ob[rr] = b[u];
+    oxe[rr] = xe[u];
+    opart[rr] = perm[sorted_of_u[u]];
+}
+
+}  // namespace
+
+void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out) {
+    LSMPS_REQUIRE(ctx->have_neighbors && ctx->have_classes, LSMPS_ERR_STATE,
+                  "PPE assembly needs neighbor lists and classification first");
+    LSMPS_REQUIRE(o && o->variant >= 0 && o->variant <= 2, LSMPS_ERR_ARG, "unknown PPE variant");
+    LSMPS_REQUIRE(o->variant != LSMPS_PPE_WLS || ctx->have_wls, LSMPS_ERR_STATE,
+                  "WLS-Laplacian PPE needs the all-particle WLS (lsmps_wls mode 1) first");
+    LSMPS_REQUIRE(o->re > 0 && o->l0 > 0, LSMPS_ERR_ARG, "PPE options need re > 0 and l0 > 0");
+    cudaStream_t s = ctx->stream;
+    size_t n = ctx->n;
+    int* dflag = ctx->dflags.get<int>();
+    ev_record(ctx, 8);
+    long long cap = std::min<long long>((long long)n, std::max<long long>(0, o->max_unknowns));
+
+    uint8_t* elig = ctx->A_cnt.ensure<uint8_t>(2 * n + 16);
+    uint8_t* isu = elig + n + 8;
+    int* rank = ctx->ref_rank.ensure<int>(n + 1);
+    int* uidx = ctx->u_of_sorted.ensure<int>(n + 1);
+    if (n) {
+        k_elig_orig<<<blocks_for(n, 256), 256, 0, s>>>(ctx->iperm.get<int>(), ctx->cls.get<uint8_t>(), n, elig);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<uint8_t>(elig, rank, (long long)n, s, ctx->scan_tmp, dflag);
+    if (n) {
+        k_is_unknown<<<blocks_for(n, 256), 256, 0, s>>>(ctx->perm.get<int>(), elig, rank, cap, n, isu);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<uint8_t>(isu, uidx, (long long)n, s, ctx->scan_tmp, dflag);
+    int hU = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&hU, uidx + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    const long long U = hU;
+    int* sorted_of_u = ctx->sorted_of_u.ensure<int>(U + 1);
+    int* ref_of_u = ctx->ref_of_u.ensure<int>(U + 1);
+    int* u_of_ref = ctx->u_of_ref.ensure<int>(U + 1);
+    if (n) {
+        k_number_unknowns<<<blocks_for(n, 256), 256, 0, s>>>(ctx->perm.get<int>(), isu, rank, n, uidx, sorted_of_u,
+                                                             ref_of_u, u_of_ref);
+        LSMPS_CHECK_LAUNCH();
+    }
+    PpeParams P{o->variant, o->re, o->l0, o->diag_shift, 0};
+    int* cnt = ctx->vtmp.ensure<int>(U + 1);
+    int* arow = ctx->A_row.ensure<int>(U + 1);
+    const int* wst = ctx->have_wls ? ctx->wls_status.get<int>() : nullptr;
+    const double* wz = ctx->have_wls ? ctx->wls_z.get<double>() : nullptr;
+    const double* wws = ctx->have_wls ? ctx->wls_wsum.get<double>() : nullptr;
+    if (U) {
+        k_ppe_count<<<blocks_for(U, 128), 128, 0, s>>>(P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(),
+                                                       ctx->sy.get<double>(), ctx->sz.get<double>(),
+                                                       ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), wst, wz,
+                                                       wws, cnt);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<int>(cnt, arow, U, s, ctx->scan_tmp, dflag);
+    int hnnz = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&hnnz, arow + U, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    check_device_flags(ctx, "PPE row count");
+    const long long nnz = hnnz;
+    int* acol = ctx->A_col.ensure<int>(nnz + 1);
+    double* aval = ctx->A_val.ensure<double>(nnz + 1);
+    double* xe = ctx->A_xexact.ensure<double>(U + 1);
+    double* b = ctx->A_b.ensure<double>(U + 1);
+    double* dinv = ctx->A_dinv.ensure<double>(U + 1);
+    auto* st = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 32);
+    LSMPS_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), s));
+    if (U) {
+        k_ppe_fill<<<blocks_for(U, 128), 128, 0, s>>>(P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(),
+                                                      ctx->sy.get<double>(), ctx->sz.get<double>(),
+                                                      ctx->cls.get<uint8_t>(), ctx->nbr_row.get<int>(),
+                                                      ctx->nbr_col.get<int>(), wst, wz, wws, arow, acol, aval,
+                                                      xe, st);
+        LSMPS_CHECK_LAUNCH();
+        k_ppe_rhs<<<blocks_for(U, 256), 256, 0, s>>>(U, arow, acol, aval, xe, b, dinv);
+        LSMPS_CHECK_LAUNCH();
+    }
+    ev_record(ctx, 9);
+    unsigned long long hs[2];
+    LSMPS_CUDA(cudaMemcpyAsync(hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    lsmps_ppe_stats ps{};
+    ps.unknowns = (uint64_t)U;
+    ps.nnz = (uint64_t)nnz;
+    ps.dirichlet = (uint64_t)(n - U);
+    // the reference counts NearWall rows except the pinned row 0 (src/lsmps.cpp:45,56)
+    ps.neumann = hs[0];
+    ps.failed_rows = hs[1];
+    ps.assembly_ms = ev_elapsed(ctx, 8, 9);
+    ctx->U = U;
+    ctx->nnz = nnz;
+    ctx->ppe_variant = o->variant;
+    ctx->have_ppe = true;
+    ctx->have_solution = false;
+    ctx->ppe_assembly = ps;
+    if (out) *out = ps;
+}
+
+void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, double* b, double* xe,
+                  int32_t* unknown_particle) {
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "no PPE assembled");
+    cudaStream_t s = ctx->stream;
+    long long U = ctx->U, nnz = ctx->nnz;
+    size_t bytes = (U + 1) * 4 * 2 + nnz * 12 + U * 16 + U * 4 + 256;
+    char* base = ctx->vtmp.ensure<char>(bytes);
+    int* cnt = reinterpret_cast<int*>(base);
+    int* orow = cnt + (U + 1);
+    double* oval = reinterpret_cast<double*>(base + (((U + 1) * 8 + 15) / 16) * 16);
+    double* ob = oval + nnz;
+    double* oxe = ob + U;
+    int* ocol = reinterpret_cast<int*>(oxe + U);
+    int* opart = ocol + nnz;
+    if (U) {
+        k_ref_counts<<<blocks_for(U, 256), 256, 0, s>>>(ctx->u_of_ref.get<int>(), ctx->A_row.get<int>(), U, cnt);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<int>(cnt, orow, U, s, ctx->scan_tmp, ctx->dflags.get<int>());
+    if (U) {
+        k_ref_fill<<<blocks_for(U, 128), 128, 0, s>>>(ctx->u_of_ref.get<int>(), ctx->ref_of_u.get<int>(),
+                                                      ctx->A_row.get<int>(), ctx->A_col.get<int>(),
+                                                      ctx->A_val.get<double>(), ctx->A_b.get<double>(),
+                                                      ctx->A_xexact.get<double>(), ctx->sorted_of_u.get<int>(),
+                                                      ctx->perm.get<int>(), U, orow, ocol, oval, ob, oxe, opart);
+        LSMPS_CHECK_LAUNCH();
+    }
+    if (row) LSMPS_CUDA(cudaMemcpyAsync(row, orow, (U + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (U) {
+        if (col) LSMPS_CUDA(cudaMemcpyAsync(col, ocol, nnz * sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (val) LSMPS_CUDA(cudaMemcpyAsync(val, oval, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (b) LSMPS_CUDA(cudaMemcpyAsync(b, ob, U * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (xe) LSMPS_CUDA(cudaMemcpyAsync(xe, oxe, U * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (unknown_particle)
+            LSMPS_CUDA(cudaMemcpyAsync(unknown_particle, opart, U * sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace lsmps_gpu

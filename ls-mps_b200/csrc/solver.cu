@@ -1,0 +1,960 @@
+// PPE solvers on sm_100a.
+//
+// * REFERENCE: the reference's unpreconditioned FP64 BiCGStab (src/lsmps.cpp:65-67)
+//   reproduced bit for bit: exactly rounded FP64 vector updates in the reference's
+//   expression order, row-sequential SpMV in stored entry order, and dot products summed
+//   sequentially in the reference's unknown order by one thread (products formed in
+//   parallel). Slow by design; it exists so small cases match the reference exactly.
+// * FP64 / JACOBI: the same iteration with GPU reductions. Jacobi right preconditioning
+//   is applied as a column scaling of the matrix (A D^-1, solve for y, x = D^-1 y), which
+//   costs nothing per iteration.
+// * MIXED / LEARNED: FP64 iterative refinement, r = b - A x with the FP64 matrix, around
+//   FP32 Jacobi-BiCGStab inner solves of A D^-1 y = r / |r| on an FP32 copy of the matrix.
+//   LEARNED starts each inner solve from the message-passing network's guess.
+//
+// The fast engine runs five kernels per iteration. Each reduction is fused into the
+// kernel that produces its operands; the last block of the grid to finish (atomic ticket)
+// sums the per-block partials in a fixed order, so results are deterministic, and updates
+// the scalars in device memory. Every kernel returns at once when the run is done, so a
+// CUDA graph of several iterations can be replayed without host round trips; the host
+// reads the status once per graph launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ops.cuh"
+#include "scan.cuh"
+#include "solver.cuh"
+
+namespace lsmps_gpu {
+
+void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y);  // mpnn.cu
+bool mpnn_ready(lsmps_ctx* ctx);
+
+namespace {
+
+constexpr int RB = 256;            // threads per block
+constexpr int RGRID = 148 * 6;     // persistent grid of the vector / SpMV kernels
+
+// ---------------------------------------------------------------------------------------
+// REFERENCE (bit-exact) solver
+// ---------------------------------------------------------------------------------------
+struct ExactState {
+    double rho, rho0, alpha, omega, beta, bnorm, thresh, den, tt;
+    int done;    // 1 converged, 2 break
+    int s_conv;
+    int iters;
+    int it;
+    int converged;
+};
+
+__global__ void k_x_prod(const double* __restrict__ a, const double* __restrict__ b,
+                         const int* __restrict__ u_of_ref, long long U, double* __restrict__ prod,
+                         const ExactState* st) {
+    if (st->done) return;
+    for (long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x; rr < U;
+         rr += (long long)gridDim.x * blockDim.x) {
+        int u = u_of_ref[rr];
+        prod[rr] = xmul(a[u], b[u]);
+    }
+}
+
+enum ExactOp { OP_BNORM, OP_RHO, OP_DEN, OP_SN, OP_TT, OP_TS, OP_RN };
+
+// One thread: sequential sum (the reference's dot, src/lsmps.cpp:66) and the scalar step.
+__global__ void k_x_tail(const double* __restrict__ prod, long long U, ExactState* st, int op, double tol,
+                         int max_iter) {
+    if (threadIdx.x || blockIdx.x) return;
+    if (st->done) return;
+    double s = 0;
+    for (long long rr = 0; rr < U; ++rr) s = xadd(s, prod[rr]);
+    switch (op) {
+        case OP_BNORM:
+            st->bnorm = __dsqrt_rn(s);
+            st->thresh = xmul(tol, fmax(1.0, st->bnorm));
+            st->rho0 = st->alpha = st->omega = 1.0;
+            st->it = 0;
+            st->iters = 0;
+            if (max_iter <= 0) st->done = 2;
+            break;
+        case OP_RHO:
+            st->rho = s;
+            if (fabs(s) < 1e-30) { st->done = 2; break; }
+            st->beta = xmul(xdiv(st->rho, st->rho0), xdiv(st->alpha, st->omega));
+            break;
+        case OP_DEN:
+            if (fabs(s) < 1e-30) { st->done = 2; break; }
+            st->alpha = xdiv(st->rho, s);
+            break;
+        case OP_SN:
+            if (__dsqrt_rn(s) <= st->thresh) { st->s_conv = 1; st->iters = st->it + 1; st->converged = 1; }
+            break;
+        case OP_TT:
+            st->tt = s;
+            if (s < 1e-30) st->done = 2;
+            break;
+        case OP_TS:
+            st->omega = xdiv(s, st->tt);
+            break;
+        case OP_RN:
+            st->iters = st->it + 1;
+            if (__dsqrt_rn(s) <= st->thresh) { st->converged = 1; st->done = 1; break; }
+            if (fabs(st->omega) < 1e-30) { st->done = 2; break; }
+            st->rho0 = st->rho;
+            st->it += 1;
+            if (st->it >= max_iter) st->done = 2;
+            break;
+    }
+}
+
+__global__ void k_x_spmv(long long U, const int* __restrict__ row, const int* __restrict__ col,
+                         const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                         const ExactState* st, int check) {
+    if (check && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < U;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int e = row[i]; e < row[i + 1]; ++e) s = xadd(s, xmul(val[e], x[col[e]]));
+        y[i] = s;
+    }
+}
+
+// kind 0: p = r + beta (p - omega v); 1: s = r - alpha v; 2: x += alpha p (and finish when
+// the |s| test passed); 3: x += alpha p + omega s, r = s - omega t.
+__global__ void k_x_vec(long long U, int kind, double* __restrict__ x, double* __restrict__ r,
+                        double* __restrict__ p, const double* __restrict__ v, double* __restrict__ s,
+                        const double* __restrict__ t, ExactState* st) {
+    if (st->done) return;
+    if (kind == 2 && !st->s_conv) return;
+    if (kind == 3 && st->s_conv) return;
+    const double alpha = st->alpha, beta = st->beta, omega = st->omega;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < U;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (kind == 0) p[i] = xadd(r[i], xmul(beta, xsub(p[i], xmul(omega, v[i]))));
+        else if (kind == 1) s[i] = xsub(r[i], xmul(alpha, v[i]));
+        else if (kind == 2) { x[i] = xadd(x[i], xmul(alpha, p[i])); r[i] = s[i]; }
+        else {
+            x[i] = xadd(x[i], xadd(xmul(alpha, p[i]), xmul(omega, s[i])));
+            r[i] = xsub(s[i], xmul(omega, t[i]));
+        }
+    }
+}
+
+__global__ void k_x_finish_sconv(ExactState* st) {
+    if (st->s_conv && !st->done) st->done = 1;
+}
+
+// Final statistics (src/lsmps.cpp:67 tail): sequential sums in reference order.
+__global__ void k_x_final(const double* __restrict__ Ax, const double* __restrict__ b,
+                          const double* __restrict__ x, const double* __restrict__ xe,
+                          const int* __restrict__ u_of_ref, long long U, double* out) {
+    if (threadIdx.x || blockIdx.x) return;
+    double res = 0, se = 0, mx = 0, exn = 0;
+    for (long long rr = 0; rr < U; ++rr) {
+        int u = u_of_ref[rr];
+        double d = xsub(Ax[u], b[u]);
+        res = xadd(res, xmul(d, d));
+        double e = xsub(x[u], xe[u]);
+        se = xadd(se, xmul(e, e));
+        exn = xadd(exn, xmul(xe[u], xe[u]));
+        mx = fmax(mx, fabs(e));
+    }
+    out[0] = __dsqrt_rn(res);
+    out[1] = __dsqrt_rn(xdiv(se, fmax(exn, 1e-30)));
+    out[2] = mx;
+}
+
+// ---------------------------------------------------------------------------------------
+// Fast engine
+// ---------------------------------------------------------------------------------------
+struct Partials {
+    double* a;   // RGRID entries
+    double* b;   // RGRID entries
+};
+
+// Block sum of two doubles into partials[blockIdx]; returns true in the last block to
+// arrive, after which the caller may read all partials (fixed-order final sum).
+__device__ __forceinline__ bool block_partials(double va, double vb, Partials P, unsigned int* counter) {
+    __shared__ double sa[RB / 32], sb[RB / 32];
+    __shared__ bool last;
+    va = warp_sum(va);
+    vb = warp_sum(vb);
+    int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sa[w] = va; sb[w] = vb; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0, tb = 0;
+        for (int k = 0; k < RB / 32; ++k) { ta += sa[k]; tb += sb[k]; }
+        P.a[blockIdx.x] = ta;
+        P.b[blockIdx.x] = tb;
+        __threadfence();
+        unsigned int ticket = atomicAdd(counter, 1u);
+        last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    return last;
+}
+
+// In the last block: fixed-order sum of the partials (thread t sums entries t, t+RB, ...
+// then a fixed tree), result in *ra / *rb for thread 0.
+__device__ __forceinline__ void final_sum(Partials P, double* ra, double* rb) {
+    __shared__ double sa[RB / 32], sb[RB / 32];
+    double va = 0, vb = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += RB) {
+        va += __ldcg(P.a + k);
+        vb += __ldcg(P.b + k);
+    }
+    va = warp_sum(va);
+    vb = warp_sum(vb);
+    if ((threadIdx.x & 31) == 0) { sa[threadIdx.x >> 5] = va; sb[threadIdx.x >> 5] = vb; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0, tb = 0;
+        for (int k = 0; k < RB / 32; ++k) { ta += sa[k]; tb += sb[k]; }
+        *ra = ta;
+        *rb = tb;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T ldstream(const T* p) { return __ldcs(p); }
+
+// y_i = sum_e val[e] x[col[e]] for rows handled by a group of G lanes; returns the row sum
+// in every lane of the group.
+template <class T, int G>
+__device__ __forceinline__ double row_dot(const int* __restrict__ row, const int* __restrict__ col,
+                                          const T* __restrict__ val, const T* __restrict__ x, long long i,
+                                          int g) {
+    int e0 = row[i], e1 = row[i + 1];
+    double s = 0;
+    for (int e = e0 + g; e < e1; e += G) s += (double)ldstream(val + e) * (double)x[ldstream(col + e)];
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+    return s;
+}
+
+// p = r + beta (p - omega v)
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__ r, T* __restrict__ p,
+                                              const T* __restrict__ v, const BcgScalars* S) {
+    if (S->done) return;
+    const T beta = (T)S->beta, omega = (T)S->omega;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB)
+        p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// v = A p; den = (r0, v); alpha = rho / den
+template <class T, int G>
+__global__ void __launch_bounds__(RB) k_bcg_v(Csr<T> A, const T* __restrict__ p, T* __restrict__ v,
+                                              const T* __restrict__ r0, BcgScalars* S, Partials P) {
+    if (S->done) return;
+    const int g = threadIdx.x & (G - 1);
+    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
+    const long long ngroups = (long long)gridDim.x * RB / G;
+    double acc = 0;
+    for (long long i = gid; i < A.n; i += ngroups) {
+        double y = row_dot<T, G>(A.row, A.col, A.val, p, i, g);
+        if (g == 0) {
+            v[i] = (T)y;
+            acc += (double)r0[i] * (double)(T)y;
+        }
+    }
+    if (block_partials(acc, 0.0, P, &S->counter[0])) {
+        double den, unused;
+        final_sum(P, &den, &unused);
+        if (threadIdx.x == 0) {
+            S->counter[0] = 0;
+            if (!isfinite(den)) { S->nonfinite = 1; S->done = 2; }
+            else if (fabs(den) < 1e-30) S->done = 2;
+            else S->alpha = S->rho / den;
+        }
+    }
+}
+
+// s = r - alpha v; |s|
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__ r, const T* __restrict__ v,
+                                              T* __restrict__ s, BcgScalars* S, Partials P) {
+    if (S->done) return;
+    const T alpha = (T)S->alpha;
+    double acc = 0;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+        T si = r[i] - alpha * v[i];
+        s[i] = si;
+        acc += (double)si * (double)si;
+    }
+    if (block_partials(acc, 0.0, P, &S->counter[1])) {
+        double ss, unused;
+        final_sum(P, &ss, &unused);
+        if (threadIdx.x == 0) {
+            S->counter[1] = 0;
+            S->sn = sqrt(ss);
+            if (S->sn <= S->thresh) { S->s_conv = 1; S->iters = S->it + 1; }
+        }
+    }
+}
+
+// t = A s; omega = (t, s) / (t, t)
+template <class T, int G>
+__global__ void __launch_bounds__(RB) k_bcg_t(Csr<T> A, const T* __restrict__ s, T* __restrict__ t,
+                                              BcgScalars* S, Partials P) {
+    if (S->done || S->s_conv) return;
+    const int g = threadIdx.x & (G - 1);
+    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
+    const long long ngroups = (long long)gridDim.x * RB / G;
+    double ats = 0, att = 0;
+    for (long long i = gid; i < A.n; i += ngroups) {
+        double y = row_dot<T, G>(A.row, A.col, A.val, s, i, g);
+        if (g == 0) {
+            T ti = (T)y;
+            t[i] = ti;
+            ats += (double)ti * (double)s[i];
+            att += (double)ti * (double)ti;
+        }
+    }
+    if (block_partials(ats, att, P, &S->counter[2])) {
+        double ts, tt;
+        final_sum(P, &ts, &tt);
+        if (threadIdx.x == 0) {
+            S->counter[2] = 0;
+            S->tt = tt;
+            if (!isfinite(tt) || !isfinite(ts)) { S->nonfinite = 1; S->done = 2; }
+            else if (tt < 1e-30) S->done = 2;
+            else S->omega = ts / tt;
+        }
+    }
+}
+
+// x += alpha p + omega s; r = s - omega t; |r|, rho' = (r0, r); beta
+// (or, when the |s| test passed: x += alpha p and finish)
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T* __restrict__ r,
+                                              const T* __restrict__ p, const T* __restrict__ s,
+                                              const T* __restrict__ t, const T* __restrict__ r0,
+                                              BcgScalars* S, Partials P) {
+    if (S->done) return;
+    const T alpha = (T)S->alpha, omega = (T)S->omega;
+    if (S->s_conv) {
+        for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+            x[i] += alpha * p[i];
+            r[i] = s[i];
+        }
+        __syncthreads();
+        if (block_partials(0.0, 0.0, P, &S->counter[3]) && threadIdx.x == 0) {
+            S->counter[3] = 0;
+            S->rn = S->sn;
+            S->done = 1;
+        }
+        return;
+    }
+    double arr = 0, ar0r = 0;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+        T si = s[i];
+        x[i] += alpha * p[i] + omega * si;
+        T ri = si - omega * t[i];
+        r[i] = ri;
+        arr += (double)ri * (double)ri;
+        ar0r += (double)r0[i] * (double)ri;
+    }
+    if (block_partials(arr, ar0r, P, &S->counter[3])) {
+        double rr, rho;
+        final_sum(P, &rr, &rho);
+        if (threadIdx.x == 0) {
+            S->counter[3] = 0;
+            S->iters = S->it + 1;
+            S->it += 1;
+            double rn = sqrt(rr);
+            S->rn = rn;
+            if (!isfinite(rn)) { S->nonfinite = 1; S->done = 2; return; }
+            if (rn <= S->thresh) { S->done = 1; return; }
+            // stall bookkeeping (learned solver fallback rule)
+            if (rn < 0.99 * S->best_rn) { S->best_rn = rn; S->since_best = 0; }
+            else if (++S->since_best >= S->stall_window && S->stall_window > 0) { S->done = 4; return; }
+            if (fabs(S->omega) < 1e-30) { S->done = 2; return; }
+            if (S->it >= S->max_iter) { S->done = 3; return; }
+            if (fabs(rho) < 1e-30) { S->done = 2; return; }
+            S->beta = (rho / S->rho) * (S->alpha / S->omega);
+            S->rho0 = S->rho;
+            S->rho = rho;
+        }
+    }
+}
+
+// Initialisation: r = b - A x (or r = b when x = 0), r0 = r, p = v = 0, |b|, rho = (r0, r).
+template <class T, int G>
+__global__ void __launch_bounds__(RB) k_bcg_init(Csr<T> A, const T* __restrict__ b, const T* __restrict__ x,
+                                                 int use_x, T* __restrict__ r, T* __restrict__ r0,
+                                                 T* __restrict__ p, T* __restrict__ v, BcgScalars* S,
+                                                 Partials P, double tol, double bnorm_override) {
+    const int g = threadIdx.x & (G - 1);
+    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
+    const long long ngroups = (long long)gridDim.x * RB / G;
+    double abb = 0, arr = 0;
+    for (long long i = gid; i < A.n; i += ngroups) {
+        double ax = use_x ? row_dot<T, G>(A.row, A.col, A.val, x, i, g) : 0.0;
+        if (g == 0) {
+            T bi = b[i];
+            T ri = use_x ? (T)((double)bi - ax) : bi;
+            r[i] = ri;
+            r0[i] = ri;
+            p[i] = 0;
+            v[i] = 0;
+            abb += (double)bi * (double)bi;
+            arr += (double)ri * (double)ri;
+        }
+    }
+    if (block_partials(abb, arr, P, &S->counter[4])) {
+        double bb, rr;
+        final_sum(P, &bb, &rr);
+        if (threadIdx.x == 0) {
+            S->counter[4] = 0;
+            double bnorm = bnorm_override >= 0 ? bnorm_override : sqrt(bb);
+            S->thresh = tol * fmax(1.0, bnorm);
+            S->rho0 = S->alpha = S->omega = 1.0;
+            S->rho = rr;
+            S->beta = rr;  // (rho / rho0) (alpha / omega) with rho0 = alpha = omega = 1
+            S->rn = sqrt(rr);
+            S->best_rn = S->rn;
+            S->since_best = 0;
+            S->it = 0;
+            S->iters = 0;
+            S->s_conv = 0;
+            S->nonfinite = !isfinite(rr) ? 1 : 0;
+            S->done = 0;
+            if (S->nonfinite) S->done = 2;
+            else if (S->rn <= S->thresh) S->done = 1;  // already converged
+            else if (fabs(rr) < 1e-30) S->done = 2;
+            else if (S->max_iter <= 0) S->done = 3;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Mixed-precision helpers
+// ---------------------------------------------------------------------------------------
+// FP32 copy of A D^-1 (column scaling) and FP64 A D^-1.
+template <class T>
+__global__ void k_scale_cols(long long nnz, const int* __restrict__ col, const double* __restrict__ val,
+                             const double* __restrict__ dinv, T* __restrict__ out) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
+        out[e] = (T)(val[e] * dinv[col[e]]);
+}
+
+// r = b - A x (FP64), |r|^2 into partials; rf = r / |r| is produced by k_scale_rhs.
+template <int G>
+__global__ void __launch_bounds__(RB) k_residual64(Csr<double> A, const double* __restrict__ b,
+                                                   const double* __restrict__ x, double* __restrict__ r,
+                                                   double* out2, Partials P, unsigned int* counter) {
+    const int g = threadIdx.x & (G - 1);
+    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
+    const long long ngroups = (long long)gridDim.x * RB / G;
+    double arr = 0, abb = 0;
+    for (long long i = gid; i < A.n; i += ngroups) {
+        double ax = row_dot<double, G>(A.row, A.col, A.val, x, i, g);
+        if (g == 0) {
+            double ri = b[i] - ax;
+            r[i] = ri;
+            arr += ri * ri;
+            abb += b[i] * b[i];
+        }
+    }
+    if (block_partials(arr, abb, P, counter)) {
+        double rr, bb;
+        final_sum(P, &rr, &bb);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            out2[0] = rr;
+            out2[1] = bb;
+        }
+    }
+}
+
+__global__ void k_scale_rhs(long long n, const double* __restrict__ r, const double* scal, float* __restrict__ rf,
+                            float* __restrict__ yf) {
+    double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0]) : 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        rf[i] = (float)(r[i] * inv);
+        if (yf) yf[i] = 0.f;
+    }
+}
+
+// x += |r| D^-1 y
+__global__ void k_apply_correction(long long n, double* __restrict__ x, const float* __restrict__ y,
+                                   const double* __restrict__ dinv, const double* scal) {
+    double nr = sqrt(scal[0]);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] += nr * dinv[i] * (double)y[i];
+}
+
+__global__ void k_unscale(long long n, double* __restrict__ x, const double* __restrict__ dinv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] *= dinv[i];
+}
+
+__global__ void k_scale_by_diag(long long n, double* __restrict__ x, const double* __restrict__ dinv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = dinv[i] != 0 ? x[i] / dinv[i] : x[i];
+}
+
+// error statistics against p*: |x - p*|^2, |p*|^2, max |x - p*| (fixed-order partials)
+__global__ void __launch_bounds__(RB) k_error_stats(long long n, const double* __restrict__ x,
+                                                    const double* __restrict__ xe, double* out3, Partials P,
+                                                    unsigned int* counter, unsigned long long* maxbits) {
+    double se = 0, ee = 0, mx = 0;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+        double e = x[i] - xe[i];
+        se += e * e;
+        ee += xe[i] * xe[i];
+        mx = fmax(mx, fabs(e));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+    if (block_partials(se, ee, P, counter)) {
+        double a, b;
+        final_sum(P, &a, &b);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            out3[0] = a;
+            out3[1] = b;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+struct Engine {
+    lsmps_ctx* ctx;
+    cudaStream_t s;
+    BcgScalars* S;
+    Partials P;
+    int group;  // lanes per row (4, 8, 16 or 32)
+};
+
+template <class T>
+struct Vecs {
+    T *x, *r, *r0, *p, *v, *s, *t;
+};
+
+template <class T, int G>
+void launch_iteration(Engine& E, const Csr<T>& A, const Vecs<T>& V) {
+    k_bcg_p<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.p, V.v, E.S);
+    k_bcg_v<T, G><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
+    k_bcg_s<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.v, V.s, E.S, E.P);
+    k_bcg_t<T, G><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
+    k_bcg_x<T><<<RGRID, RB, 0, E.s>>>(A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P);
+}
+
+template <class T>
+void iteration(Engine& E, const Csr<T>& A, const Vecs<T>& V) {
+    note_launches(5);
+    switch (E.group) {
+        case 4: launch_iteration<T, 4>(E, A, V); break;
+        case 8: launch_iteration<T, 8>(E, A, V); break;
+        case 16: launch_iteration<T, 16>(E, A, V); break;
+        default: launch_iteration<T, 32>(E, A, V); break;
+    }
+}
+
+template <class T>
+void init(Engine& E, const Csr<T>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
+    switch (E.group) {
+        case 4: k_bcg_init<T, 4><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
+        case 8: k_bcg_init<T, 8><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
+        case 16: k_bcg_init<T, 16><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
+        default: k_bcg_init<T, 32><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
+    }
+    LSMPS_CHECK_LAUNCH();
+}
+
+void residual64(Engine& E, const Csr<double>& A, const double* b, const double* x, double* r, double* out2) {
+    unsigned int* counter = &E.S->counter[5];
+    switch (E.group) {
+        case 4: k_residual64<4><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
+        case 8: k_residual64<8><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
+        case 16: k_residual64<16><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
+        default: k_residual64<32><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
+    }
+    LSMPS_CHECK_LAUNCH();
+}
+
+// Lanes per row from the mean row length (the tuning table picks among these).
+int pick_group(long long n, long long nnz) {
+    double mean = n ? (double)nnz / (double)n : 0;
+    if (mean <= 6) return 4;
+    if (mean <= 12) return 8;
+    if (mean <= 24) return 16;
+    return 32;
+}
+
+// Runs the iteration until done, as a CUDA graph of `chunk` iterations when requested.
+// Returns the final scalars.
+template <class T>
+BcgScalars run_loop(Engine& E, const Csr<T>& A, const Vecs<T>& V, int chunk, bool use_graph) {
+    BcgScalars h{};
+    cudaGraphExec_t exec = nullptr;
+    if (use_graph) {
+        cudaGraph_t graph;
+        LSMPS_CUDA(cudaStreamBeginCapture(E.s, cudaStreamCaptureModeThreadLocal));
+        for (int c = 0; c < chunk; ++c) iteration<T>(E, A, V);
+        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        cudaError_t e = cudaStreamEndCapture(E.s, &graph);
+        LSMPS_CUDA(e);
+        LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        cudaGraphDestroy(graph);
+    }
+    LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, E.s));
+    LSMPS_CUDA(cudaStreamSynchronize(E.s));
+    // the iteration cap bounds the loop; two extra chunks cover the final no-op kernels
+    const long long max_chunks = (h.max_iter + chunk - 1) / chunk + 2;
+    for (long long c = 0; c < max_chunks && !h.done; ++c) {
+        if (use_graph) {
+            LSMPS_CUDA(cudaGraphLaunch(exec, E.s));
+            note_launches(5 * (uint64_t)chunk);
+        } else {
+            for (int k = 0; k < chunk; ++k) iteration<T>(E, A, V);
+            LSMPS_CHECK_LAUNCH();
+        }
+        LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, E.s));
+        LSMPS_CUDA(cudaStreamSynchronize(E.s));
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    return h;
+}
+
+void set_scalar_caps(Engine& E, int max_iter, int stall_window) {
+    BcgScalars init{};
+    init.max_iter = max_iter;
+    init.stall_window = stall_window;
+    LSMPS_CUDA(cudaMemcpyAsync(E.S, &init, sizeof(init), cudaMemcpyHostToDevice, E.s));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+static void solve_exact(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps) {
+    cudaStream_t s = ctx->stream;
+    long long U = ctx->U;
+    double* x = ctx->vx.ensure<double>(U + 1);
+    double* r = ctx->vr.ensure<double>(U + 1);
+    double* r0 = ctx->vr0.ensure<double>(U + 1);
+    double* p = ctx->vp.ensure<double>(U + 1);
+    double* v = ctx->vv.ensure<double>(U + 1);
+    double* sv = ctx->vs.ensure<double>(U + 1);
+    double* t = ctx->vt.ensure<double>(U + 1);
+    double* prod = ctx->vph.ensure<double>(U + 1);
+    ExactState* st = reinterpret_cast<ExactState*>(ctx->red.ensure<double>(64));
+    const double* b = ctx->A_b.get<double>();
+    const int* uref = ctx->u_of_ref.get<int>();
+    const int* row = ctx->A_row.get<int>();
+    const int* col = ctx->A_col.get<int>();
+    const double* val = ctx->A_val.get<double>();
+    LSMPS_CUDA(cudaMemsetAsync(st, 0, sizeof(ExactState), s));
+    LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
+    LSMPS_CUDA(cudaMemsetAsync(p, 0, U * sizeof(double), s));
+    LSMPS_CUDA(cudaMemsetAsync(v, 0, U * sizeof(double), s));
+    LSMPS_CUDA(cudaMemcpyAsync(r, b, U * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    LSMPS_CUDA(cudaMemcpyAsync(r0, b, U * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const unsigned G = 148 * 4, B = 256;
+    const int max_iter = o->max_iter;
+    const double tol = o->tol;
+    auto dot = [&](const double* a, const double* c, int op) {
+        k_x_prod<<<G, B, 0, s>>>(a, c, uref, U, prod, st);
+        k_x_tail<<<1, 32, 0, s>>>(prod, U, st, op, tol, max_iter);
+    };
+    ev_record(ctx, 10);
+    if (U > 0) {
+        dot(b, b, OP_BNORM);
+        const int check = std::max(1, o->check_every > 0 ? o->check_every : 16);
+        for (int it = 0; it < max_iter; ++it) {
+            dot(r0, r, OP_RHO);
+            k_x_vec<<<G, B, 0, s>>>(U, 0, x, r, p, v, sv, t, st);
+            k_x_spmv<<<G, B, 0, s>>>(U, row, col, val, p, v, st, 1);
+            dot(r0, v, OP_DEN);
+            k_x_vec<<<G, B, 0, s>>>(U, 1, x, r, p, v, sv, t, st);
+            dot(sv, sv, OP_SN);
+            k_x_vec<<<G, B, 0, s>>>(U, 2, x, r, p, v, sv, t, st);
+            k_x_finish_sconv<<<1, 1, 0, s>>>(st);
+            k_x_spmv<<<G, B, 0, s>>>(U, row, col, val, sv, t, st, 1);
+            dot(t, t, OP_TT);
+            dot(t, sv, OP_TS);
+            k_x_vec<<<G, B, 0, s>>>(U, 3, x, r, p, v, sv, t, st);
+            dot(r, r, OP_RN);
+            LSMPS_CHECK_LAUNCH();
+            note_launches(18);
+            if ((it + 1) % check == 0) {
+                int done = 0;
+                LSMPS_CUDA(cudaMemcpyAsync(&done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+                LSMPS_CUDA(cudaStreamSynchronize(s));
+                if (done) break;
+            }
+        }
+    }
+    ev_record(ctx, 11);
+    ExactState h{};
+    LSMPS_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s));
+    double fin[3] = {0, 0, 0};
+    if (U > 0) {
+        k_x_spmv<<<G, B, 0, s>>>(U, row, col, val, x, t, st, 0);
+        double* out = reinterpret_cast<double*>(st + 1);
+        k_x_final<<<1, 32, 0, s>>>(t, b, x, ctx->A_xexact.get<double>(), uref, U, out);
+        LSMPS_CHECK_LAUNCH();
+        LSMPS_CUDA(cudaMemcpyAsync(fin, out, sizeof(fin), cudaMemcpyDeviceToHost, s));
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ps->iterations = h.iters;
+    ps->converged = h.converged;
+    ps->initial_residual = h.bnorm;
+    ps->final_residual = fin[0];
+    ps->relative_l2_error = fin[1];
+    ps->max_error = fin[2];
+    ps->relative_residual = fin[0] / std::max(h.bnorm, 1e-300);
+    ps->solve_ms = ev_elapsed(ctx, 10, 11);
+}
+
+// Fast FP64 / Jacobi: BiCGStab on A (or A D^-1) in FP64.
+static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool jacobi) {
+    cudaStream_t s = ctx->stream;
+    long long U = ctx->U, nnz = ctx->nnz;
+    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
+    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
+    E.P = Partials{red, red + RGRID};
+    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+    Vecs<double> V{ctx->vx.ensure<double>(U + 1), ctx->vr.ensure<double>(U + 1), ctx->vr0.ensure<double>(U + 1),
+                   ctx->vp.ensure<double>(U + 1), ctx->vv.ensure<double>(U + 1), ctx->vs.ensure<double>(U + 1),
+                   ctx->vt.ensure<double>(U + 1)};
+    const double* dinv = ctx->A_dinv.get<double>();
+    Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
+    Csr<double> Aop = A;
+    if (jacobi) {
+        double* sc = ctx->A_cnt.ensure<double>(nnz + 1);  // reused as the scaled FP64 values
+        k_scale_cols<double><<<1184, 256, 0, s>>>(nnz, A.col, A.val, dinv, sc);
+        LSMPS_CHECK_LAUNCH();
+        Aop.val = sc;
+    }
+    bool warm = o->warm_start && ctx->have_solution;
+    ev_record(ctx, 10);
+    set_scalar_caps(E, o->max_iter, 0);
+    if (warm && jacobi) {  // the iteration works on y = D x
+        k_scale_by_diag<<<1184, 256, 0, s>>>(U, V.x, dinv);
+    } else if (!warm) {
+        LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
+    }
+    init<double>(E, Aop, ctx->A_b.get<double>(), V, warm, o->tol, -1.0);
+    int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
+    BcgScalars h = run_loop<double>(E, Aop, V, chunk, o->use_graph != 0);
+    if (jacobi) {
+        k_unscale<<<1184, 256, 0, s>>>(U, V.x, dinv);
+        LSMPS_CHECK_LAUNCH();
+    }
+    ev_record(ctx, 11);
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ps->iterations = h.iters;
+    ps->converged = h.done == 1;
+    ps->solve_ms = ev_elapsed(ctx, 10, 11);
+    if (h.nonfinite) ps->converged = 0;
+}
+
+// Mixed precision (and learned): FP64 refinement around FP32 inner solves.
+static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
+    cudaStream_t s = ctx->stream;
+    long long U = ctx->U, nnz = ctx->nnz;
+    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
+    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
+    E.P = Partials{red, red + RGRID};
+    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+    double* scal = red + 2 * RGRID + 128;  // [0] |r|^2, [1] |b|^2
+    const double* dinv = ctx->A_dinv.get<double>();
+    Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
+    float* valf = ctx->A_valf.ensure<float>(nnz + 1);
+    k_scale_cols<float><<<1184, 256, 0, s>>>(nnz, A.col, A.val, dinv, valf);
+    LSMPS_CHECK_LAUNCH();
+    Csr<float> Af{U, A.row, A.col, valf};
+    double* x = ctx->vx.ensure<double>(U + 1);
+    double* r = ctx->vr.ensure<double>(U + 1);
+    float* rhs = ctx->fph.ensure<float>(U + 1);
+    Vecs<float> V{ctx->fx.ensure<float>(U + 1), ctx->fr.ensure<float>(U + 1), ctx->fr0.ensure<float>(U + 1),
+                  ctx->fp.ensure<float>(U + 1), ctx->fv.ensure<float>(U + 1), ctx->fs.ensure<float>(U + 1),
+                  ctx->ft.ensure<float>(U + 1)};
+    const bool use_nn = learned && mpnn_ready(ctx);
+    bool warm = o->warm_start && ctx->have_solution;
+    const double inner_tol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
+    const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : 200;
+    const int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
+    const int stall = o->stall_window > 0 ? o->stall_window : 20;
+    ev_record(ctx, 10);
+    set_scalar_caps(E, 0, 0);  // zero the reduction tickets before the first residual
+    if (!warm) LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
+    int total_inner = 0, outer = 0, fallback = 0;
+    bool converged = false;
+    double bnorm = 0, rnorm = 0;
+    const int max_outer = 200;
+    for (; outer < max_outer; ++outer) {
+        residual64(E, A, ctx->A_b.get<double>(), x, r, scal);
+        double h2[2];
+        LSMPS_CUDA(cudaMemcpyAsync(h2, scal, sizeof(h2), cudaMemcpyDeviceToHost, s));
+        LSMPS_CUDA(cudaStreamSynchronize(s));
+        rnorm = std::sqrt(h2[0]);
+        bnorm = std::sqrt(h2[1]);
+        if (!std::isfinite(rnorm)) break;
+        if (rnorm <= o->tol * std::max(1.0, bnorm)) { converged = true; break; }
+        if (total_inner >= o->max_iter) break;
+        k_scale_rhs<<<1184, 256, 0, s>>>(U, r, scal, rhs, V.x);
+        LSMPS_CHECK_LAUNCH();
+        bool nn_now = use_nn && !fallback;
+        if (nn_now) mpnn_warm_start(ctx, rhs, V.x);
+        set_scalar_caps(E, std::min(inner_max, o->max_iter - total_inner), nn_now ? stall : 0);
+        // relative inner tolerance on the unit-norm right-hand side
+        init<float>(E, Af, rhs, V, nn_now, inner_tol, 1.0);
+        BcgScalars h = run_loop<float>(E, Af, V, chunk, o->use_graph != 0);
+        total_inner += h.iters;
+        if (h.done == 4 && nn_now) fallback = 1;  // stalled: continue with plain Jacobi sweeps
+        k_apply_correction<<<1184, 256, 0, s>>>(U, x, V.x, dinv, scal);
+        LSMPS_CHECK_LAUNCH();
+        if (h.iters == 0 && h.done != 1) { fallback = fallback || nn_now; if (!nn_now) break; }
+    }
+    ev_record(ctx, 11);
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ps->iterations = total_inner;
+    ps->outer_iterations = outer;
+    ps->converged = converged;
+    ps->fallback = fallback;
+    ps->solve_ms = ev_elapsed(ctx, 10, 11);
+}
+
+void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out) {
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "PPE solve needs lsmps_ppe_assemble first");
+    LSMPS_REQUIRE(o && o->solver >= 0 && o->solver <= 4, LSMPS_ERR_ARG, "unknown solver");
+    LSMPS_REQUIRE(o->solver != LSMPS_SOLVER_LEARNED || mpnn_ready(ctx), LSMPS_ERR_STATE,
+                  "learned solver needs lsmps_mpnn_init / lsmps_mpnn_load first");
+    lsmps_ppe_stats ps = ctx->ppe_assembly;
+    ps.iterations = 0;
+    ps.converged = 0;
+    long long U = ctx->U;
+    if (U == 0) {  // src/lsmps.cpp:67: if(!n) return st;
+        if (out) *out = ps;
+        return;
+    }
+    if (o->solver == LSMPS_SOLVER_REFERENCE) {
+        solve_exact(ctx, o, &ps);
+    } else {
+        if (o->solver == LSMPS_SOLVER_FP64) solve_fast64(ctx, o, &ps, false);
+        else if (o->solver == LSMPS_SOLVER_JACOBI) solve_fast64(ctx, o, &ps, true);
+        else solve_mixed(ctx, o, &ps, o->solver == LSMPS_SOLVER_LEARNED);
+        // final statistics in FP64: |Ax - b|, |b|, error against p*
+        cudaStream_t s = ctx->stream;
+        Engine E{ctx, s, nullptr, {}, pick_group(U, ctx->nnz)};
+        double* red = ctx->red.ensure<double>(2 * RGRID + 256);
+        E.P = Partials{red, red + RGRID};
+        E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+        double* scal = red + 2 * RGRID + 128;
+        Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
+        double* x = ctx->vx.get<double>();
+        double* tmp = ctx->vt.ensure<double>(U + 1);
+        residual64(E, A, ctx->A_b.get<double>(), x, tmp, scal);
+        auto* maxbits = reinterpret_cast<unsigned long long*>(scal + 4);
+        LSMPS_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), s));
+        k_error_stats<<<RGRID, RB, 0, s>>>(U, x, ctx->A_xexact.get<double>(), scal + 2, E.P, &E.S->counter[6],
+                                            maxbits);
+        LSMPS_CHECK_LAUNCH();
+        double h[5];
+        LSMPS_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+        LSMPS_CUDA(cudaStreamSynchronize(s));
+        ps.initial_residual = std::sqrt(h[1]);
+        ps.final_residual = std::sqrt(h[0]);
+        ps.relative_residual = ps.final_residual / std::max(ps.initial_residual, 1e-300);
+        ps.relative_l2_error = std::sqrt(h[2] / std::max(h[3], 1e-30));
+        unsigned long long mb;
+        std::memcpy(&mb, &h[4], sizeof(mb));
+        double mx;
+        std::memcpy(&mx, &mb, sizeof(mx));
+        ps.max_error = mx;
+        if (!std::isfinite(ps.final_residual)) ps.converged = 0;
+    }
+    ctx->have_solution = true;
+    ctx->timings[5] = ps.solve_ms;
+    if (out) *out = ps;
+}
+
+void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes) {
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "SpMV bench needs an assembled PPE");
+    cudaStream_t s = ctx->stream;
+    long long U = ctx->U, nnz = ctx->nnz;
+    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
+    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
+    E.P = Partials{red, red + RGRID};
+    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+    set_scalar_caps(E, 1 << 30, 0);
+    BcgScalars init{};
+    init.max_iter = 1 << 30;
+    init.rho = 1.0;
+    LSMPS_CUDA(cudaMemcpyAsync(E.S, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const bool f32 = kernel == LSMPS_KB_SPMV32;
+    if (f32) {
+        float* valf = ctx->A_valf.ensure<float>(nnz + 1);
+        k_scale_cols<float><<<1184, 256, 0, s>>>(nnz, ctx->A_col.get<int>(), ctx->A_val.get<double>(),
+                                                 ctx->A_dinv.get<double>(), valf);
+        LSMPS_CHECK_LAUNCH();
+        float* x = ctx->fp.ensure<float>(U + 1);
+        float* r0 = ctx->fr0.ensure<float>(U + 1);
+        ctx->fv.ensure<float>(U + 1);
+        LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(float), s));
+        LSMPS_CUDA(cudaMemsetAsync(r0, 0, U * sizeof(float), s));
+    } else {
+        double* x = ctx->vp.ensure<double>(U + 1);
+        double* r0 = ctx->vr0.ensure<double>(U + 1);
+        ctx->vv.ensure<double>(U + 1);
+        LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
+        LSMPS_CUDA(cudaMemsetAsync(r0, 0, U * sizeof(double), s));
+    }
+    auto launch = [&] {
+        if (f32) {
+            Csr<float> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_valf.get<float>()};
+            switch (E.group) {
+                case 4: k_bcg_v<float, 4><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
+                case 8: k_bcg_v<float, 8><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
+                case 16: k_bcg_v<float, 16><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
+                default: k_bcg_v<float, 32><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
+            }
+        } else {
+            Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
+            switch (E.group) {
+                case 4: k_bcg_v<double, 4><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
+                case 8: k_bcg_v<double, 8><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
+                case 16: k_bcg_v<double, 16><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
+                default: k_bcg_v<double, 32><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
+            }
+        }
+        LSMPS_CHECK_LAUNCH();
+    };
+    launch();
+    ev_record(ctx, 14);
+    for (int r = 0; r < reps; ++r) launch();
+    ev_record(ctx, 15);
+    *ms = ev_elapsed(ctx, 14, 15) / reps;
+    *bytes = f32 ? 8.0 * nnz + 16.0 * U + 4.0 : 12.0 * nnz + 28.0 * U + 4.0;
+    // the bench overwrote solver vectors: a warm start from them is no longer valid
+    ctx->have_solution = false;
+}
+
+__global__ void k_to_ref(const double* __restrict__ x, const int* __restrict__ u_of_ref, long long U,
+                         double* __restrict__ out) {
+    long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (rr < U) out[rr] = x[u_of_ref[rr]];
+}
+
+void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
+    LSMPS_REQUIRE(ctx->have_solution, LSMPS_ERR_STATE, "no PPE solution");
+    LSMPS_REQUIRE((long long)u == ctx->U, LSMPS_ERR_ARG, "pressure buffer size differs from the unknown count");
+    if (!u) return;
+    double* tmp = ctx->vtmp.ensure<double>(u + 1);
+    k_to_ref<<<blocks_for(u, 256), 256, 0, ctx->stream>>>(ctx->vx.get<double>(), ctx->u_of_ref.get<int>(),
+                                                          (long long)u, tmp);
+    LSMPS_CHECK_LAUNCH();
+    LSMPS_CUDA(cudaMemcpyAsync(p, tmp, u * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace lsmps_gpu

@@ -1,0 +1,34 @@
+// BiCGStab engine shared by the FP64, Jacobi, mixed-precision and learned solvers.
+#pragma once
+#include "ctx.cuh"
+
+namespace lsmps_gpu {
+
+// Scalars of one BiCGStab run, resident in device memory and updated by the last block of
+// each reduction kernel, so the iteration runs without host round trips.
+struct BcgScalars {
+    double rho, rho0, alpha, omega, beta;
+    double thresh;        // converged when |s| or |r| <= thresh
+    double sn, rn;        // last |s| and |r|
+    double tt;
+    double best_rn;       // smallest |r| seen (stall detection)
+    int done;             // 0 running, 1 converged, 2 breakdown, 3 iteration cap, 4 stalled
+    int s_conv;           // |s| test passed this iteration
+    int iters;            // completed iterations (reference bookkeeping)
+    int it;               // iteration counter
+    int max_iter;
+    int stall_window, since_best;
+    int nonfinite;
+    unsigned int counter[8];  // last-block tickets of the reduction kernels
+};
+
+// A CSR matrix view in the solver's numbering.
+template <class T>
+struct Csr {
+    long long n;
+    const int* row;
+    const int* col;
+    const T* val;
+};
+
+}  // namespace lsmps_gpu

@@ -1,0 +1,323 @@
+"""ctypes binding of the LS-MPS sm_100a library (include/lsmps_gpu.h).
+
+This is the Python face of the C ABI, used by the tests and bench.py; the struct layouts
+below mirror the header field for field. The library is loaded from ``lib/`` next to this
+file (built by ``make`` in this directory); there is no fallback of any kind: if the
+shared library is missing, importing ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "liblsmps_b200.so")
+CLI_PATH = os.path.join(HERE, "bin", "lsmps-bench")
+
+OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_GRID, ERR_OVERFLOW, ERR_NONFINITE, ERR_TIMEOUT, ERR_IO = range(10)
+INTERIOR, FREE_SURFACE, SPLASH, NEAR_WALL, WALL = range(5)
+NBR_CLASSIFY = 1
+PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
+SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED = range(5)
+KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS = range(5)
+SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4}
+VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}
+
+REF_QUADRATIC = np.array([1, 2, -3, 0.5, 0.7, -0.2, 0.4, 0.3, -0.1, 0.25], dtype=np.float64)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the library and CLI for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+class NeighborStats(C.Structure):
+    _fields_ = [("pairs", C.c_uint64), ("truncated", C.c_uint64), ("mean", C.c_double),
+                ("p50", C.c_int32), ("p90", C.c_int32), ("p99", C.c_int32), ("max_count", C.c_int32),
+                ("type_count", C.c_uint64 * 5), ("grid_cells", C.c_int64),
+                ("max_cell_occupancy", C.c_int32), ("reserved", C.c_int32)]
+
+
+class WlsOpts(C.Structure):
+    _fields_ = [("re", C.c_double), ("l0", C.c_double), ("regularization", C.c_double),
+                ("mode", C.c_int32), ("wls_samples", C.c_int32), ("nrhs", C.c_int32),
+                ("precision", C.c_int32), ("quad_coef", C.POINTER(C.c_double)),
+                ("store_solutions", C.c_int32), ("reserved", C.c_int32)]
+
+
+class WlsStats(C.Structure):
+    _fields_ = [("sampled", C.c_uint64), ("ok", C.c_uint64), ("regularized", C.c_uint64),
+                ("failed", C.c_uint64), ("virtual_points", C.c_uint64),
+                ("max_gradient_error", C.c_double), ("rms_gradient_error", C.c_double),
+                ("max_laplacian_error", C.c_double), ("rms_laplacian_error", C.c_double),
+                ("skipped", C.c_uint64), ("fp64_fallback", C.c_uint64)]
+
+
+class PpeOpts(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("reserved", C.c_int32), ("max_unknowns", C.c_int64),
+                ("re", C.c_double), ("l0", C.c_double), ("diag_shift", C.c_double)]
+
+
+class PpeStats(C.Structure):
+    _fields_ = [("unknowns", C.c_uint64), ("nnz", C.c_uint64), ("dirichlet", C.c_uint64),
+                ("neumann", C.c_uint64), ("failed_rows", C.c_uint64), ("iterations", C.c_int32),
+                ("converged", C.c_int32), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double), ("relative_l2_error", C.c_double),
+                ("max_error", C.c_double), ("assembly_ms", C.c_double), ("solve_ms", C.c_double),
+                ("outer_iterations", C.c_int32), ("fallback", C.c_int32),
+                ("relative_residual", C.c_double)]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("max_iter", C.c_int32), ("tol", C.c_double),
+                ("warm_start", C.c_int32), ("use_graph", C.c_int32), ("inner_tol", C.c_double),
+                ("inner_max_iter", C.c_int32), ("stall_window", C.c_int32), ("check_every", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class MpnnTrainOpts(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("weight_decay", C.c_float), ("seed", C.c_uint32), ("reserved", C.c_int32)]
+
+
+# Every function the header declares, with its ctypes signature.
+_vp = C.c_void_p
+SIGNATURES = {
+    "lsmps_ctx_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "lsmps_ctx_destroy": (None, [_vp]),
+    "lsmps_last_error": (C.c_char_p, [_vp]),
+    "lsmps_abi_version": (C.c_int, []),
+    "lsmps_get_timings": (C.c_int, [_vp, C.POINTER(C.c_double * 8)]),
+    "lsmps_sync": (C.c_int, [_vp]),
+    "lsmps_stream": (C.c_void_p, [_vp]),
+    "lsmps_launch_count": (C.c_uint64, []),
+    "lsmps_kernel_bench": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "lsmps_upload_particles": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "lsmps_upload_particles_device": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "lsmps_build_neighbors": (C.c_int, [_vp, C.c_double, C.c_int, C.c_double, C.c_int,
+                                        C.POINTER(NeighborStats)]),
+    "lsmps_classify": (C.c_int, [_vp, C.c_double, C.POINTER(NeighborStats)]),
+    "lsmps_wls": (C.c_int, [_vp, C.POINTER(WlsOpts), C.POINTER(WlsStats)]),
+    "lsmps_ppe_assemble": (C.c_int, [_vp, C.POINTER(PpeOpts), C.POINTER(PpeStats)]),
+    "lsmps_ppe_solve": (C.c_int, [_vp, C.POINTER(SolverOpts), C.POINTER(PpeStats)]),
+    "lsmps_download_types": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_download_neighbors": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "lsmps_download_wls": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "lsmps_download_ppe": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_mpnn_init": (C.c_int, [_vp, C.c_uint32]),
+    "lsmps_mpnn_add_sample": (C.c_int, [_vp]),
+    "lsmps_mpnn_train": (C.c_int, [_vp, C.POINTER(MpnnTrainOpts), C.POINTER(C.c_float)]),
+    "lsmps_mpnn_save": (C.c_int, [_vp, C.c_char_p]),
+    "lsmps_mpnn_load": (C.c_int, [_vp, C.c_char_p]),
+    "lsmps_host_generate": (C.c_int, [C.c_char_p, C.c_char_p, _vp, _vp, _vp, C.POINTER(C.c_size_t)]),
+}
+
+_LIB = None
+
+
+def load():
+    """Load lib/liblsmps_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run make in {HERE} (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class LsmpsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+def generate(cfg_path: str | None = None, **overrides):
+    """Particles of a .cfg case through the library's generate_case (host code, no GPU)."""
+    L = load()
+    ov = ";".join(f"{k}={v}" for k, v in overrides.items()).encode()
+    n = C.c_size_t(0)
+    cp = cfg_path.encode() if cfg_path else None
+    rc = L.lsmps_host_generate(cp, ov, None, None, None, C.byref(n))
+    if rc != OK:
+        raise LsmpsError(rc, "generate failed")
+    xyz = np.zeros((n.value, 3)); t = np.zeros(n.value, np.uint8); u = np.zeros((n.value, 3))
+    rc = L.lsmps_host_generate(cp, ov, _p(xyz), _p(t), _p(u), C.byref(n))
+    if rc != OK:
+        raise LsmpsError(rc, "generate failed")
+    return xyz, t, u
+
+
+class Context:
+    """One lsmps_ctx: device buffers and stream of one particle set on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.lsmps_ctx_create(device, C.byref(h))
+        if rc != OK:
+            raise LsmpsError(rc, f"cannot create a context on device {device}")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lsmps_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != OK:
+            raise LsmpsError(rc, self.L.lsmps_last_error(self.h).decode())
+
+    def timings(self):
+        t = (C.c_double * 8)()
+        self._check(self.L.lsmps_get_timings(self.h, C.byref(t)))
+        return list(t)
+
+    def sync(self):
+        self._check(self.L.lsmps_sync(self.h))
+
+    def stream(self):
+        return self.L.lsmps_stream(self.h)
+
+    def kernel_bench(self, kernel, reps=20):
+        ms, nb = C.c_double(), C.c_double()
+        self._check(self.L.lsmps_kernel_bench(self.h, kernel, reps, C.byref(ms), C.byref(nb)))
+        return ms.value, nb.value
+
+    def upload(self, xyz, types):
+        self._xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self._types = np.ascontiguousarray(types, dtype=np.uint8)
+        self.n = len(self._types)
+        self._check(self.L.lsmps_upload_particles(self.h, _p(self._xyz), _p(self._types), self.n))
+
+    def build_neighbors(self, re, max_neighbors, l0, classify=True):
+        st = NeighborStats()
+        self._check(self.L.lsmps_build_neighbors(self.h, re, max_neighbors, l0,
+                                                 NBR_CLASSIFY if classify else 0, C.byref(st)))
+        return st
+
+    def classify(self, l0):
+        st = NeighborStats()
+        self._check(self.L.lsmps_classify(self.h, l0, C.byref(st)))
+        return st
+
+    def wls(self, re, l0, mode=1, wls_samples=4096, coef=None, precision=0, store=False, reg=1e-8):
+        coef = REF_QUADRATIC[None, :] if coef is None else np.atleast_2d(coef)
+        self._coef = np.ascontiguousarray(coef, dtype=np.float64)
+        o = WlsOpts(re=re, l0=l0, regularization=reg, mode=mode, wls_samples=wls_samples,
+                    nrhs=self._coef.shape[0], precision=precision,
+                    quad_coef=self._coef.ctypes.data_as(C.POINTER(C.c_double)),
+                    store_solutions=1 if store else 0)
+        st = WlsStats()
+        self._check(self.L.lsmps_wls(self.h, C.byref(o), C.byref(st)))
+        return st
+
+    def ppe_assemble(self, variant, max_unknowns, re, l0, diag_shift=1e-3):
+        o = PpeOpts(variant=VARIANTS.get(variant, variant), max_unknowns=int(max_unknowns), re=re,
+                    l0=l0, diag_shift=diag_shift)
+        st = PpeStats()
+        self._check(self.L.lsmps_ppe_assemble(self.h, C.byref(o), C.byref(st)))
+        self._last_ppe = st
+        return st
+
+    def ppe_solve(self, solver, max_iter, tol, warm_start=False, use_graph=True, inner_tol=0.0,
+                  inner_max_iter=0, stall_window=0, check_every=0):
+        o = SolverOpts(solver=SOLVERS.get(solver, solver), max_iter=int(max_iter), tol=tol,
+                       warm_start=1 if warm_start else 0, use_graph=1 if use_graph else 0,
+                       inner_tol=inner_tol, inner_max_iter=inner_max_iter, stall_window=stall_window,
+                       check_every=check_every)
+        st = PpeStats()
+        self._check(self.L.lsmps_ppe_solve(self.h, C.byref(o), C.byref(st)))
+        return st
+
+    def types(self):
+        t = np.zeros(self.n, np.uint8)
+        self._check(self.L.lsmps_download_types(self.h, _p(t), self.n))
+        return t
+
+    def neighbors(self, pairs):
+        row = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(max(int(pairs), 1), np.int32)
+        self._check(self.L.lsmps_download_neighbors(self.h, _p(row), _p(col), int(pairs)))
+        return row, col[: int(pairs)]
+
+    def wls_result(self, nrhs=1, with_x=False):
+        x = np.zeros((self.n, nrhs, 9)) if with_x else None
+        st = np.zeros(self.n, np.int32); z = np.zeros((self.n, 9)); ws = np.zeros(self.n)
+        self._check(self.L.lsmps_download_wls(self.h, _p(x), _p(st), _p(z), _p(ws)))
+        return x, st, z, ws
+
+    def ppe(self, unknowns, nnz):
+        row = np.zeros(unknowns + 1, np.int32); col = np.zeros(max(nnz, 1), np.int32)
+        val = np.zeros(max(nnz, 1)); b = np.zeros(unknowns); xe = np.zeros(unknowns)
+        part = np.zeros(unknowns, np.int32)
+        self._check(self.L.lsmps_download_ppe(self.h, _p(row), _p(col), _p(val), _p(b), _p(xe), _p(part)))
+        return row, col[:nnz], val[:nnz], b, xe, part
+
+    def pressure(self, unknowns):
+        p = np.zeros(unknowns)
+        self._check(self.L.lsmps_download_pressure(self.h, _p(p), unknowns))
+        return p
+
+    def pressure_into(self, out):
+        """Download the solution into a caller buffer (e.g. pinned host memory)."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        self._check(self.L.lsmps_download_pressure(self.h, _p(out), len(out)))
+        return out
+
+    def ppe_reference_numbering(self):
+        """The assembled system in the reference's numbering (row, col, val, b, p*, particle)."""
+        st = PpeStats()
+        o = self._last_ppe
+        return self.ppe(o.unknowns, o.nnz)
+
+    def mpnn_init(self, seed=0):
+        self._check(self.L.lsmps_mpnn_init(self.h, seed))
+
+    def mpnn_add_sample(self):
+        self._check(self.L.lsmps_mpnn_add_sample(self.h))
+
+    def mpnn_train(self, steps, batch=4, lr=1e-3, weight_decay=0.0, seed=0):
+        o = MpnnTrainOpts(steps=steps, batch=batch, lr=lr, weight_decay=weight_decay, seed=seed)
+        loss = C.c_float()
+        self._check(self.L.lsmps_mpnn_train(self.h, C.byref(o), C.byref(loss)))
+        return loss.value
+
+    def mpnn_save(self, path):
+        self._check(self.L.lsmps_mpnn_save(self.h, path.encode()))
+
+    def mpnn_load(self, path):
+        self._check(self.L.lsmps_mpnn_load(self.h, path.encode()))
+
+
+def struct_dict(s):
+    out = {}
+    for name, _ in s._fields_:
+        v = getattr(s, name)
+        if hasattr(v, "__len__") and not isinstance(v, (bytes, str)):
+            v = list(v)
+        out[name] = v
+    return out

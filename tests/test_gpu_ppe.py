@@ -1,0 +1,91 @@
+"""GPU PPE assembly: the reference variant bit for bit; shifted and WLS variants against
+the oracle (values within 1e-12 relative)."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import lsmps_b200 as lib
+from _util import cfg_params, jittered_lattice, sha
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+CASES = ["smoke", "bulk_uniform", "wall_film", "rain_injection", "narrow_gap"]
+
+
+@pytest.fixture(scope="module")
+def ctx(built):
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_variant_bit_exact(ctx, golden, cfg_dir, name):
+    g = golden["cases"][name]
+    p = cfg_params(g["cfg_text"])
+    xyz, t, _ = lib.generate(str(cfg_dir / f"{name}.cfg"))
+    ctx.upload(xyz, t)
+    ctx.build_neighbors(p["re"], p["max_neighbors"], p["l0"])
+    st = ctx.ppe_assemble("reference", p["ppe_max_unknowns"], p["re"], p["l0"])
+    for k in ("unknowns", "nnz", "dirichlet", "neumann", "failed_rows"):
+        assert getattr(st, k) == g["ppe"][k], k
+    row, col, val, b, xe, part = ctx.ppe(st.unknowns, st.nnz)
+    assert sha(row, col, val) == g["ppe"]["csr_sha256"]
+    assert sha(b) == g["ppe"]["b_sha256"]
+    assert sha(xe) == g["ppe"]["x_exact_sha256"]
+
+
+def _csr(row, col, val, n):
+    return sp.csr_matrix((val, col, row), shape=(n, n))
+
+
+@pytest.mark.parametrize("variant", ["shifted", "wls"])
+@pytest.mark.parametrize("case", ["lattice", "rain_plate"])
+def test_variants_match_oracle(ctx, variant, case):
+    if case == "lattice":
+        xyz = jittered_lattice(18, 0.1, seed=7)
+        t = np.zeros(len(xyz), np.uint8)
+    else:
+        xyz, t, _ = lib.generate(None, case="rain_plate", particles=40_000, l0=1.0, seed=9)
+    ctx.upload(xyz, t)
+    ctx.build_neighbors(2.1, 128, 1.0)
+    types = ctx.types()
+    row, col, _ = Oracle.neighbors(xyz, 2.1, 128)
+    z = ws = wst = None
+    if variant == "wls":
+        ctx.wls(2.1, 1.0, mode=1)
+        _, wst, z, ws = ctx.wls_result()
+        _, so, zo, wo = Oracle.wls(xyz, types, row, col, 2.1, 1.0)
+        assert np.array_equal(wst, so)
+        z, ws = zo, wo  # the oracle assembles from its own WLS vectors
+    cap = 10**9
+    st = ctx.ppe_assemble(variant, cap, 2.1, 1.0, diag_shift=1e-3)
+    prow, pcol, pval, b, xe, part = ctx.ppe(st.unknowns, st.nnz)
+    vid = lib.VARIANTS[variant]
+    orow, ocol, oval, ob, oxe, oup, ost = Oracle.ppe_assemble(vid, xyz, types, row, col, 2.1, 1.0, cap, 1e-3,
+                                                              z, ws, wst)
+    assert st.unknowns == ost["unknowns"]
+    assert np.array_equal(part, oup)
+    assert np.allclose(xe, oxe, rtol=1e-14, atol=1e-14)
+    n = st.unknowns
+    A, O = _csr(prow, pcol, pval, n), _csr(orow, ocol, oval, n)
+    diff = abs(A - O).max()
+    assert diff <= 1e-12 * abs(O).max()
+    if variant == "shifted":
+        assert np.array_equal(prow, orow) and np.array_equal(pcol, ocol)
+    else:
+        # clipping may differ only for coefficients within rounding of zero
+        assert abs(st.nnz - ost["nnz"]) <= max(2, st.nnz // 100000)
+    assert np.allclose(b, ob, rtol=1e-11, atol=1e-11 * np.abs(ob).max())
+
+
+def test_cap_and_empty(ctx):
+    xyz = jittered_lattice(10, 0.1, seed=3)
+    ctx.upload(xyz, np.zeros(len(xyz), np.uint8))
+    ctx.build_neighbors(2.1, 96, 1.0)
+    st = ctx.ppe_assemble("reference", 100, 2.1, 1.0)
+    assert st.unknowns == 100
+    st = ctx.ppe_assemble("reference", 0, 2.1, 1.0)
+    assert st.unknowns == 0 and st.nnz == 0
+    s = ctx.ppe_solve("reference", 10, 1e-7)
+    assert s.iterations == 0 and s.converged == 0
