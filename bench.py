@@ -117,9 +117,10 @@ class ClockSampler:
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
+            self.err_path = self.path + ".err"
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                                         stdout=open(self.path, "w"), stderr=open(self.err_path, "w"))
         except OSError:
             self.proc = None
 
@@ -137,8 +138,10 @@ class ClockSampler:
             if len(parts) >= 10:
                 rows.append(parts)
         os.unlink(self.path)
+        err = open(self.err_path).read().strip()[:200]
+        os.unlink(self.err_path)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples: " + err]}
 
         def num(x):
             try:

@@ -129,7 +129,8 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->vs, &ctx->vt, &ctx->vph, &ctx->vsh, &ctx->vtmp, &ctx->fx, &ctx->fr,
                                  &ctx->fr0, &ctx->fp, &ctx->fv, &ctx->fs, &ctx->ft, &ctx->fph, &ctx->fsh,
                                  &ctx->red, &ctx->mpnn_w, &ctx->mpnn_m, &ctx->mpnn_v, &ctx->mpnn_g,
-                                 &ctx->mpnn_act, &ctx->mpnn_samples};
+                                 &ctx->mpnn_act, &ctx->mpnn_samples, &ctx->S_ptr, &ctx->S_len,
+                                 &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf};
     for (auto* b : bufs) b->release();
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);

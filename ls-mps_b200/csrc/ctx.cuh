@@ -8,9 +8,12 @@
 //   neighbor CSR (sorted)      nbr_row: n + 1 x i32, nbr_col: P x i32 (sorted indices; the
 //                              reference's row order is ascending sorted index)
 //   WLS                        wls_status: n x i32, wls_z: n x 9 f64, wls_wsum: n x f64
-//   PPE (unknowns in sorted    A_row: U + 1 x i32, A_col: Z x i32, A_val: Z x f64, A_valf:
-//   order)                     Z x f32, b, x*, diag_inv: U x f64, u_of_sorted: n x i32,
-//                              sorted_of_u / ref_of_u / u_of_ref: U x i32
+//   PPE (unknowns in sorted    A_row: U + 1 x i32, A_col: Z x i32, A_val: Z x f64, b, x*,
+//   order)                     diag_inv: U x f64, u_of_sorted: n x i32, sorted_of_u /
+//                              ref_of_u / u_of_ref: U x i32
+//   SELL-32 solver copies      S_ptr / S_len: U/32 x i32, S_col: E x i32, S_val (A) and
+//                              S_vals (A D^-1): E x f64, S_valf (A D^-1): E x f32, with
+//                              E = Z + padding (each slice padded to its longest row)
 #pragma once
 #include <cuda_runtime.h>
 
@@ -61,6 +64,10 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf ref_rank, u_of_sorted, sorted_of_u, ref_of_u, u_of_ref;
     lsmps_gpu::DevBuf A_row, A_col, A_val, A_valf, A_b, A_xexact, A_dinv, A_dinvf, A_cnt;
     lsmps_ppe_stats ppe_assembly{};
+    // SELL-32 copies of A for the fast solvers (built on first use after an assembly)
+    bool have_sell = false, have_sell_s = false, have_sell_f = false;
+    long long sell_nslices = 0, sell_entries = 0;
+    lsmps_gpu::DevBuf S_ptr, S_len, S_col, S_val, S_vals, S_valf;
 
     // ---- solver state ----
     bool have_solution = false;

@@ -217,22 +217,38 @@ __device__ __forceinline__ void final_sum(Partials P, double* ra, double* rb) {
     }
 }
 
+// Row i of a SELL-32 matrix: slice s = i / 32 stores its rows' k-th entries contiguously
+// (entry k of lane l at sptr[s] + 32 k + l), padded with zeros to the slice's longest row.
+// One thread per row, one warp per slice: every matrix load is a coalesced 128-byte (FP32)
+// or 256-byte (FP64) line, and the k-loop is unrolled four ways so that each thread keeps
+// eight matrix loads and four gathers in flight. Matrix loads stream past L1/L2 (__ldcs) so
+// the vectors, which are re-read every iteration, stay in the 126 MB L2.
 template <class T>
-__device__ __forceinline__ T ldstream(const T* p) { return __ldcs(p); }
-
-// y_i = sum_e val[e] x[col[e]] for rows handled by a group of G lanes; returns the row sum
-// in every lane of the group.
-template <class T, int G>
-__device__ __forceinline__ double row_dot(const int* __restrict__ row, const int* __restrict__ col,
-                                          const T* __restrict__ val, const T* __restrict__ x, long long i,
-                                          int g) {
-    int e0 = row[i], e1 = row[i + 1];
-    double s = 0;
-    for (int e = e0 + g; e < e1; e += G) s += (double)ldstream(val + e) * (double)x[ldstream(col + e)];
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
-    return s;
+__device__ __forceinline__ double sell_row(const Sell<T>& A, long long s, int lane, const T* __restrict__ x) {
+    const T* __restrict__ val = A.val + A.sptr[s] + lane;
+    const int* __restrict__ col = A.col + A.sptr[s] + lane;
+    const int len = A.slen[s];
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    int k = 0;
+    for (; k + 4 <= len; k += 4) {
+        const T v0 = __ldcs(val + 32 * k), v1 = __ldcs(val + 32 * (k + 1)), v2 = __ldcs(val + 32 * (k + 2)),
+                v3 = __ldcs(val + 32 * (k + 3));
+        const int c0 = __ldcs(col + 32 * k), c1 = __ldcs(col + 32 * (k + 1)), c2 = __ldcs(col + 32 * (k + 2)),
+                  c3 = __ldcs(col + 32 * (k + 3));
+        a0 += (double)v0 * (double)x[c0];
+        a1 += (double)v1 * (double)x[c1];
+        a2 += (double)v2 * (double)x[c2];
+        a3 += (double)v3 * (double)x[c3];
+    }
+    for (; k < len; ++k) a0 += (double)__ldcs(val + 32 * k) * (double)x[__ldcs(col + 32 * k)];
+    return (a0 + a1) + (a2 + a3);
 }
+
+#define SELL_LOOP(A)                                                              \
+    const int lane = threadIdx.x & 31;                                            \
+    const long long w0 = (blockIdx.x * (long long)RB + threadIdx.x) >> 5;         \
+    const long long nw = ((long long)gridDim.x * RB) >> 5;                        \
+    for (long long s = w0; s < (A).nslices; s += nw)
 
 // p = r + beta (p - omega v)
 template <class T>
@@ -245,19 +261,18 @@ __global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__
 }
 
 // v = A p; den = (r0, v); alpha = rho / den
-template <class T, int G>
-__global__ void __launch_bounds__(RB) k_bcg_v(Csr<T> A, const T* __restrict__ p, T* __restrict__ v,
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_v(Sell<T> A, const T* __restrict__ p, T* __restrict__ v,
                                               const T* __restrict__ r0, BcgScalars* S, Partials P) {
     if (S->done) return;
-    const int g = threadIdx.x & (G - 1);
-    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
-    const long long ngroups = (long long)gridDim.x * RB / G;
     double acc = 0;
-    for (long long i = gid; i < A.n; i += ngroups) {
-        double y = row_dot<T, G>(A.row, A.col, A.val, p, i, g);
-        if (g == 0) {
-            v[i] = (T)y;
-            acc += (double)r0[i] * (double)(T)y;
+    SELL_LOOP(A) {
+        double y = sell_row(A, s, lane, p);
+        long long i = (s << 5) + lane;
+        if (i < A.n) {
+            T yi = (T)y;
+            v[i] = yi;
+            acc += (double)r0[i] * (double)yi;
         }
     }
     if (block_partials(acc, 0.0, P, &S->counter[0])) {
@@ -296,20 +311,18 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
 }
 
 // t = A s; omega = (t, s) / (t, t)
-template <class T, int G>
-__global__ void __launch_bounds__(RB) k_bcg_t(Csr<T> A, const T* __restrict__ s, T* __restrict__ t,
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_t(Sell<T> A, const T* __restrict__ sv, T* __restrict__ t,
                                               BcgScalars* S, Partials P) {
     if (S->done || S->s_conv) return;
-    const int g = threadIdx.x & (G - 1);
-    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
-    const long long ngroups = (long long)gridDim.x * RB / G;
     double ats = 0, att = 0;
-    for (long long i = gid; i < A.n; i += ngroups) {
-        double y = row_dot<T, G>(A.row, A.col, A.val, s, i, g);
-        if (g == 0) {
+    SELL_LOOP(A) {
+        double y = sell_row(A, s, lane, sv);
+        long long i = (s << 5) + lane;
+        if (i < A.n) {
             T ti = (T)y;
             t[i] = ti;
-            ats += (double)ti * (double)s[i];
+            ats += (double)ti * (double)sv[i];
             att += (double)ti * (double)ti;
         }
     }
@@ -382,18 +395,16 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
 }
 
 // Initialisation: r = b - A x (or r = b when x = 0), r0 = r, p = v = 0, |b|, rho = (r0, r).
-template <class T, int G>
-__global__ void __launch_bounds__(RB) k_bcg_init(Csr<T> A, const T* __restrict__ b, const T* __restrict__ x,
+template <class T>
+__global__ void __launch_bounds__(RB) k_bcg_init(Sell<T> A, const T* __restrict__ b, const T* __restrict__ x,
                                                  int use_x, T* __restrict__ r, T* __restrict__ r0,
                                                  T* __restrict__ p, T* __restrict__ v, BcgScalars* S,
                                                  Partials P, double tol, double bnorm_override) {
-    const int g = threadIdx.x & (G - 1);
-    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
-    const long long ngroups = (long long)gridDim.x * RB / G;
     double abb = 0, arr = 0;
-    for (long long i = gid; i < A.n; i += ngroups) {
-        double ax = use_x ? row_dot<T, G>(A.row, A.col, A.val, x, i, g) : 0.0;
-        if (g == 0) {
+    SELL_LOOP(A) {
+        double ax = use_x ? sell_row(A, s, lane, x) : 0.0;
+        long long i = (s << 5) + lane;
+        if (i < A.n) {
             T bi = b[i];
             T ri = use_x ? (T)((double)bi - ax) : bi;
             r[i] = ri;
@@ -430,29 +441,15 @@ __global__ void __launch_bounds__(RB) k_bcg_init(Csr<T> A, const T* __restrict__
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// Mixed-precision helpers
-// ---------------------------------------------------------------------------------------
-// FP32 copy of A D^-1 (column scaling) and FP64 A D^-1.
-template <class T>
-__global__ void k_scale_cols(long long nnz, const int* __restrict__ col, const double* __restrict__ val,
-                             const double* __restrict__ dinv, T* __restrict__ out) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
-        out[e] = (T)(val[e] * dinv[col[e]]);
-}
-
-// r = b - A x (FP64), |r|^2 into partials; rf = r / |r| is produced by k_scale_rhs.
-template <int G>
-__global__ void __launch_bounds__(RB) k_residual64(Csr<double> A, const double* __restrict__ b,
+// r = b - A x (FP64), |r|^2 and |b|^2 into out2 (fixed-order partials).
+__global__ void __launch_bounds__(RB) k_residual64(Sell<double> A, const double* __restrict__ b,
                                                    const double* __restrict__ x, double* __restrict__ r,
                                                    double* out2, Partials P, unsigned int* counter) {
-    const int g = threadIdx.x & (G - 1);
-    const long long gid = (blockIdx.x * (long long)RB + threadIdx.x) / G;
-    const long long ngroups = (long long)gridDim.x * RB / G;
     double arr = 0, abb = 0;
-    for (long long i = gid; i < A.n; i += ngroups) {
-        double ax = row_dot<double, G>(A.row, A.col, A.val, x, i, g);
-        if (g == 0) {
+    SELL_LOOP(A) {
+        double ax = sell_row(A, s, lane, x);
+        long long i = (s << 5) + lane;
+        if (i < A.n) {
             double ri = b[i] - ax;
             r[i] = ri;
             arr += ri * ri;
@@ -470,6 +467,63 @@ __global__ void __launch_bounds__(RB) k_residual64(Csr<double> A, const double* 
     }
 }
 
+// ---- SELL-32 construction from the CSR rows ----
+// slice lengths: one warp per slice
+__global__ void k_sell_len(long long n, long long nslices, const int* __restrict__ row, int* __restrict__ slen,
+                           int* __restrict__ ssize) {
+    const int lane = threadIdx.x & 31;
+    long long s = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    if (s >= nslices) return;
+    long long i = (s << 5) + lane;
+    int len = i < n ? row[i + 1] - row[i] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+    if (lane == 0) {
+        slen[s] = len;
+        ssize[s] = len * 32;
+    }
+}
+
+// one thread per slot row (padding rows of the last slice included): entries in CSR
+// order, padding with value 0 and the row's own column (always a valid index)
+__global__ void k_sell_fill(long long n, long long nslices, const int* __restrict__ row,
+                            const int* __restrict__ acol, const double* __restrict__ aval,
+                            const int* __restrict__ sptr, const int* __restrict__ slen, int* __restrict__ col,
+                            double* __restrict__ val) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nslices * 32) return;
+    long long s = i >> 5;
+    int lane = (int)(i & 31);
+    int e0 = 0, len = 0;
+    if (i < n) {
+        e0 = row[i];
+        len = row[i + 1] - e0;
+    }
+    const int pad_col = i < n ? (int)i : 0;
+    long long base = (long long)sptr[s] + lane;
+    for (int k = 0; k < slen[s]; ++k) {
+        long long e = base + 32LL * k;
+        if (k < len) {
+            col[e] = acol[e0 + k];
+            val[e] = aval[e0 + k];
+        } else {
+            col[e] = pad_col;
+            val[e] = 0.0;
+        }
+    }
+}
+
+// Column scaling A D^-1 (Jacobi right preconditioning folded into the matrix).
+template <class T>
+__global__ void k_scale_cols(long long nnz, const int* __restrict__ col, const double* __restrict__ val,
+                             const double* __restrict__ dinv, T* __restrict__ out) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
+        out[e] = (T)(val[e] * dinv[col[e]]);
+}
+
+// ---------------------------------------------------------------------------------------
+// Mixed-precision helpers
+// ---------------------------------------------------------------------------------------
 __global__ void k_scale_rhs(long long n, const double* __restrict__ r, const double* scal, float* __restrict__ rf,
                             float* __restrict__ yf) {
     double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0]) : 0.0;
@@ -485,6 +539,12 @@ __global__ void k_apply_correction(long long n, double* __restrict__ x, const fl
     double nr = sqrt(scal[0]);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         x[i] += nr * dinv[i] * (double)y[i];
+}
+
+template <class T>
+__global__ void k_fill(long long n, T* __restrict__ x, T v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = v;
 }
 
 __global__ void k_unscale(long long n, double* __restrict__ x, const double* __restrict__ dinv) {
@@ -523,14 +583,13 @@ __global__ void __launch_bounds__(RB) k_error_stats(long long n, const double* _
 }
 
 // ---------------------------------------------------------------------------------------
-// host side
+// host side of the engine
 // ---------------------------------------------------------------------------------------
 struct Engine {
     lsmps_ctx* ctx;
     cudaStream_t s;
     BcgScalars* S;
     Partials P;
-    int group;  // lanes per row (4, 8, 16 or 32)
 };
 
 template <class T>
@@ -538,61 +597,41 @@ struct Vecs {
     T *x, *r, *r0, *p, *v, *s, *t;
 };
 
-template <class T, int G>
-void launch_iteration(Engine& E, const Csr<T>& A, const Vecs<T>& V) {
+Engine make_engine(lsmps_ctx* ctx) {
+    Engine E{ctx, ctx->stream, nullptr, {}};
+    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
+    E.P = Partials{red, red + RGRID};
+    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+    return E;
+}
+
+double* engine_scalars(lsmps_ctx* ctx) { return ctx->red.get<double>() + 2 * RGRID + 128; }
+
+template <class T>
+void iteration(Engine& E, const Sell<T>& A, const Vecs<T>& V) {
+    note_launches(5);
     k_bcg_p<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.p, V.v, E.S);
-    k_bcg_v<T, G><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
+    k_bcg_v<T><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
     k_bcg_s<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.v, V.s, E.S, E.P);
-    k_bcg_t<T, G><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
+    k_bcg_t<T><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
     k_bcg_x<T><<<RGRID, RB, 0, E.s>>>(A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P);
 }
 
 template <class T>
-void iteration(Engine& E, const Csr<T>& A, const Vecs<T>& V) {
-    note_launches(5);
-    switch (E.group) {
-        case 4: launch_iteration<T, 4>(E, A, V); break;
-        case 8: launch_iteration<T, 8>(E, A, V); break;
-        case 16: launch_iteration<T, 16>(E, A, V); break;
-        default: launch_iteration<T, 32>(E, A, V); break;
-    }
-}
-
-template <class T>
-void init(Engine& E, const Csr<T>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
-    switch (E.group) {
-        case 4: k_bcg_init<T, 4><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
-        case 8: k_bcg_init<T, 8><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
-        case 16: k_bcg_init<T, 16><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
-        default: k_bcg_init<T, 32><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override); break;
-    }
+void init(Engine& E, const Sell<T>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
+    k_bcg_init<T><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override);
     LSMPS_CHECK_LAUNCH();
 }
 
-void residual64(Engine& E, const Csr<double>& A, const double* b, const double* x, double* r, double* out2) {
-    unsigned int* counter = &E.S->counter[5];
-    switch (E.group) {
-        case 4: k_residual64<4><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
-        case 8: k_residual64<8><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
-        case 16: k_residual64<16><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
-        default: k_residual64<32><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, counter); break;
-    }
+void residual64(Engine& E, const Sell<double>& A, const double* b, const double* x, double* r, double* out2) {
+    k_residual64<<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, &E.S->counter[5]);
     LSMPS_CHECK_LAUNCH();
-}
-
-// Lanes per row from the mean row length (the tuning table picks among these).
-int pick_group(long long n, long long nnz) {
-    double mean = n ? (double)nnz / (double)n : 0;
-    if (mean <= 6) return 4;
-    if (mean <= 12) return 8;
-    if (mean <= 24) return 16;
-    return 32;
 }
 
 // Runs the iteration until done, as a CUDA graph of `chunk` iterations when requested.
 // Returns the final scalars.
 template <class T>
-BcgScalars run_loop(Engine& E, const Csr<T>& A, const Vecs<T>& V, int chunk, bool use_graph) {
+BcgScalars run_loop(Engine& E, const Sell<T>& A, const Vecs<T>& V, int chunk, bool use_graph) {
     BcgScalars h{};
     cudaGraphExec_t exec = nullptr;
     if (use_graph) {
@@ -714,31 +753,88 @@ static void solve_exact(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     ps->solve_ms = ev_elapsed(ctx, 10, 11);
 }
 
+
+// ---- SELL-32 copies of the assembled matrix (built on first use after an assembly) ----
+// kind 0: A (FP64), 1: A D^-1 (FP64), 2: A D^-1 (FP32)
+static void sell_structure(lsmps_ctx* ctx) {
+    if (ctx->have_sell) return;
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    const long long ns = (U + 31) / 32;
+    int* slen = ctx->S_len.ensure<int>(ns + 1);
+    int* ssize = ctx->vtmp.ensure<int>(ns + 1);
+    int* sptr = ctx->S_ptr.ensure<int>(ns + 1);
+    if (ns) {
+        k_sell_len<<<blocks_for(ns * 32, 256), 256, 0, s>>>(U, ns, ctx->A_row.get<int>(), slen, ssize);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<int>(ssize, sptr, ns, s, ctx->scan_tmp, ctx->dflags.get<int>());
+    int total = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&total, sptr + ns, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    check_device_flags(ctx, "SELL layout");
+    ctx->sell_nslices = ns;
+    ctx->sell_entries = total;
+    int* col = ctx->S_col.ensure<int>((size_t)total + 1);
+    double* val = ctx->S_val.ensure<double>((size_t)total + 1);
+    if (ns) {
+        k_sell_fill<<<blocks_for(ns * 32, 256), 256, 0, s>>>(U, ns, ctx->A_row.get<int>(), ctx->A_col.get<int>(),
+                                                             ctx->A_val.get<double>(), sptr, slen, col, val);
+        LSMPS_CHECK_LAUNCH();
+    }
+    ctx->have_sell = true;
+}
+
+template <class T>
+static Sell<T> sell_view(lsmps_ctx* ctx, const T* val) {
+    return Sell<T>{ctx->U, ctx->sell_nslices, ctx->S_ptr.get<int>(), ctx->S_len.get<int>(), ctx->S_col.get<int>(), val};
+}
+
+static Sell<double> sell_a64(lsmps_ctx* ctx) {
+    sell_structure(ctx);
+    return sell_view<double>(ctx, ctx->S_val.get<double>());
+}
+
+static Sell<double> sell_scaled64(lsmps_ctx* ctx) {
+    sell_structure(ctx);
+    if (!ctx->have_sell_s) {
+        double* v = ctx->S_vals.ensure<double>((size_t)ctx->sell_entries + 1);
+        k_scale_cols<double><<<1184, 256, 0, ctx->stream>>>(ctx->sell_entries, ctx->S_col.get<int>(),
+                                                           ctx->S_val.get<double>(), ctx->A_dinv.get<double>(), v);
+        LSMPS_CHECK_LAUNCH();
+        ctx->have_sell_s = true;
+    }
+    return sell_view<double>(ctx, ctx->S_vals.get<double>());
+}
+
+static Sell<float> sell_scaled32(lsmps_ctx* ctx) {
+    sell_structure(ctx);
+    if (!ctx->have_sell_f) {
+        float* v = ctx->S_valf.ensure<float>((size_t)ctx->sell_entries + 1);
+        k_scale_cols<float><<<1184, 256, 0, ctx->stream>>>(ctx->sell_entries, ctx->S_col.get<int>(),
+                                                          ctx->S_val.get<double>(), ctx->A_dinv.get<double>(), v);
+        LSMPS_CHECK_LAUNCH();
+        ctx->have_sell_f = true;
+    }
+    return sell_view<float>(ctx, ctx->S_valf.get<float>());
+}
+
 // Fast FP64 / Jacobi: BiCGStab on A (or A D^-1) in FP64.
 static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool jacobi) {
     cudaStream_t s = ctx->stream;
-    long long U = ctx->U, nnz = ctx->nnz;
-    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
-    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
-    E.P = Partials{red, red + RGRID};
-    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
+    long long U = ctx->U;
+    Engine E = make_engine(ctx);
     Vecs<double> V{ctx->vx.ensure<double>(U + 1), ctx->vr.ensure<double>(U + 1), ctx->vr0.ensure<double>(U + 1),
                    ctx->vp.ensure<double>(U + 1), ctx->vv.ensure<double>(U + 1), ctx->vs.ensure<double>(U + 1),
                    ctx->vt.ensure<double>(U + 1)};
     const double* dinv = ctx->A_dinv.get<double>();
-    Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
-    Csr<double> Aop = A;
-    if (jacobi) {
-        double* sc = ctx->A_cnt.ensure<double>(nnz + 1);  // reused as the scaled FP64 values
-        k_scale_cols<double><<<1184, 256, 0, s>>>(nnz, A.col, A.val, dinv, sc);
-        LSMPS_CHECK_LAUNCH();
-        Aop.val = sc;
-    }
     bool warm = o->warm_start && ctx->have_solution;
     ev_record(ctx, 10);
+    Sell<double> Aop = jacobi ? sell_scaled64(ctx) : sell_a64(ctx);
     set_scalar_caps(E, o->max_iter, 0);
     if (warm && jacobi) {  // the iteration works on y = D x
         k_scale_by_diag<<<1184, 256, 0, s>>>(U, V.x, dinv);
+        LSMPS_CHECK_LAUNCH();
     } else if (!warm) {
         LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
     }
@@ -760,18 +856,10 @@ static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_s
 // Mixed precision (and learned): FP64 refinement around FP32 inner solves.
 static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
     cudaStream_t s = ctx->stream;
-    long long U = ctx->U, nnz = ctx->nnz;
-    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
-    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
-    E.P = Partials{red, red + RGRID};
-    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
-    double* scal = red + 2 * RGRID + 128;  // [0] |r|^2, [1] |b|^2
+    long long U = ctx->U;
+    Engine E = make_engine(ctx);
+    double* scal = engine_scalars(ctx);  // [0] |r|^2, [1] |b|^2
     const double* dinv = ctx->A_dinv.get<double>();
-    Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
-    float* valf = ctx->A_valf.ensure<float>(nnz + 1);
-    k_scale_cols<float><<<1184, 256, 0, s>>>(nnz, A.col, A.val, dinv, valf);
-    LSMPS_CHECK_LAUNCH();
-    Csr<float> Af{U, A.row, A.col, valf};
     double* x = ctx->vx.ensure<double>(U + 1);
     double* r = ctx->vr.ensure<double>(U + 1);
     float* rhs = ctx->fph.ensure<float>(U + 1);
@@ -781,29 +869,29 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     const bool use_nn = learned && mpnn_ready(ctx);
     bool warm = o->warm_start && ctx->have_solution;
     const double inner_tol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
-    const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : 200;
+    const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : 400;
     const int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
     const int stall = o->stall_window > 0 ? o->stall_window : 20;
     ev_record(ctx, 10);
+    Sell<double> A = sell_a64(ctx);
+    Sell<float> Af = sell_scaled32(ctx);
     set_scalar_caps(E, 0, 0);  // zero the reduction tickets before the first residual
     if (!warm) LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
     int total_inner = 0, outer = 0, fallback = 0;
     bool converged = false;
-    double bnorm = 0, rnorm = 0;
     const int max_outer = 200;
     for (; outer < max_outer; ++outer) {
         residual64(E, A, ctx->A_b.get<double>(), x, r, scal);
         double h2[2];
         LSMPS_CUDA(cudaMemcpyAsync(h2, scal, sizeof(h2), cudaMemcpyDeviceToHost, s));
         LSMPS_CUDA(cudaStreamSynchronize(s));
-        rnorm = std::sqrt(h2[0]);
-        bnorm = std::sqrt(h2[1]);
+        const double rnorm = std::sqrt(h2[0]), bnorm = std::sqrt(h2[1]);
         if (!std::isfinite(rnorm)) break;
         if (rnorm <= o->tol * std::max(1.0, bnorm)) { converged = true; break; }
         if (total_inner >= o->max_iter) break;
         k_scale_rhs<<<1184, 256, 0, s>>>(U, r, scal, rhs, V.x);
         LSMPS_CHECK_LAUNCH();
-        bool nn_now = use_nn && !fallback;
+        const bool nn_now = use_nn && !fallback;
         if (nn_now) mpnn_warm_start(ctx, rhs, V.x);
         set_scalar_caps(E, std::min(inner_max, o->max_iter - total_inner), nn_now ? stall : 0);
         // relative inner tolerance on the unit-norm right-hand side
@@ -813,7 +901,10 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         if (h.done == 4 && nn_now) fallback = 1;  // stalled: continue with plain Jacobi sweeps
         k_apply_correction<<<1184, 256, 0, s>>>(U, x, V.x, dinv, scal);
         LSMPS_CHECK_LAUNCH();
-        if (h.iters == 0 && h.done != 1) { fallback = fallback || nn_now; if (!nn_now) break; }
+        if (h.iters == 0 && h.done != 1) {
+            if (!nn_now) break;
+            fallback = 1;
+        }
     }
     ev_record(ctx, 11);
     LSMPS_CUDA(cudaStreamSynchronize(s));
@@ -845,15 +936,11 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
         else solve_mixed(ctx, o, &ps, o->solver == LSMPS_SOLVER_LEARNED);
         // final statistics in FP64: |Ax - b|, |b|, error against p*
         cudaStream_t s = ctx->stream;
-        Engine E{ctx, s, nullptr, {}, pick_group(U, ctx->nnz)};
-        double* red = ctx->red.ensure<double>(2 * RGRID + 256);
-        E.P = Partials{red, red + RGRID};
-        E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
-        double* scal = red + 2 * RGRID + 128;
-        Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
+        Engine E = make_engine(ctx);
+        double* scal = engine_scalars(ctx);
         double* x = ctx->vx.get<double>();
         double* tmp = ctx->vt.ensure<double>(U + 1);
-        residual64(E, A, ctx->A_b.get<double>(), x, tmp, scal);
+        residual64(E, sell_a64(ctx), ctx->A_b.get<double>(), x, tmp, scal);
         auto* maxbits = reinterpret_cast<unsigned long long*>(scal + 4);
         LSMPS_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), s));
         k_error_stats<<<RGRID, RB, 0, s>>>(U, x, ctx->A_xexact.get<double>(), scal + 2, E.P, &E.S->counter[6],
@@ -881,52 +968,31 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
 void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes) {
     LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "SpMV bench needs an assembled PPE");
     cudaStream_t s = ctx->stream;
-    long long U = ctx->U, nnz = ctx->nnz;
-    Engine E{ctx, s, nullptr, {}, pick_group(U, nnz)};
-    double* red = ctx->red.ensure<double>(2 * RGRID + 256);
-    E.P = Partials{red, red + RGRID};
-    E.S = reinterpret_cast<BcgScalars*>(red + 2 * RGRID);
-    set_scalar_caps(E, 1 << 30, 0);
+    const long long U = ctx->U;
+    Engine E = make_engine(ctx);
     BcgScalars init{};
     init.max_iter = 1 << 30;
     init.rho = 1.0;
     LSMPS_CUDA(cudaMemcpyAsync(E.S, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     const bool f32 = kernel == LSMPS_KB_SPMV32;
+    // operands of ones: the fused dot is then nonzero, so no breakdown guard stops the kernel
     if (f32) {
-        float* valf = ctx->A_valf.ensure<float>(nnz + 1);
-        k_scale_cols<float><<<1184, 256, 0, s>>>(nnz, ctx->A_col.get<int>(), ctx->A_val.get<double>(),
-                                                 ctx->A_dinv.get<double>(), valf);
-        LSMPS_CHECK_LAUNCH();
-        float* x = ctx->fp.ensure<float>(U + 1);
-        float* r0 = ctx->fr0.ensure<float>(U + 1);
+        k_fill<float><<<1184, 256, 0, s>>>(U, ctx->fp.ensure<float>(U + 1), 1.0f);
+        k_fill<float><<<1184, 256, 0, s>>>(U, ctx->fr0.ensure<float>(U + 1), 1.0f);
         ctx->fv.ensure<float>(U + 1);
-        LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(float), s));
-        LSMPS_CUDA(cudaMemsetAsync(r0, 0, U * sizeof(float), s));
     } else {
-        double* x = ctx->vp.ensure<double>(U + 1);
-        double* r0 = ctx->vr0.ensure<double>(U + 1);
+        k_fill<double><<<1184, 256, 0, s>>>(U, ctx->vp.ensure<double>(U + 1), 1.0);
+        k_fill<double><<<1184, 256, 0, s>>>(U, ctx->vr0.ensure<double>(U + 1), 1.0);
         ctx->vv.ensure<double>(U + 1);
-        LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
-        LSMPS_CUDA(cudaMemsetAsync(r0, 0, U * sizeof(double), s));
     }
+    LSMPS_CHECK_LAUNCH();
+    Sell<float> Af{};
+    Sell<double> Ad{};
+    if (f32) Af = sell_scaled32(ctx);
+    else Ad = sell_a64(ctx);
     auto launch = [&] {
-        if (f32) {
-            Csr<float> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_valf.get<float>()};
-            switch (E.group) {
-                case 4: k_bcg_v<float, 4><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
-                case 8: k_bcg_v<float, 8><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
-                case 16: k_bcg_v<float, 16><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
-                default: k_bcg_v<float, 32><<<RGRID, RB, 0, s>>>(A, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P); break;
-            }
-        } else {
-            Csr<double> A{U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>()};
-            switch (E.group) {
-                case 4: k_bcg_v<double, 4><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
-                case 8: k_bcg_v<double, 8><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
-                case 16: k_bcg_v<double, 16><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
-                default: k_bcg_v<double, 32><<<RGRID, RB, 0, s>>>(A, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P); break;
-            }
-        }
+        if (f32) k_bcg_v<float><<<RGRID, RB, 0, s>>>(Af, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P);
+        else k_bcg_v<double><<<RGRID, RB, 0, s>>>(Ad, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P);
         LSMPS_CHECK_LAUNCH();
     };
     launch();
@@ -934,7 +1000,10 @@ void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, doubl
     for (int r = 0; r < reps; ++r) launch();
     ev_record(ctx, 15);
     *ms = ev_elapsed(ctx, 14, 15) / reps;
-    *bytes = f32 ? 8.0 * nnz + 16.0 * U + 4.0 : 12.0 * nnz + 28.0 * U + 4.0;
+    // algorithmic bytes: matrix values + columns once (nonzeros, not padding), row data,
+    // x once, y written once, r0 read once
+    const double nnz = (double)ctx->nnz;
+    *bytes = f32 ? 8.0 * nnz + 16.0 * U : 12.0 * nnz + 28.0 * U;
     // the bench overwrote solver vectors: a warm start from them is no longer valid
     ctx->have_solution = false;
 }

@@ -22,11 +22,15 @@ struct BcgScalars {
     unsigned int counter[8];  // last-block tickets of the reduction kernels
 };
 
-// A CSR matrix view in the solver's numbering.
+// A SELL-32 matrix view in the solver's numbering: rows in slices of 32, slice s holding
+// slen[s] entries per row stored column-major from sptr[s] (entry k of row 32 s + l at
+// sptr[s] + 32 k + l), zero-padded to its longest row.
 template <class T>
-struct Csr {
+struct Sell {
     long long n;
-    const int* row;
+    long long nslices;
+    const int* sptr;
+    const int* slen;
     const int* col;
     const T* val;
 };

@@ -353,14 +353,14 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                     for (int a = 0; a < NT; ++a) Lf[a] = (float)L[a];
                     fp32 = chol_packed<float>(Lf, 0.0f);
                     if (fp32) {
-                        // ill-conditioned systems go to FP64: pivot ratio below 1e-5
+                        // ill-conditioned systems go to FP64: squared pivot ratio below 1e-3
                         float dmin = Lf[0], dmax = Lf[0];
 #pragma unroll
                         for (int a = 1; a < K; ++a) {
                             dmin = fminf(dmin, Lf[tri(a, a)]);
                             dmax = fmaxf(dmax, Lf[tri(a, a)]);
                         }
-                        if (dmin * dmin < 1e-5f * dmax * dmax) fp32 = false;
+                        if (dmin * dmin < 1e-3f * dmax * dmax) fp32 = false;
                     }
                 }
                 if (fp32) {
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                     double inv = 1.0 / ws;
                     double z[K] = {0, 0, 0, 1, 1, 1, 0, 0, 0};
                     if (PREC && fp32) {
-                        // FP32 solves refined against the FP64 moments (two sweeps); L still
+                        // FP32 solves refined against the FP64 moments (three sweeps); L still
                         // holds the FP64 moments because the FP32 factor lives in Lf.
                         const double* Md = L;
                         auto refine = [&](double* x) {
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
 #pragma unroll
                             for (int a = 0; a < K; ++a) x[a] = xf[a];
 #pragma unroll
-                            for (int sweep = 0; sweep < 2; ++sweep) {
+                            for (int sweep = 0; sweep < 3; ++sweep) {
                                 float rf[K];
 #pragma unroll
                                 for (int a = 0; a < K; ++a) {

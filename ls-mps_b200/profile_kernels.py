@@ -1,0 +1,41 @@
+"""Runs one kernel of the path on a named workload, for profilers (ncu) and quick timing.
+
+    python ls-mps_b200/profile_kernels.py --kernel spmv32 --particles 1000000 --reps 3
+
+Builds the workload of bench.py (case `mixed`, l0 = 1, re = 2.1, max_neighbors 128,
+WLS-Laplacian PPE) with the library, then launches the chosen kernel `reps` times through
+lsmps_kernel_bench and prints its mean time and achieved bandwidth. Under ncu, select the
+kernel with -k (spmv32/spmv64: k_bcg_v, nbr_count: k_count, nbr_fill: k_fill, wls: k_wls_all).
+"""
+import argparse
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import lsmps_b200 as lib  # noqa: E402
+
+KERNELS = {"spmv32": lib.KB_SPMV32, "spmv64": lib.KB_SPMV64, "nbr_count": lib.KB_NBR_COUNT,
+           "nbr_fill": lib.KB_NBR_FILL, "wls": lib.KB_WLS}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel", choices=sorted(KERNELS), nargs="+", default=["spmv32"])
+    ap.add_argument("--particles", type=int, default=1_000_000)
+    ap.add_argument("--case", default="mixed")
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    xyz, t, _ = lib.generate(None, case=a.case, particles=a.particles, l0=1.0, seed=7)
+    with lib.Context(0) as ctx:
+        ctx.upload(xyz, t)
+        ctx.build_neighbors(2.1, 128, 1.0)
+        ctx.wls(2.1, 1.0, mode=1)
+        st = ctx.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
+        print(f"particles {len(t)} unknowns {st.unknowns} nnz {st.nnz}")
+        for k in a.kernel:
+            ms, nb = ctx.kernel_bench(KERNELS[k], a.reps)
+            print(f"{k}: {ms * 1e3:.1f} us per launch, {nb / 1e6:.1f} MB algorithmic, {nb / ms / 1e6:.0f} GB/s")
+
+
+if __name__ == "__main__":
+    main()
