@@ -35,6 +35,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "ls-mps_b200"))
+# oracle/ (test infrastructure) is imported only by the CPU-baseline leg and the reference arm
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "PPE solve ms & particle-steps/s at 1M, learned+mixed vs plain FP64 @ L2<=1e-8"
 UNIT = "particle-steps/s"
@@ -310,7 +312,6 @@ def run_mine(args, dist):
 
 def _ref_case(xyz, types):
     """A reference handle on this particle set with the bench's parameters."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Ref
 
     fd, path = tempfile.mkstemp(suffix=".cfg")
@@ -373,7 +374,6 @@ def run_reference(args, dist):
     restatement stands in; BiCGStab runs the reference's iteration for a bounded sample and
     is extrapolated to the iteration count that the same FP64 iteration (run once, in the
     warm-up, multi-threaded) needs to reach the tolerance."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import lsmps_b200 as lib
     from oracle import Oracle, Ref
 

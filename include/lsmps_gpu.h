@@ -160,9 +160,11 @@ enum {
                                    sequential-order dot products; for small systems */
     LSMPS_SOLVER_FP64 = 1,      /* the reference iteration in FP64, GPU reductions */
     LSMPS_SOLVER_JACOBI = 2,    /* FP64, Jacobi right preconditioning */
-    LSMPS_SOLVER_MIXED = 3,     /* FP32 Jacobi BiCGStab inner solves + FP64 residual refinement */
-    LSMPS_SOLVER_LEARNED = 4    /* MIXED with the message-passing network as warm start of each
-                                   refinement sweep; Jacobi fallback when the residual stalls */
+    LSMPS_SOLVER_MIXED = 3,     /* Jacobi BiCGStab, FP64 vectors, FP32 matrix in the iteration's SpMVs,
+                                   FP64 true-residual replacement every `inner_tol` drop */
+    LSMPS_SOLVER_LEARNED = 4,   /* MIXED started from the message-passing network's guess; plain
+                                   Jacobi continuation when the residual stalls */
+    LSMPS_SOLVER_MIXED_F32 = 5  /* FP32 vectors and matrix, FP64 solution and residual refinement */
 };
 
 typedef struct lsmps_solver_opts {
@@ -171,8 +173,9 @@ typedef struct lsmps_solver_opts {
     double tol;              /* converged when |r| <= tol * max(1, |b|) (src/lsmps.cpp:67) */
     int32_t warm_start;      /* start from the last solution held by the context */
     int32_t use_graph;       /* capture the iteration in a CUDA graph (FP64 / JACOBI / MIXED) */
-    double inner_tol;        /* MIXED: relative reduction per FP32 inner solve (default 1e-4) */
-    int32_t inner_max_iter;  /* MIXED: inner iteration cap per sweep (default 200) */
+    double inner_tol;        /* MIXED / LEARNED / MIXED_F32: residual drop between FP64 residual
+                                replacements (default 0.1) */
+    int32_t inner_max_iter;  /* reserved */
     int32_t stall_window;    /* LEARNED: iterations without progress before fallback (20) */
     int32_t check_every;     /* iterations between host convergence checks (default 8) */
     int32_t reserved;

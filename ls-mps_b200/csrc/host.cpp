@@ -246,6 +246,7 @@ int solver_id(const std::string& s) {
     if (s == "jacobi") return LSMPS_SOLVER_JACOBI;
     if (s == "mixed") return LSMPS_SOLVER_MIXED;
     if (s == "learned") return LSMPS_SOLVER_LEARNED;
+    if (s == "mixed_f32") return LSMPS_SOLVER_MIXED_F32;
     throw std::runtime_error("unknown solver: " + s);
 }
 

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "ops.cuh"
@@ -217,31 +219,64 @@ __device__ __forceinline__ void final_sum(Partials P, double* ra, double* rb) {
     }
 }
 
-// Row i of a SELL-32 matrix: slice s = i / 32 stores its rows' k-th entries contiguously
-// (entry k of lane l at sptr[s] + 32 k + l), padded with zeros to the slice's longest row.
-// One thread per row, one warp per slice: every matrix load is a coalesced 128-byte (FP32)
-// or 256-byte (FP64) line, and the k-loop is unrolled four ways so that each thread keeps
-// eight matrix loads and four gathers in flight. Matrix loads stream past L1/L2 (__ldcs) so
-// the vectors, which are re-read every iteration, stay in the 126 MB L2.
-template <class T>
-__device__ __forceinline__ double sell_row(const Sell<T>& A, long long s, int lane, const T* __restrict__ x) {
-    const T* __restrict__ val = A.val + A.sptr[s] + lane;
-    const int* __restrict__ col = A.col + A.sptr[s] + lane;
-    const int len = A.slen[s];
-    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    int k = 0;
-    for (; k + 4 <= len; k += 4) {
-        const T v0 = __ldcs(val + 32 * k), v1 = __ldcs(val + 32 * (k + 1)), v2 = __ldcs(val + 32 * (k + 2)),
-                v3 = __ldcs(val + 32 * (k + 3));
-        const int c0 = __ldcs(col + 32 * k), c1 = __ldcs(col + 32 * (k + 1)), c2 = __ldcs(col + 32 * (k + 2)),
-                  c3 = __ldcs(col + 32 * (k + 3));
-        a0 += (double)v0 * (double)x[c0];
-        a1 += (double)v1 * (double)x[c1];
-        a2 += (double)v2 * (double)x[c2];
-        a3 += (double)v3 * (double)x[c3];
+// Row i of a SELL-32x4 matrix: slice s = i / 32 stores its 32 rows in chunks of four
+// consecutive entries per row (entries 4c..4c+3 of lane l at sptr[s] + 128 c + 4 l), zero-
+// padded to the slice's longest row rounded up to a multiple of four. One thread per row,
+// one warp per slice: each thread reads its next four values and four columns with two
+// 16-byte loads (a warp covers 512 contiguous bytes per load), and two chunks are issued
+// before their eight x gathers, so each thread keeps 64-96 bytes of matrix loads and eight
+// gathers in flight. Matrix loads stream past L1/L2 (__ldcs) so the vectors, re-read every
+// iteration, stay in the 126 MB L2.
+__device__ __forceinline__ void ld4(const float* p, float v[4]) {
+    float4 q = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+    double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const int* p, int v[4]) {
+    int4 q = __ldcs(reinterpret_cast<const int4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+
+template <class TM, class T>
+__device__ __forceinline__ double sell_row(const Sell<TM>& A, long long s, int lane, const T* __restrict__ x) {
+    const long long base = (long long)A.sptr[s] + 4 * lane;
+    const TM* __restrict__ val = A.val + base;
+    const int* __restrict__ col = A.col + base;
+    const int chunks = A.slen[s] >> 2;
+    double a0 = 0, a1 = 0;
+    int c = 0;
+    for (; c + 2 <= chunks; c += 2) {
+        TM v0[4], v1[4];
+        int c0[4], c1[4];
+        ld4(val + 128 * c, v0);
+        ld4(col + 128 * c, c0);
+        ld4(val + 128 * (c + 1), v1);
+        ld4(col + 128 * (c + 1), c1);
+        T x0[4], x1[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            x0[j] = x[c0[j]];
+            x1[j] = x[c1[j]];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a0 += (double)v0[j] * (double)x0[j];
+            a1 += (double)v1[j] * (double)x1[j];
+        }
     }
-    for (; k < len; ++k) a0 += (double)__ldcs(val + 32 * k) * (double)x[__ldcs(col + 32 * k)];
-    return (a0 + a1) + (a2 + a3);
+    if (c < chunks) {
+        TM v0[4];
+        int c0[4];
+        ld4(val + 128 * c, v0);
+        ld4(col + 128 * c, c0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a0 += (double)v0[j] * (double)x[c0[j]];
+    }
+    return a0 + a1;
 }
 
 #define SELL_LOOP(A)                                                              \
@@ -250,19 +285,54 @@ __device__ __forceinline__ double sell_row(const Sell<T>& A, long long s, int la
     const long long nw = ((long long)gridDim.x * RB) >> 5;                        \
     for (long long s = w0; s < (A).nslices; s += nw)
 
+// Four consecutive vector elements per thread and access (float4, or two double2), so
+// the elementwise kernels keep 16-32 bytes per array in flight per thread.
+template <class T>
+struct V4 {
+    T a[4];
+};
+__device__ __forceinline__ V4<float> ld_v4(const float* p) {
+    float4 q = *reinterpret_cast<const float4*>(p);
+    return {{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ V4<double> ld_v4(const double* p) {
+    double2 u = reinterpret_cast<const double2*>(p)[0], w = reinterpret_cast<const double2*>(p)[1];
+    return {{u.x, u.y, w.x, w.y}};
+}
+__device__ __forceinline__ void st_v4(float* p, const V4<float>& v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
+}
+__device__ __forceinline__ void st_v4(double* p, const V4<double>& v) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v.a[0], v.a[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v.a[2], v.a[3]);
+}
+
+// Calls f4(i) for i = 0, 4, 8, ... (groups of four elements), then f1(i) for the tail.
+template <class F4, class F1>
+__device__ __forceinline__ void vec_loop(long long n, F4&& f4, F1&& f1) {
+    const long long n4 = n >> 2;
+    for (long long q = blockIdx.x * (long long)RB + threadIdx.x; q < n4; q += (long long)gridDim.x * RB) f4(q << 2);
+    for (long long i = (n4 << 2) + blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB)
+        f1(i);
+}
+
 // p = r + beta (p - omega v)
 template <class T>
 __global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__ r, T* __restrict__ p,
                                               const T* __restrict__ v, const BcgScalars* S) {
     if (S->done) return;
     const T beta = (T)S->beta, omega = (T)S->omega;
-    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB)
-        p[i] = r[i] + beta * (p[i] - omega * v[i]);
+    vec_loop(n, [&](long long i) {
+        V4<T> rr = ld_v4(r + i), pp = ld_v4(p + i), vv = ld_v4(v + i);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pp.a[j] = rr.a[j] + beta * (pp.a[j] - omega * vv.a[j]);
+        st_v4(p + i, pp);
+    }, [&](long long i) { p[i] = r[i] + beta * (p[i] - omega * v[i]); });
 }
 
 // v = A p; den = (r0, v); alpha = rho / den
-template <class T>
-__global__ void __launch_bounds__(RB) k_bcg_v(Sell<T> A, const T* __restrict__ p, T* __restrict__ v,
+template <class T, class TM = T>
+__global__ void __launch_bounds__(RB, 6) k_bcg_v(Sell<TM> A, const T* __restrict__ p, T* __restrict__ v,
                                               const T* __restrict__ r0, BcgScalars* S, Partials P) {
     if (S->done) return;
     double acc = 0;
@@ -294,11 +364,19 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
     if (S->done) return;
     const T alpha = (T)S->alpha;
     double acc = 0;
-    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+    vec_loop(n, [&](long long i) {
+        V4<T> rr = ld_v4(r + i), vv = ld_v4(v + i), ss;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            ss.a[j] = rr.a[j] - alpha * vv.a[j];
+            acc += (double)ss.a[j] * (double)ss.a[j];
+        }
+        st_v4(s + i, ss);
+    }, [&](long long i) {
         T si = r[i] - alpha * v[i];
         s[i] = si;
         acc += (double)si * (double)si;
-    }
+    });
     if (block_partials(acc, 0.0, P, &S->counter[1])) {
         double ss, unused;
         final_sum(P, &ss, &unused);
@@ -311,8 +389,8 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
 }
 
 // t = A s; omega = (t, s) / (t, t)
-template <class T>
-__global__ void __launch_bounds__(RB) k_bcg_t(Sell<T> A, const T* __restrict__ sv, T* __restrict__ t,
+template <class T, class TM = T>
+__global__ void __launch_bounds__(RB, 6) k_bcg_t(Sell<TM> A, const T* __restrict__ sv, T* __restrict__ t,
                                               BcgScalars* S, Partials P) {
     if (S->done || S->s_conv) return;
     double ats = 0, att = 0;
@@ -362,14 +440,25 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
         return;
     }
     double arr = 0, ar0r = 0;
-    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+    vec_loop(n, [&](long long i) {
+        V4<T> xx = ld_v4(x + i), pp = ld_v4(p + i), ss = ld_v4(s + i), tt = ld_v4(t + i), q0 = ld_v4(r0 + i), rr;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            xx.a[j] += alpha * pp.a[j] + omega * ss.a[j];
+            rr.a[j] = ss.a[j] - omega * tt.a[j];
+            arr += (double)rr.a[j] * (double)rr.a[j];
+            ar0r += (double)q0.a[j] * (double)rr.a[j];
+        }
+        st_v4(x + i, xx);
+        st_v4(r + i, rr);
+    }, [&](long long i) {
         T si = s[i];
         x[i] += alpha * p[i] + omega * si;
         T ri = si - omega * t[i];
         r[i] = ri;
         arr += (double)ri * (double)ri;
         ar0r += (double)r0[i] * (double)ri;
-    }
+    });
     if (block_partials(arr, ar0r, P, &S->counter[3])) {
         double rr, rho;
         final_sum(P, &rr, &rho);
@@ -395,8 +484,8 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
 }
 
 // Initialisation: r = b - A x (or r = b when x = 0), r0 = r, p = v = 0, |b|, rho = (r0, r).
-template <class T>
-__global__ void __launch_bounds__(RB) k_bcg_init(Sell<T> A, const T* __restrict__ b, const T* __restrict__ x,
+template <class T, class TM = T>
+__global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restrict__ b, const T* __restrict__ x,
                                                  int use_x, T* __restrict__ r, T* __restrict__ r0,
                                                  T* __restrict__ p, T* __restrict__ v, BcgScalars* S,
                                                  Partials P, double tol, double bnorm_override) {
@@ -442,7 +531,7 @@ __global__ void __launch_bounds__(RB) k_bcg_init(Sell<T> A, const T* __restrict_
 }
 
 // r = b - A x (FP64), |r|^2 and |b|^2 into out2 (fixed-order partials).
-__global__ void __launch_bounds__(RB) k_residual64(Sell<double> A, const double* __restrict__ b,
+__global__ void __launch_bounds__(RB, 6) k_residual64(Sell<double> A, const double* __restrict__ b,
                                                    const double* __restrict__ x, double* __restrict__ r,
                                                    double* out2, Partials P, unsigned int* counter) {
     double arr = 0, abb = 0;
@@ -478,6 +567,7 @@ __global__ void k_sell_len(long long n, long long nslices, const int* __restrict
     int len = i < n ? row[i + 1] - row[i] : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+    len = (len + 3) & ~3;  // chunks of four entries
     if (lane == 0) {
         slen[s] = len;
         ssize[s] = len * 32;
@@ -500,9 +590,9 @@ __global__ void k_sell_fill(long long n, long long nslices, const int* __restric
         len = row[i + 1] - e0;
     }
     const int pad_col = i < n ? (int)i : 0;
-    long long base = (long long)sptr[s] + lane;
+    long long base = (long long)sptr[s] + 4 * lane;
     for (int k = 0; k < slen[s]; ++k) {
-        long long e = base + 32LL * k;
+        long long e = base + 128LL * (k >> 2) + (k & 3);
         if (k < len) {
             col[e] = acol[e0 + k];
             val[e] = aval[e0 + k];
@@ -524,23 +614,6 @@ __global__ void k_scale_cols(long long nnz, const int* __restrict__ col, const d
 // ---------------------------------------------------------------------------------------
 // Mixed-precision helpers
 // ---------------------------------------------------------------------------------------
-__global__ void k_scale_rhs(long long n, const double* __restrict__ r, const double* scal, float* __restrict__ rf,
-                            float* __restrict__ yf) {
-    double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0]) : 0.0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        rf[i] = (float)(r[i] * inv);
-        if (yf) yf[i] = 0.f;
-    }
-}
-
-// x += |r| D^-1 y
-__global__ void k_apply_correction(long long n, double* __restrict__ x, const float* __restrict__ y,
-                                   const double* __restrict__ dinv, const double* scal) {
-    double nr = sqrt(scal[0]);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        x[i] += nr * dinv[i] * (double)y[i];
-}
-
 template <class T>
 __global__ void k_fill(long long n, T* __restrict__ x, T v) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -582,6 +655,124 @@ __global__ void __launch_bounds__(RB) k_error_stats(long long n, const double* _
     }
 }
 
+// ---- reliable updates of the mixed-precision solver ----
+// x_hi += sigma D^-1 y_lo (FP64), y_lo = 0
+__global__ void k_reliable_x(long long n, double* __restrict__ x, float* __restrict__ y,
+                             const double* __restrict__ dinv, const double* sigma) {
+    const double sg = *sigma;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] += sg * dinv[i] * (double)y[i];
+        y[i] = 0.f;
+    }
+}
+
+// r = r64 / sigma in FP32 replaces the recursive residual; rho' = (r0, r) and the next
+// beta follow, so the iteration continues with its search direction (van der Vorst & Ye
+// residual replacement).
+__global__ void __launch_bounds__(RB) k_reliable_r(long long n, const double* __restrict__ r64,
+                                                   const double* sigma, float* __restrict__ r,
+                                                   const float* __restrict__ r0, BcgScalars* S, Partials P) {
+    const double inv = 1.0 / *sigma;
+    double arr = 0, ar0r = 0;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+        float ri = (float)(r64[i] * inv);
+        r[i] = ri;
+        arr += (double)ri * (double)ri;
+        ar0r += (double)r0[i] * (double)ri;
+    }
+    if (block_partials(arr, ar0r, P, &S->counter[7])) {
+        double rr, rho;
+        final_sum(P, &rr, &rho);
+        if (threadIdx.x == 0) {
+            S->counter[7] = 0;
+            S->rn = sqrt(rr);
+            if (S->rn < S->best_rn) S->best_rn = S->rn;
+            S->beta = (rho / S->rho0) * (S->alpha / S->omega);
+            S->rho = rho;
+            S->done = 0;
+            S->s_conv = 0;
+            if (!isfinite(rho) || fabs(rho) < 1e-30) S->done = 2;
+        }
+    }
+}
+
+// rf = r64 / sigma (start of an FP32 run), sigma = |r64| given as its square in scal[0]
+__global__ void k_start_rhs(long long n, const double* __restrict__ r64, const double* scal, double* sigma,
+                            float* __restrict__ rf, float* __restrict__ y) {
+    const double sg = sqrt(scal[0]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *sigma = sg;
+    const double inv = sg > 0 ? 1.0 / sg : 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        rf[i] = (float)(r64[i] * inv);
+        y[i] = 0.f;
+    }
+}
+
+// Residual replacement of the mixed solver (FP64 vectors, FP32 matrix in the iteration):
+// r = b - (A D^-1) y with the FP64 matrix; rho' = (r0, r) and the next beta follow, so the
+// iteration continues with its search direction (van der Vorst & Ye). |r| goes to S->rn.
+__global__ void __launch_bounds__(RB, 6) k_replace_residual(Sell<double> A, const double* __restrict__ b,
+                                                            const double* __restrict__ y, double* __restrict__ r,
+                                                            const double* __restrict__ r0, BcgScalars* S,
+                                                            Partials P) {
+    double arr = 0, ar0r = 0;
+    SELL_LOOP(A) {
+        double ay = sell_row(A, s, lane, y);
+        long long i = (s << 5) + lane;
+        if (i < A.n) {
+            double ri = b[i] - ay;
+            r[i] = ri;
+            arr += ri * ri;
+            ar0r += r0[i] * ri;
+        }
+    }
+    if (block_partials(arr, ar0r, P, &S->counter[7])) {
+        double rr, rho;
+        final_sum(P, &rr, &rho);
+        if (threadIdx.x == 0) {
+            S->counter[7] = 0;
+            S->rn = sqrt(rr);
+            if (S->rn < S->best_rn) S->best_rn = S->rn;
+            S->beta = (rho / S->rho0) * (S->alpha / S->omega);
+            S->rho = rho;
+            S->done = 0;
+            S->s_conv = 0;
+            if (!isfinite(rr)) { S->nonfinite = 1; S->done = 2; }
+            else if (S->rn <= S->thresh) S->done = 1;
+            else if (!isfinite(rho) || fabs(rho) < 1e-30) S->done = 2;
+        }
+    }
+}
+
+// |b|^2 into scal[0]: one block, fixed order (once per learned solve)
+__global__ void k_norm2_one_block(long long n, const double* __restrict__ b, double* scal) {
+    __shared__ double part[32];
+    double acc = 0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc += b[i] * b[i];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tot += part[k];
+        scal[0] = tot;
+    }
+}
+
+// network input b / |b| (FP32)
+__global__ void k_rhs_unit(long long n, const double* __restrict__ b, float* __restrict__ rf, const double* scal) {
+    const double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0]) : 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        rf[i] = (float)(b[i] * inv);
+}
+
+// y0 = |b| net(b / |b|)
+__global__ void k_y_from_net(long long n, const float* __restrict__ yf, const double* scal, double* __restrict__ y) {
+    const double nb = sqrt(scal[0]);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = nb * (double)yf[i];
+}
+
 // ---------------------------------------------------------------------------------------
 // host side of the engine
 // ---------------------------------------------------------------------------------------
@@ -607,19 +798,19 @@ Engine make_engine(lsmps_ctx* ctx) {
 
 double* engine_scalars(lsmps_ctx* ctx) { return ctx->red.get<double>() + 2 * RGRID + 128; }
 
-template <class T>
-void iteration(Engine& E, const Sell<T>& A, const Vecs<T>& V) {
+template <class T, class TM = T>
+void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V) {
     note_launches(5);
     k_bcg_p<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.p, V.v, E.S);
-    k_bcg_v<T><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
+    k_bcg_v<T, TM><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
     k_bcg_s<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.v, V.s, E.S, E.P);
-    k_bcg_t<T><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
+    k_bcg_t<T, TM><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
     k_bcg_x<T><<<RGRID, RB, 0, E.s>>>(A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P);
 }
 
-template <class T>
-void init(Engine& E, const Sell<T>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
-    k_bcg_init<T><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override);
+template <class T, class TM = T>
+void init(Engine& E, const Sell<TM>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
+    k_bcg_init<T, TM><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override);
     LSMPS_CHECK_LAUNCH();
 }
 
@@ -853,63 +1044,245 @@ static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_s
     if (h.nonfinite) ps->converged = 0;
 }
 
-// Mixed precision (and learned): FP64 refinement around FP32 inner solves.
-static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
+// Mixed precision with FP32 vectors (MIXED_F32). One FP32 Jacobi-BiCGStab on A D^-1 y = r0 / sigma (sigma =
+// |r0|, so FP32 values start at O(1)) accumulates y_lo; whenever its recursive residual has
+// dropped by a factor `inner_tol` since the last update (checked every `check_every`
+// iterations), a reliable update folds y_lo into the FP64 solution x_hi, recomputes the
+// true residual b - A x_hi with the FP64 matrix, and replaces the FP32 residual with it,
+// keeping the search direction. Convergence is always decided on the FP64 residual. A
+// breakdown, a stall (LEARNED: no 1 % progress in `stall_window` iterations) or an FP32
+// residual that claims convergence the FP64 one does not confirm restarts the Krylov space
+// from the true residual; LEARNED starts the first run from the network's guess and, after
+// a stall, continues as plain Jacobi-BiCGStab (fallback).
+static void solve_mixed_f32(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
     cudaStream_t s = ctx->stream;
     long long U = ctx->U;
     Engine E = make_engine(ctx);
-    double* scal = engine_scalars(ctx);  // [0] |r|^2, [1] |b|^2
+    double* scal = engine_scalars(ctx);  // [0] |r|^2, [1] |b|^2, [6] sigma
+    double* sigma = scal + 6;
     const double* dinv = ctx->A_dinv.get<double>();
     double* x = ctx->vx.ensure<double>(U + 1);
-    double* r = ctx->vr.ensure<double>(U + 1);
+    double* r64 = ctx->vr.ensure<double>(U + 1);
     float* rhs = ctx->fph.ensure<float>(U + 1);
     Vecs<float> V{ctx->fx.ensure<float>(U + 1), ctx->fr.ensure<float>(U + 1), ctx->fr0.ensure<float>(U + 1),
                   ctx->fp.ensure<float>(U + 1), ctx->fv.ensure<float>(U + 1), ctx->fs.ensure<float>(U + 1),
                   ctx->ft.ensure<float>(U + 1)};
     const bool use_nn = learned && mpnn_ready(ctx);
-    bool warm = o->warm_start && ctx->have_solution;
-    const double inner_tol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
-    const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : 400;
+    const bool warm = o->warm_start && ctx->have_solution;
+    const double delta = o->inner_tol > 0 ? o->inner_tol : 0.1;  // residual drop between updates
     const int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
     const int stall = o->stall_window > 0 ? o->stall_window : 20;
     ev_record(ctx, 10);
     Sell<double> A = sell_a64(ctx);
     Sell<float> Af = sell_scaled32(ctx);
-    set_scalar_caps(E, 0, 0);  // zero the reduction tickets before the first residual
+    set_scalar_caps(E, 0, 0);  // zero the reduction tickets
     if (!warm) LSMPS_CUDA(cudaMemsetAsync(x, 0, U * sizeof(double), s));
-    int total_inner = 0, outer = 0, fallback = 0;
-    bool converged = false;
-    const int max_outer = 200;
-    for (; outer < max_outer; ++outer) {
-        residual64(E, A, ctx->A_b.get<double>(), x, r, scal);
+    auto true_residual = [&]() {
+        residual64(E, A, ctx->A_b.get<double>(), x, r64, scal);
         double h2[2];
         LSMPS_CUDA(cudaMemcpyAsync(h2, scal, sizeof(h2), cudaMemcpyDeviceToHost, s));
         LSMPS_CUDA(cudaStreamSynchronize(s));
-        const double rnorm = std::sqrt(h2[0]), bnorm = std::sqrt(h2[1]);
-        if (!std::isfinite(rnorm)) break;
-        if (rnorm <= o->tol * std::max(1.0, bnorm)) { converged = true; break; }
-        if (total_inner >= o->max_iter) break;
-        k_scale_rhs<<<1184, 256, 0, s>>>(U, r, scal, rhs, V.x);
+        return std::make_pair(std::sqrt(h2[0]), std::sqrt(h2[1]));
+    };
+    auto [rnorm, bnorm] = true_residual();
+    const double thresh = o->tol * std::max(1.0, bnorm);
+    int total = 0, runs = 0, updates = 0, fallback = 0;
+    bool converged = rnorm <= thresh;
+    bool nonfinite = !std::isfinite(rnorm);
+    cudaGraphExec_t exec = nullptr;
+    auto read_scalars = [&](BcgScalars& h) {
+        LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, s));
+        LSMPS_CUDA(cudaStreamSynchronize(s));
+    };
+    while (!converged && !nonfinite && total < o->max_iter) {
+        // ---- an FP32 run from the true residual: sigma = |r|, rhs = r / sigma ----
+        k_start_rhs<<<1184, 256, 0, s>>>(U, r64, scal, sigma, rhs, V.x);
         LSMPS_CHECK_LAUNCH();
-        const bool nn_now = use_nn && !fallback;
+        const bool nn_now = use_nn && !fallback && runs == 0;
         if (nn_now) mpnn_warm_start(ctx, rhs, V.x);
-        set_scalar_caps(E, std::min(inner_max, o->max_iter - total_inner), nn_now ? stall : 0);
-        // relative inner tolerance on the unit-norm right-hand side
-        init<float>(E, Af, rhs, V, nn_now, inner_tol, 1.0);
-        BcgScalars h = run_loop<float>(E, Af, V, chunk, o->use_graph != 0);
-        total_inner += h.iters;
-        if (h.done == 4 && nn_now) fallback = 1;  // stalled: continue with plain Jacobi sweeps
-        k_apply_correction<<<1184, 256, 0, s>>>(U, x, V.x, dinv, scal);
-        LSMPS_CHECK_LAUNCH();
-        if (h.iters == 0 && h.done != 1) {
-            if (!nn_now) break;
-            fallback = 1;
+        set_scalar_caps(E, o->max_iter - total, nn_now ? stall : 0);
+        // FP32 threshold in the scaled system's units: |r| / sigma <= thresh / sigma
+        init<float>(E, Af, rhs, V, nn_now, thresh / std::max(rnorm, 1e-300), 1.0);
+        ++runs;
+        if (!exec && o->use_graph) {
+            cudaGraph_t graph;
+            LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int c = 0; c < chunk; ++c) iteration<float>(E, Af, V);
+            note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+            cudaError_t e = cudaStreamEndCapture(s, &graph);
+            LSMPS_CUDA(e);
+            LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            cudaGraphDestroy(graph);
         }
+        BcgScalars h{};
+        read_scalars(h);
+        double rn_upd = h.rn;  // FP32 residual at the last update of this run
+        int run_base = 0;      // iterations of this run already counted
+        while (true) {
+            if (!h.done) {
+                if (exec) {
+                    LSMPS_CUDA(cudaGraphLaunch(exec, s));
+                    note_launches(5 * (uint64_t)chunk);
+                } else {
+                    for (int k = 0; k < chunk; ++k) iteration<float>(E, Af, V);
+                    LSMPS_CHECK_LAUNCH();
+                }
+                read_scalars(h);
+            }
+            total += h.iters - run_base;
+            run_base = h.iters;
+            if (!h.done && h.rn > delta * rn_upd) continue;
+            // ---- reliable update: fold y_lo into x_hi, true FP64 residual ----
+            k_reliable_x<<<1184, 256, 0, s>>>(U, x, V.x, dinv, sigma);
+            LSMPS_CHECK_LAUNCH();
+            std::tie(rnorm, bnorm) = true_residual();
+            ++updates;
+            if (!std::isfinite(rnorm)) { nonfinite = true; break; }
+            if (rnorm <= thresh) { converged = true; break; }
+            if (total >= o->max_iter || h.done == 3) break;
+            if (h.done) {  // breakdown, stall, or an FP32 convergence the FP64 residual denies
+                if (h.done == 4 && nn_now) fallback = 1;
+                break;     // restart from the true residual
+            }
+            k_reliable_r<<<RGRID, RB, 0, s>>>(U, r64, sigma, V.r, V.r0, E.S, E.P);
+            LSMPS_CHECK_LAUNCH();
+            read_scalars(h);
+            rn_upd = h.rn;
+            if (h.done) break;  // rho breakdown after the replacement: restart
+        }
+        if (h.done == 3) break;
     }
+    if (exec) cudaGraphExecDestroy(exec);
     ev_record(ctx, 11);
     LSMPS_CUDA(cudaStreamSynchronize(s));
-    ps->iterations = total_inner;
-    ps->outer_iterations = outer;
+    ps->iterations = total;
+    ps->outer_iterations = updates;
+    ps->converged = converged && !nonfinite;
+    ps->fallback = fallback;
+    ps->solve_ms = ev_elapsed(ctx, 10, 11);
+}
+
+// Mixed precision (MIXED, and LEARNED): Jacobi-BiCGStab with FP64 vectors and recurrences
+// whose two SpMVs per iteration read the FP32 copy of A D^-1 (8 bytes per entry instead
+// of 12: the matrix is the bandwidth). The FP32 matrix perturbs each product at ~6e-8
+// relative, so the recursive residual drifts from the true one; whenever it has fallen by
+// `inner_tol` (default 0.1) since the last replacement, or the iteration stops, the true
+// residual b - A D^-1 y is recomputed with the FP64 matrix and replaces it, keeping the
+// search direction. Convergence is decided on that FP64 residual only. A breakdown, a
+// stall (LEARNED: no 1 % progress in `stall_window` iterations) or an FP32-driven
+// convergence claim the FP64 residual denies restarts the Krylov space from the current
+// iterate; LEARNED starts from the network's guess and, after a stall, continues as plain
+// Jacobi-BiCGStab (fallback).
+static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    Engine E = make_engine(ctx);
+    const double* dinv = ctx->A_dinv.get<double>();
+    const double* b = ctx->A_b.get<double>();
+    Vecs<double> V{ctx->vx.ensure<double>(U + 1), ctx->vr.ensure<double>(U + 1), ctx->vr0.ensure<double>(U + 1),
+                   ctx->vp.ensure<double>(U + 1), ctx->vv.ensure<double>(U + 1), ctx->vs.ensure<double>(U + 1),
+                   ctx->vt.ensure<double>(U + 1)};
+    const bool use_nn = learned && mpnn_ready(ctx);
+    const bool warm = o->warm_start && ctx->have_solution;
+    const double delta = o->inner_tol > 0 ? o->inner_tol : 0.1;
+    const int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
+    const int stall = o->stall_window > 0 ? o->stall_window : 20;
+    ev_record(ctx, 10);
+    Sell<double> As = sell_scaled64(ctx);
+    Sell<float> Af = sell_scaled32(ctx);
+    set_scalar_caps(E, o->max_iter, use_nn ? stall : 0);
+    bool have_start = warm;
+    if (warm) {  // the iteration works on y = D x
+        k_scale_by_diag<<<1184, 256, 0, s>>>(U, V.x, dinv);
+        LSMPS_CHECK_LAUNCH();
+    } else if (use_nn) {
+        float* rhs = ctx->fph.ensure<float>(U + 1);
+        float* yf = ctx->fx.ensure<float>(U + 1);
+        double* scal = engine_scalars(ctx);
+        k_norm2_one_block<<<1, 1024, 0, s>>>(U, b, scal);
+        k_rhs_unit<<<1184, 256, 0, s>>>(U, b, rhs, scal);  // network input: b / |b| in FP32
+        LSMPS_CHECK_LAUNCH();
+        mpnn_warm_start(ctx, rhs, yf);
+        k_y_from_net<<<1184, 256, 0, s>>>(U, yf, scal, V.x);  // y0 = |b| net(b / |b|)
+        LSMPS_CHECK_LAUNCH();
+        have_start = true;
+    } else {
+        LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
+    }
+    init<double, double>(E, As, b, V, have_start, o->tol, -1.0);
+    cudaGraphExec_t exec = nullptr;
+    if (o->use_graph) {
+        cudaGraph_t graph;
+        LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
+        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        LSMPS_CUDA(e);
+        LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        cudaGraphDestroy(graph);
+    }
+    auto read = [&](BcgScalars& h) {
+        LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, s));
+        LSMPS_CUDA(cudaStreamSynchronize(s));
+    };
+    BcgScalars h{};
+    read(h);
+    double rn_upd = h.rn;
+    int total = 0, base = 0, replacements = 0, restarts = 0, fallback = 0;
+    bool converged = h.done == 1, failed = h.done == 2 && h.nonfinite;
+    const long long max_chunks = (long long)o->max_iter / chunk + 4 + o->max_iter;  // bounded loop
+    for (long long guard = 0; !converged && !failed && guard < max_chunks; ++guard) {
+        if (!h.done) {
+            if (exec) {
+                LSMPS_CUDA(cudaGraphLaunch(exec, s));
+                note_launches(5 * (uint64_t)chunk);
+            } else {
+                for (int k = 0; k < chunk; ++k) iteration<double, float>(E, Af, V);
+                LSMPS_CHECK_LAUNCH();
+            }
+            read(h);
+        }
+        total += h.iters - base;
+        base = h.iters;
+        if (!h.done && h.rn > delta * rn_upd) continue;
+        const int why = h.done;  // 0: drop by delta; else the iteration stopped
+        if (why == 3 || total >= o->max_iter) {
+            // iteration cap: report the true residual of the last iterate
+            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P);
+            LSMPS_CHECK_LAUNCH();
+            read(h);
+            converged = h.done == 1;
+            break;
+        }
+        if (why == 0) {
+            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P);
+            LSMPS_CHECK_LAUNCH();
+            ++replacements;
+            read(h);
+            rn_upd = h.rn;
+            if (h.done == 1) { converged = true; break; }
+            if (h.done == 0) continue;
+            // rho breakdown after the replacement: fall through to a restart
+        }
+        if (why == 4 && use_nn) fallback = 1;
+        if (h.nonfinite) { failed = true; break; }
+        // restart from the current iterate with the FP64 matrix (true residual)
+        set_scalar_caps(E, o->max_iter - total, 0);
+        init<double, double>(E, As, b, V, true, o->tol, -1.0);
+        ++restarts;
+        read(h);
+        base = 0;
+        rn_upd = h.rn;
+        if (h.done == 1) { converged = true; break; }
+        if (h.done) { failed = true; break; }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    k_unscale<<<1184, 256, 0, s>>>(U, V.x, dinv);
+    LSMPS_CHECK_LAUNCH();
+    ev_record(ctx, 11);
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ps->iterations = total;
+    ps->outer_iterations = replacements + restarts;
     ps->converged = converged;
     ps->fallback = fallback;
     ps->solve_ms = ev_elapsed(ctx, 10, 11);
@@ -917,7 +1290,7 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
 
 void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out) {
     LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "PPE solve needs lsmps_ppe_assemble first");
-    LSMPS_REQUIRE(o && o->solver >= 0 && o->solver <= 4, LSMPS_ERR_ARG, "unknown solver");
+    LSMPS_REQUIRE(o && o->solver >= 0 && o->solver <= 5, LSMPS_ERR_ARG, "unknown solver");
     LSMPS_REQUIRE(o->solver != LSMPS_SOLVER_LEARNED || mpnn_ready(ctx), LSMPS_ERR_STATE,
                   "learned solver needs lsmps_mpnn_init / lsmps_mpnn_load first");
     lsmps_ppe_stats ps = ctx->ppe_assembly;
@@ -933,6 +1306,7 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
     } else {
         if (o->solver == LSMPS_SOLVER_FP64) solve_fast64(ctx, o, &ps, false);
         else if (o->solver == LSMPS_SOLVER_JACOBI) solve_fast64(ctx, o, &ps, true);
+        else if (o->solver == LSMPS_SOLVER_MIXED_F32) solve_mixed_f32(ctx, o, &ps, false);
         else solve_mixed(ctx, o, &ps, o->solver == LSMPS_SOLVER_LEARNED);
         // final statistics in FP64: |Ax - b|, |b|, error against p*
         cudaStream_t s = ctx->stream;

@@ -22,9 +22,10 @@ struct BcgScalars {
     unsigned int counter[8];  // last-block tickets of the reduction kernels
 };
 
-// A SELL-32 matrix view in the solver's numbering: rows in slices of 32, slice s holding
-// slen[s] entries per row stored column-major from sptr[s] (entry k of row 32 s + l at
-// sptr[s] + 32 k + l), zero-padded to its longest row.
+// A SELL-32x4 matrix view in the solver's numbering: rows in slices of 32, slice s holding
+// slen[s] (a multiple of 4) entries per row from sptr[s], in chunks of four consecutive
+// entries per row (entry k of row 32 s + l at sptr[s] + 128 (k / 4) + 4 l + k % 4),
+// zero-padded to its longest row.
 template <class T>
 struct Sell {
     long long n;

@@ -21,9 +21,9 @@ OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_GRID, ERR_OVERFLOW, ERR_NONFINI
 INTERIOR, FREE_SURFACE, SPLASH, NEAR_WALL, WALL = range(5)
 NBR_CLASSIFY = 1
 PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
-SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED = range(5)
+SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED, SOLVER_MIXED_F32 = range(6)
 KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS = range(5)
-SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4}
+SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4, "mixed_f32": 5}
 VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}
 
 REF_QUADRATIC = np.array([1, 2, -3, 0.5, 0.7, -0.2, 0.4, 0.3, -0.1, 0.25], dtype=np.float64)

@@ -20,10 +20,12 @@ KERNELS = {"spmv32": lib.KB_SPMV32, "spmv64": lib.KB_SPMV64, "nbr_count": lib.KB
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", choices=sorted(KERNELS), nargs="+", default=["spmv32"])
+    ap.add_argument("--kernel", choices=sorted(KERNELS), nargs="*", default=["spmv32"])
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--case", default="mixed")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--solve", choices=["fp64", "jacobi", "mixed", "learned"], default=None,
+                    help="also run one PPE solve to relative residual 1e-10")
     a = ap.parse_args()
     xyz, t, _ = lib.generate(None, case=a.case, particles=a.particles, l0=1.0, seed=7)
     with lib.Context(0) as ctx:
@@ -35,6 +37,10 @@ def main():
         for k in a.kernel:
             ms, nb = ctx.kernel_bench(KERNELS[k], a.reps)
             print(f"{k}: {ms * 1e3:.1f} us per launch, {nb / 1e6:.1f} MB algorithmic, {nb / ms / 1e6:.0f} GB/s")
+        if a.solve:
+            s = ctx.ppe_solve(a.solve, 20000, 1e-10)
+            print(f"solve {a.solve}: {s.solve_ms:.2f} ms, {s.iterations} iterations, {s.outer_iterations} sweeps, "
+                  f"relative L2 {s.relative_l2_error:.2e}")
 
 
 if __name__ == "__main__":

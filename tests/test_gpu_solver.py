@@ -56,9 +56,9 @@ def test_fast_fp64_solver_tracks_reference(ctx, golden, cfg_dir, name):
     assert abs(st.iterations - g["solve"]["iterations"]) <= max(3, 0.15 * g["solve"]["iterations"])
     assert st.final_residual <= p["ppe_tol"] * max(1.0, st.initial_residual) * 1.0000001
     # the pinned graph Laplacian is nearly singular: the error at the stopping residual is
-    # sensitive to rounding, so only its magnitude is compared
+    # sensitive to rounding, so it is only bounded by the reference's
     ref = g["solve"]["relative_l2_error"]["value"]
-    assert 0.5 * ref <= st.relative_l2_error <= 2.0 * ref
+    assert st.relative_l2_error <= 2.0 * ref
 
 
 @pytest.fixture(scope="module")
