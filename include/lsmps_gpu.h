@@ -173,8 +173,8 @@ typedef struct lsmps_solver_opts {
     double tol;              /* converged when |r| <= tol * max(1, |b|) (src/lsmps.cpp:67) */
     int32_t warm_start;      /* start from the last solution held by the context */
     int32_t use_graph;       /* capture the iteration in a CUDA graph (FP64 / JACOBI / MIXED) */
-    double inner_tol;        /* MIXED / LEARNED / MIXED_F32: residual drop between FP64 residual
-                                replacements (default 0.1) */
+    double inner_tol;        /* MIXED / LEARNED: residual drop between FP64 residual replacements
+                                (default 0.01); MIXED_F32: the same (default 0.1) */
     int32_t inner_max_iter;  /* reserved */
     int32_t stall_window;    /* LEARNED: iterations without progress before fallback (20) */
     int32_t check_every;     /* iterations between host convergence checks (default 8) */
