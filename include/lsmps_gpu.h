@@ -197,23 +197,52 @@ int lsmps_download_ppe(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, 
 /* Solution of the last solve (U, reference numbering). */
 int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
 
-/* ---- learned preconditioner (message-passing network over the neighbor graph) ----- */
+/* ---- manufactured right-hand sides ------------------------------------------------ */
+/* p* = c0 + sum_m a_m sin(kx_m x + ky_m y + kz_m z + phi_m) + gz z over the unknowns'
+ * particle positions, b = A p* (the reference's discrete manufactured solution,
+ * src/lsmps.cpp:59-61, with a caller-chosen smooth field). params: c0, gz, then nmodes x
+ * (a, kx, ky, kz, phi). No reference counterpart beyond the fixed p* of the variants. */
+int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
+
+/* ---- learned preconditioner (message-passing network over the PPE graph) ----------- */
+/* No reference counterpart. Nodes are the PPE unknowns, edges the
+ * off-diagonal entries with weight -a_ij / a_ii. Input features per node: residual
+ * (unit-norm residual times sqrt(U)), diagonal a_ii / mean(a) - 1, NearWall flag,
+ * row length / 32 - 1. Encoder 4 -> 64 (ReLU); three residual message-passing layers
+ * h += ReLU(W_l [h | sum_j w_ij h_j] + b_l), W_l 64 x 128; decoder 64 -> 1; output y / sqrt(U)
+ * is the guess for the Jacobi-scaled solution y = D A^-1 r of the unit residual r.
+ * Activations and weights BF16, accumulation FP32 (tensor-core mma). FP32 master weights
+ * in this order: W_enc[64][4], b_enc[64], 3 x (W_l[64][128], b_l[64]), w_dec[64], b_dec. */
+#define LSMPS_MPNN_HIDDEN 64
+#define LSMPS_MPNN_LAYERS 3
+#define LSMPS_MPNN_FEATURES 4
+size_t lsmps_mpnn_param_count(void);
+
 typedef struct lsmps_mpnn_train_opts {
-    int32_t steps;           /* optimiser steps on the samples added so far */
-    int32_t batch;           /* samples per step */
+    int32_t steps;           /* optimiser steps */
+    int32_t batch;           /* samples accumulated per step */
     float lr;                /* Adam learning rate */
-    float weight_decay;
-    uint32_t seed;
+    float weight_decay;      /* decoupled weight decay */
+    uint32_t seed;           /* sample order */
     int32_t reserved;
 } lsmps_mpnn_train_opts;
 
-/* Initialise the network (3 layers, hidden 64, BF16 weights) from a seed. */
+/* Initialise the weights from a seed (He-scaled normals; residual branches scaled down). */
 int lsmps_mpnn_init(lsmps_ctx* ctx, uint32_t seed);
-/* Add the current assembled system's (residual -> correction) training pair, using the
- * current solution as the target. */
+int lsmps_mpnn_get_weights(lsmps_ctx* ctx, float* w, size_t n);
+int lsmps_mpnn_set_weights(lsmps_ctx* ctx, const float* w, size_t n);
+/* Store a training pair from the current state: input b / |b| of the assembled system,
+ * target D x / |b| with x the last solution. The graph is stored once per assembly. */
 int lsmps_mpnn_add_sample(lsmps_ctx* ctx);
-/* Train on the stored samples; loss_out gets the final mean loss. */
+int lsmps_mpnn_clear_samples(lsmps_ctx* ctx);
+int lsmps_mpnn_sample_count(lsmps_ctx* ctx);
+/* Loss |y - t|^2 / |t|^2 of stored sample `index` and its gradient (FP32, parameter
+ * order above; grad may be NULL). */
+int lsmps_mpnn_grad(lsmps_ctx* ctx, int index, float* grad, float* loss);
+/* Adam on the stored samples; loss_out: mean loss of the last `batch` samples. */
 int lsmps_mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss_out);
+/* y = net(r) on the current assembled system (reference numbering, U entries each). */
+int lsmps_mpnn_infer(lsmps_ctx* ctx, const double* r, double* y);
 int lsmps_mpnn_save(lsmps_ctx* ctx, const char* path);
 int lsmps_mpnn_load(lsmps_ctx* ctx, const char* path);
 

@@ -102,7 +102,7 @@ int lsmps_ctx_create(int device, lsmps_ctx** out) {
         for (auto& e : ctx->ev) LSMPS_CUDA(cudaEventCreate(&e));
         int* f = ctx->dflags.ensure<int>(16);
         LSMPS_CUDA(cudaMemsetAsync(f, 0, 16 * sizeof(int), ctx->stream));
-        ctx->scratch.ensure<int>(256);
+        ctx->scratch.ensure<int>(4096);  // small device scalars (see the offsets at their uses)
         LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
     if (rc != LSMPS_OK) {
@@ -128,10 +128,10 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->A_dinvf, &ctx->A_cnt, &ctx->vx, &ctx->vr, &ctx->vr0, &ctx->vp, &ctx->vv,
                                  &ctx->vs, &ctx->vt, &ctx->vph, &ctx->vsh, &ctx->vtmp, &ctx->fx, &ctx->fr,
                                  &ctx->fr0, &ctx->fp, &ctx->fv, &ctx->fs, &ctx->ft, &ctx->fph, &ctx->fsh,
-                                 &ctx->red, &ctx->mpnn_w, &ctx->mpnn_m, &ctx->mpnn_v, &ctx->mpnn_g,
-                                 &ctx->mpnn_act, &ctx->mpnn_samples, &ctx->S_ptr, &ctx->S_len,
+                                 &ctx->red, &ctx->S_ptr, &ctx->S_len,
                                  &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf};
     for (auto* b : bufs) b->release();
+    mpnn_destroy(ctx);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -280,16 +280,47 @@ int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
     });
 }
 
+int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
+    return guarded(ctx, [&] { ppe_manufacture(ctx, params, nmodes); });
+}
+
+size_t lsmps_mpnn_param_count(void) { return mpnn_param_count(); }
+
 int lsmps_mpnn_init(lsmps_ctx* ctx, uint32_t seed) {
     return guarded(ctx, [&] { mpnn_init(ctx, seed); });
 }
+int lsmps_mpnn_get_weights(lsmps_ctx* ctx, float* w, size_t n) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(w, LSMPS_ERR_ARG, "null weight buffer");
+        mpnn_get_weights(ctx, w, n);
+    });
+}
+int lsmps_mpnn_set_weights(lsmps_ctx* ctx, const float* w, size_t n) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(w, LSMPS_ERR_ARG, "null weight buffer");
+        mpnn_set_weights(ctx, w, n);
+    });
+}
 int lsmps_mpnn_add_sample(lsmps_ctx* ctx) {
     return guarded(ctx, [&] { mpnn_add_sample(ctx); });
+}
+int lsmps_mpnn_clear_samples(lsmps_ctx* ctx) {
+    return guarded(ctx, [&] { mpnn_clear_samples(ctx); });
+}
+int lsmps_mpnn_sample_count(lsmps_ctx* ctx) { return ctx ? mpnn_sample_count(ctx) : 0; }
+int lsmps_mpnn_grad(lsmps_ctx* ctx, int index, float* grad, float* loss) {
+    return guarded(ctx, [&] { mpnn_grad(ctx, index, grad, loss); });
 }
 int lsmps_mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss_out) {
     return guarded(ctx, [&] {
         LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null training options");
         mpnn_train(ctx, opts, loss_out);
+    });
+}
+int lsmps_mpnn_infer(lsmps_ctx* ctx, const double* r, double* y) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(r && y, LSMPS_ERR_ARG, "null vectors");
+        mpnn_infer(ctx, r, y);
     });
 }
 int lsmps_mpnn_save(lsmps_ctx* ctx, const char* path) {

@@ -22,6 +22,10 @@
 
 #include "common.cuh"
 
+namespace lsmps_gpu {
+struct MpnnState;
+}
+
 struct lsmps_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -75,11 +79,9 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf fx, fr, fr0, fp, fv, fs, ft, fph, fsh;         // FP32 vectors
     lsmps_gpu::DevBuf red;                                           // reduction partials + scalars
 
-    // ---- learned preconditioner ----
-    lsmps_gpu::DevBuf mpnn_w, mpnn_m, mpnn_v, mpnn_g, mpnn_act, mpnn_samples;
-    bool have_mpnn = false;
-    int mpnn_nsamples = 0;
-    std::vector<float> mpnn_host_samples_meta;
+    // ---- learned preconditioner (weights, training store, workspace) ----
+    lsmps_gpu::MpnnState* mpnn = nullptr;
+    long long assembly_gen = 0;  // bumped by every PPE assembly
 
     void* pinned = nullptr;
     size_t pinned_bytes = 0;

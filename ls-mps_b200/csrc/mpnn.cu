@@ -1,21 +1,954 @@
-// Learned preconditioner: message-passing network over the particle neighbor graph.
-// (Placeholder until the network kernels land: reports "not ready".)
+// Learned preconditioner: a message-passing network over the PPE graph, trained and
+// evaluated on the GPU with BF16 weights / activations and FP32 accumulation on the
+// tensor cores (mma.sync m16n8k16 BF16; the 64x128 layer transform of a 16-node tile is
+// 64 MMAs, so the layer is bound by the neighbor gathers of the aggregation, not the MMA).
+//
+// Network (parameter order of lsmps_gpu.h): x_i = [r_i sqrt(U), a_ii / mean(a) - 1,
+// NearWall, row length / 32 - 1]; h0 = ReLU(W_enc x + b_enc); for l = 0..2:
+// m_i = sum_j w_ij h_j with w_ij = -a_ij / a_ii, h <- h + ReLU(W_l [h | m] + b_l);
+// y_i = (w_dec . h3_i + b_dec) / sqrt(U). Loss |y - t|^2 / |t|^2 with t = D x / |b| for the
+// input r = b / |b| (the Jacobi-scaled solution of the unit right-hand side).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
 #include "ops.cuh"
+#include "scan.cuh"
 
 namespace lsmps_gpu {
 
-bool mpnn_ready(lsmps_ctx* ctx) { return ctx->have_mpnn; }
+namespace {
+constexpr int H = 64, KIN = 128, NF = 4, NL = 3;
+constexpr int LDA = KIN + 8;  // padded shared-memory row of a [h | m] tile (bf16): conflict-free ldmatrix
+constexpr int LDG = H + 8;    // padded row of a 64-wide tile
+constexpr size_t OFF_WE = 0, OFF_BE = 256, OFF_L0 = 320, LSTRIDE = 8192 + 64;
+constexpr size_t OFF_WD = OFF_L0 + NL * LSTRIDE, OFF_BD = OFF_WD + 64, NPARAM = OFF_BD + 1;
+constexpr int WG_BLOCKS = 296;  // weight-gradient partial blocks (2 per SM)
+using bf16 = __nv_bfloat16;
+}  // namespace
 
-void mpnn_warm_start(lsmps_ctx*, const float*, float*) {
-    throw Error{LSMPS_ERR_STATE, "message-passing network not available"};
+struct MpnnGraph {
+    long long U = 0, nnz = 0;
+    DevBuf row, col, ew, feat;  // row/col copies (training store) or unused (inference view)
+    const int* prow = nullptr;
+    const int* pcol = nullptr;
+};
+
+struct MpnnSample {
+    int graph;
+    DevBuf r, t;  // float U: input b / |b|, target D x / |b|
+    double tnorm2;
+};
+
+struct MpnnState {
+    std::vector<float> w;  // FP32 master weights (host copy)
+    DevBuf dw, wbf, am, av, grad, gpart, red;
+    int adam_t = 0;
+    std::vector<std::unique_ptr<MpnnGraph>> graphs;
+    std::vector<std::unique_ptr<MpnnSample>> samples;
+    long long graph_gen = -1;  // assembly generation of graphs.back()
+    MpnnGraph infer;           // graph of the current system (inference)
+    long long infer_gen = -1;
+    long long cap = 0;         // workspace capacity (nodes)
+    DevBuf h[NL + 1], a[NL], z[NL + 1], y, gh[2], gam, gz;
+};
+
+namespace {
+
+// ---- tensor-core helpers (inline PTX) ------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned addr, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2(unsigned addr, unsigned& r0, unsigned& r1) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2_t(unsigned addr, unsigned& r0, unsigned& r1) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(addr));
+}
+// D = A (16x16 bf16, row) * B (16x8 bf16, col) + D, FP32 accumulate
+__device__ __forceinline__ void mma16816(float* d, unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b0,
+                                         unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-void mpnn_init(lsmps_ctx*, uint32_t) { throw Error{LSMPS_ERR_STATE, "message-passing network not available"}; }
-void mpnn_add_sample(lsmps_ctx*) { throw Error{LSMPS_ERR_STATE, "message-passing network not available"}; }
-void mpnn_train(lsmps_ctx*, const lsmps_mpnn_train_opts*, float*) {
-    throw Error{LSMPS_ERR_STATE, "message-passing network not available"};
+// A-operand address of a 16x16 tile at (row 0, col k0) of a row-major bf16 tile with row
+// stride ld (lanes 0-15: rows 0-15 at k0; lanes 16-31: rows 0-15 at k0 + 8)
+__device__ __forceinline__ unsigned a_addr(const bf16* tile, int ld, int k0, int lane) {
+    return smem_u32(tile + (lane & 15) * ld + k0 + ((lane >> 4) << 3));
 }
-void mpnn_save(lsmps_ctx*, const char*) { throw Error{LSMPS_ERR_STATE, "message-passing network not available"}; }
-void mpnn_load(lsmps_ctx*, const char*) { throw Error{LSMPS_ERR_STATE, "message-passing network not available"}; }
+
+// ---- graph construction from the assembled PPE ---------------------------------------
+__global__ void k_graph_ew(long long U, const int* __restrict__ row, const double* __restrict__ val,
+                           const double* __restrict__ dinv, float* __restrict__ ew) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    const int e0 = row[u], e1 = row[u + 1];
+    const double di = dinv[u];
+    for (int e = e0; e < e1 - 1; ++e) ew[e] = (float)(-val[e] * di);
+    ew[e1 - 1] = 0.f;  // the diagonal is the row's last entry
+}
+
+__global__ void k_mean_diag(long long U, const double* __restrict__ dinv, double* out) {
+    __shared__ double part[32];
+    double acc = 0;
+    for (long long i = threadIdx.x; i < U; i += blockDim.x) acc += dinv[i] != 0 ? 1.0 / dinv[i] : 1.0;
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+        *out = U ? t / (double)U : 1.0;
+    }
+}
+
+// feat[u] = [a_uu / mean - 1, NearWall, (row length - 1) / 32 - 1]
+__global__ void k_graph_feat(long long U, const int* __restrict__ row, const double* __restrict__ dinv,
+                             const uint8_t* __restrict__ cls, const int* __restrict__ sorted_of_u,
+                             const double* mean, float* __restrict__ feat) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    const double d = dinv[u] != 0 ? 1.0 / dinv[u] : 1.0;
+    feat[3 * u + 0] = (float)(d / *mean - 1.0);
+    feat[3 * u + 1] = cls[sorted_of_u[u]] == LSMPS_NEAR_WALL ? 1.f : 0.f;
+    feat[3 * u + 2] = (float)(row[u + 1] - row[u] - 1) / 32.f - 1.f;
+}
+
+// ---- forward ---------------------------------------------------------------------------
+struct GView {
+    long long U;
+    const int* row;
+    const int* col;
+    const float* ew;
+    const float* feat;
+    float sqrt_u;
+};
+
+__device__ __forceinline__ void features(const GView& G, const float* __restrict__ r, long long i, float x[NF]) {
+    x[0] = r[i] * G.sqrt_u;
+    x[1] = G.feat[3 * i];
+    x[2] = G.feat[3 * i + 1];
+    x[3] = G.feat[3 * i + 2];
+}
+
+// h0 = ReLU(W_enc x + b_enc) (CUDA cores: K = 4)
+__global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ r, const float* __restrict__ w,
+                                             bf16* __restrict__ h0, float* __restrict__ z0) {
+    __shared__ float sw[OFF_L0];
+    for (int k = threadIdx.x; k < (int)OFF_L0; k += blockDim.x) sw[k] = w[k];
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
+        float x[NF];
+        features(G, r, i, x);
+        for (int c8 = 0; c8 < H; c8 += 8) {
+            __align__(16) bf16 hv[8];
+            for (int q = 0; q < 8; ++q) {
+                const int c = c8 + q;
+                float zz = sw[OFF_BE + c];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zz += sw[OFF_WE + c * NF + f] * x[f];
+                if (z0) z0[i * H + c] = zz;
+                hv[q] = __float2bfloat16(fmaxf(zz, 0.f));
+            }
+            *reinterpret_cast<uint4*>(h0 + i * H + c8) = *reinterpret_cast<const uint4*>(hv);
+        }
+    }
+}
+
+// One message-passing layer, one warp per 16-node tile:
+//   1. aggregation m_i = sum_j w_ij h_j (each lane owns two of the 64 features; FP32),
+//      staged with h_i as the bf16 A tile [h | m] (16 x 128) in shared memory;
+//   2. z = [h | m] W^T on the tensor cores (8 k-steps x 8 n-tiles of m16n8k16);
+//   3. h_out = h + ReLU(z + b) (bf16), with [h | m] and z kept for the backward pass.
+__global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out,
+                                                   const bf16* __restrict__ Wl, const float* __restrict__ bl,
+                                                   bf16* __restrict__ a_save, float* __restrict__ z_save) {
+    __shared__ __align__(16) bf16 Ws[H * LDA];
+    __shared__ __align__(16) bf16 As[4][16 * LDA];
+    __shared__ float bs[H];
+    for (int k = threadIdx.x; k < H * KIN / 8; k += blockDim.x) {
+        const int n = k / (KIN / 8), c = (k % (KIN / 8)) * 8;
+        *reinterpret_cast<uint4*>(Ws + n * LDA + c) = *reinterpret_cast<const uint4*>(Wl + n * KIN + c);
+    }
+    if (threadIdx.x < H) bs[threadIdx.x] = bl[threadIdx.x];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    bf16* A = As[warp];
+    const long long ntiles = (G.U + 15) / 16;
+    for (long long tile = blockIdx.x * 4LL + warp; tile < ntiles; tile += gridDim.x * 4LL) {
+        const long long base = tile * 16;
+        for (int t = 0; t < 16; ++t) {
+            const long long i = base + t;
+            __nv_bfloat162 own = __floats2bfloat162_rn(0.f, 0.f);
+            float m0 = 0.f, m1 = 0.f;
+            if (i < G.U) {
+                own = *reinterpret_cast<const __nv_bfloat162*>(h_in + i * H + 2 * lane);
+                const int e0 = G.row[i], e1 = G.row[i + 1] - 1;  // the diagonal (last) has no edge
+                int e = e0;
+                for (; e + 2 <= e1; e += 2) {
+                    const int j0 = G.col[e], j1 = G.col[e + 1];
+                    const float w0 = G.ew[e], w1 = G.ew[e + 1];
+                    const float2 a0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)j0 * H + 2 * lane));
+                    const float2 a1 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)j1 * H + 2 * lane));
+                    m0 += w0 * a0.x + w1 * a1.x;
+                    m1 += w0 * a0.y + w1 * a1.y;
+                }
+                if (e < e1) {
+                    const float w0 = G.ew[e];
+                    const float2 a0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)G.col[e] * H + 2 * lane));
+                    m0 += w0 * a0.x;
+                    m1 += w0 * a0.y;
+                }
+            }
+            *reinterpret_cast<__nv_bfloat162*>(A + t * LDA + 2 * lane) = own;
+            *reinterpret_cast<__nv_bfloat162*>(A + t * LDA + H + 2 * lane) = __floats2bfloat162_rn(m0, m1);
+        }
+        __syncwarp();
+        float acc[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < KIN / 16; ++ks) {
+            unsigned a0, a1, a2, a3;
+            ldsm_x4(a_addr(A, LDA, ks * 16, lane), a0, a1, a2, a3);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                unsigned b0, b1;
+                // B (k x n) = W^T: rows n of Ws hold k contiguously -> non-transposed ldmatrix
+                ldsm_x2(smem_u32(Ws + (nt * 8 + (lane & 7)) * LDA + ks * 16 + ((lane >> 3) & 1) * 8), b0, b1);
+                mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int t = g + 8 * half;
+                const long long i = base + t;
+                if (i >= G.U) continue;
+                const int c = nt * 8 + 2 * tq;
+                const float z0 = acc[nt][2 * half] + bs[c], z1 = acc[nt][2 * half + 1] + bs[c + 1];
+                const float2 hold = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(A + t * LDA + c));
+                *reinterpret_cast<__nv_bfloat162*>(h_out + i * H + c) =
+                    __floats2bfloat162_rn(hold.x + fmaxf(z0, 0.f), hold.y + fmaxf(z1, 0.f));
+                if (z_save) *reinterpret_cast<float2*>(z_save + i * H + c) = make_float2(z0, z1);
+            }
+        }
+        if (a_save) {
+            for (int t = 0; t < 16; ++t) {
+                const long long i = base + t;
+                if (i < G.U)
+                    *reinterpret_cast<uint2*>(a_save + i * KIN + 4 * lane) =
+                        *reinterpret_cast<const uint2*>(A + t * LDA + 4 * lane);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// y_i = (w_dec . h3_i + b_dec) / sqrt(U)
+__global__ void k_dec(GView G, const bf16* __restrict__ h3, const float* __restrict__ w, float* __restrict__ y) {
+    __shared__ float sw[H + 1];
+    if (threadIdx.x <= H) sw[threadIdx.x] = w[OFF_WD + threadIdx.x];
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
+        float o = sw[H];
+        for (int c8 = 0; c8 < H; c8 += 8) {
+            uint4 q = *reinterpret_cast<const uint4*>(h3 + i * H + c8);
+            const bf16* hv = reinterpret_cast<const bf16*>(&q);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) o += sw[c8 + k] * __bfloat162float(hv[k]);
+        }
+        y[i] = o / G.sqrt_u;
+    }
+}
+
+// ---- loss and backward -------------------------------------------------------------------
+// |y - t|^2 into out[0] (one block, fixed order)
+__global__ void k_loss(long long U, const float* __restrict__ y, const float* __restrict__ t, double* out) {
+    __shared__ double part[32];
+    double acc = 0;
+    for (long long i = threadIdx.x; i < U; i += blockDim.x) {
+        const double d = (double)y[i] - (double)t[i];
+        acc += d * d;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += part[k];
+        out[0] = s;
+    }
+}
+
+// go_i = dL/dy_i / sqrt(U); gh3 = go w_dec; block partials of dw_dec (64) and db_dec (1)
+__global__ void __launch_bounds__(256) k_dec_bwd(GView G, const float* __restrict__ y, const float* __restrict__ t,
+                                                 float scale2, const bf16* __restrict__ h3,
+                                                 const float* __restrict__ w, float* __restrict__ gh3,
+                                                 float* __restrict__ part) {
+    __shared__ float sw[H];
+    __shared__ float sg[H + 1];
+    if (threadIdx.x < H) sw[threadIdx.x] = w[OFF_WD + threadIdx.x];
+    if (threadIdx.x <= H) sg[threadIdx.x] = 0.f;
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
+        const float go = scale2 * (y[i] - t[i]) / G.sqrt_u;
+        for (int c = 0; c < H; ++c) {
+            gh3[i * H + c] = go * sw[c];
+            atomicAdd(&sg[c], go * __bfloat162float(h3[i * H + c]));
+        }
+        atomicAdd(&sg[H], go);
+    }
+    __syncthreads();
+    if (threadIdx.x <= H) part[blockIdx.x * (H + 1) + threadIdx.x] = sg[threadIdx.x];
+}
+
+// Layer backward, part a (one warp per 16-node tile):
+//   gz = gh_next * (z > 0) (bf16, kept for the weight gradient), gA = gz W on the tensor
+//   cores (16 x 128: 16 n-tiles x 4 k-steps), gh_cur = gh_next + gA[:, :64], gam = gA[:, 64:];
+//   block partials of db.
+__global__ void __launch_bounds__(128) k_layer_bwd_a(GView G, const float* __restrict__ gh_next,
+                                                     const float* __restrict__ z, const bf16* __restrict__ Wl,
+                                                     bf16* __restrict__ gz_out, float* __restrict__ gh_cur,
+                                                     float* __restrict__ gam, float* __restrict__ bpart) {
+    __shared__ __align__(16) bf16 Ws[H * LDA];
+    __shared__ __align__(16) bf16 Gs[4][16 * LDG];
+    __shared__ float sb[H];
+    for (int k = threadIdx.x; k < H * KIN / 8; k += blockDim.x) {
+        const int n = k / (KIN / 8), c = (k % (KIN / 8)) * 8;
+        *reinterpret_cast<uint4*>(Ws + n * LDA + c) = *reinterpret_cast<const uint4*>(Wl + n * KIN + c);
+    }
+    if (threadIdx.x < H) sb[threadIdx.x] = 0.f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    bf16* Gt = Gs[warp];
+    float db0 = 0.f, db1 = 0.f;
+    const long long ntiles = (G.U + 15) / 16;
+    for (long long tile = blockIdx.x * 4LL + warp; tile < ntiles; tile += gridDim.x * 4LL) {
+        const long long base = tile * 16;
+        for (int t = 0; t < 16; ++t) {
+            const long long i = base + t;
+            float g0 = 0.f, g1 = 0.f;
+            if (i < G.U) {
+                const float2 gh = *reinterpret_cast<const float2*>(gh_next + i * H + 2 * lane);
+                const float2 zz = *reinterpret_cast<const float2*>(z + i * H + 2 * lane);
+                g0 = zz.x > 0.f ? gh.x : 0.f;
+                g1 = zz.y > 0.f ? gh.y : 0.f;
+            }
+            const __nv_bfloat162 gb = __floats2bfloat162_rn(g0, g1);
+            *reinterpret_cast<__nv_bfloat162*>(Gt + t * LDG + 2 * lane) = gb;
+            if (i < G.U) *reinterpret_cast<__nv_bfloat162*>(gz_out + i * H + 2 * lane) = gb;
+            db0 += g0;
+            db1 += g1;
+        }
+        __syncwarp();
+        float acc[16][4];
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < H / 16; ++ks) {
+            unsigned a0, a1, a2, a3;
+            ldsm_x4(a_addr(Gt, LDG, ks * 16, lane), a0, a1, a2, a3);
+#pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                unsigned b0, b1;
+                // B (k = out, n = in) = W (row-major [out][in]): transposed ldmatrix
+                ldsm_x2_t(smem_u32(Ws + (ks * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * LDA + nt * 8), b0, b1);
+                mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) {
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const long long i = base + g + 8 * half;
+                if (i >= G.U) continue;
+                const int c = nt * 8 + 2 * tq;
+                const float v0 = acc[nt][2 * half], v1 = acc[nt][2 * half + 1];
+                if (c < H) {
+                    const float2 gn = *reinterpret_cast<const float2*>(gh_next + i * H + c);
+                    *reinterpret_cast<float2*>(gh_cur + i * H + c) = make_float2(gn.x + v0, gn.y + v1);
+                } else {
+                    *reinterpret_cast<float2*>(gam + i * H + (c - H)) = make_float2(v0, v1);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    atomicAdd(&sb[2 * lane], db0);
+    atomicAdd(&sb[2 * lane + 1], db1);
+    __syncthreads();
+    if (threadIdx.x < H) bpart[blockIdx.x * H + threadIdx.x] = sb[threadIdx.x];
+}
+
+// Layer backward, part b: transposed aggregation gh[j] += w_ij gam[i] (one warp per node).
+__global__ void k_layer_bwd_agg(GView G, const float* __restrict__ gam, float* __restrict__ gh_cur) {
+    const int lane = threadIdx.x & 31;
+    for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < G.U;
+         i += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const float2 gm = *reinterpret_cast<const float2*>(gam + i * H + 2 * lane);
+        const int e1 = G.row[i + 1] - 1;
+        for (int e = G.row[i]; e < e1; ++e) {
+            const float w = G.ew[e];
+            float* dst = gh_cur + (long long)G.col[e] * H + 2 * lane;
+            atomicAdd(dst, w * gm.x);
+            atomicAdd(dst + 1, w * gm.y);
+        }
+    }
+}
+
+// Layer backward, part c: dW = gz^T [h | m] on the tensor cores. A block walks a range of
+// 16-node tiles; warp w owns output rows 16w..16w+15 (A operand = gz^T via a transposed
+// ldmatrix of the [node][out] tile) and all 128 inputs (B operand = [node][in] tile, a
+// transposed ldmatrix); 16 n-tiles x 4 accumulators per thread, written as a block partial.
+__global__ void __launch_bounds__(128) k_layer_bwd_w(GView G, const bf16* __restrict__ gz,
+                                                     const bf16* __restrict__ a_save, float* __restrict__ wpart) {
+    __shared__ __align__(16) bf16 Gs[16 * LDG];
+    __shared__ __align__(16) bf16 As[16 * LDA];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    float acc[16][4];
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    const long long ntiles = (G.U + 15) / 16;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long base = tile * 16;
+        __syncthreads();
+        // stage gz (16 x 64) and [h | m] (16 x 128) tiles; rows past U are zero
+        for (int k = threadIdx.x; k < 16 * (H / 8); k += blockDim.x) {
+            const int t = k / (H / 8), c = (k % (H / 8)) * 8;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (base + t < G.U) v = *reinterpret_cast<const uint4*>(gz + (base + t) * H + c);
+            *reinterpret_cast<uint4*>(Gs + t * LDG + c) = v;
+        }
+        for (int k = threadIdx.x; k < 16 * (KIN / 8); k += blockDim.x) {
+            const int t = k / (KIN / 8), c = (k % (KIN / 8)) * 8;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (base + t < G.U) v = *reinterpret_cast<const uint4*>(a_save + (base + t) * KIN + c);
+            *reinterpret_cast<uint4*>(As + t * LDA + c) = v;
+        }
+        __syncthreads();
+        // A (m = out, k = node) = gz^T: matrices (out 0-7 | 8-15) x (node 0-7 | 8-15) from Gs[node][out]
+        unsigned a0, a1, a2, a3;
+        {
+            const int mat = lane >> 3, r = lane & 7;
+            const int node = r + ((mat >> 1) << 3), out = warp * 16 + ((mat & 1) << 3);
+            ldsm_x4_t(smem_u32(Gs + node * LDG + out), a0, a1, a2, a3);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) {
+            unsigned b0, b1;
+            // B (k = node, n = in) from As[node][in]: transposed ldmatrix
+            ldsm_x2_t(smem_u32(As + ((lane & 7) + ((lane >> 3) & 1) * 8) * LDA + nt * 8), b0, b1);
+            mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+        }
+    }
+    float* out = wpart + (size_t)blockIdx.x * H * KIN;
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) {
+        const int c = nt * 8 + 2 * tq;
+        const int r0 = warp * 16 + g;
+        out[r0 * KIN + c] = acc[nt][0];
+        out[r0 * KIN + c + 1] = acc[nt][1];
+        out[(r0 + 8) * KIN + c] = acc[nt][2];
+        out[(r0 + 8) * KIN + c + 1] = acc[nt][3];
+    }
+}
+
+// Encoder backward: gz0 = gh0 * (z0 > 0); block partials of dW_enc (64 x 4) and db_enc.
+__global__ void __launch_bounds__(256) k_enc_bwd(GView G, const float* __restrict__ r, const float* __restrict__ gh0,
+                                                 const float* __restrict__ z0, float* __restrict__ part) {
+    __shared__ float sg[OFF_L0];
+    for (int k = threadIdx.x; k < (int)OFF_L0; k += blockDim.x) sg[k] = 0.f;
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
+        float x[NF];
+        features(G, r, i, x);
+        for (int c = 0; c < H; ++c) {
+            const float gz = z0[i * H + c] > 0.f ? gh0[i * H + c] : 0.f;
+            if (gz == 0.f) continue;
+            atomicAdd(&sg[OFF_BE + c], gz);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) atomicAdd(&sg[OFF_WE + c * NF + f], gz * x[f]);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < (int)OFF_L0; k += blockDim.x) part[(size_t)blockIdx.x * OFF_L0 + k] = sg[k];
+}
+
+// out[k] (+)= sum over nblk rows of part[b * stride + k], fixed order
+__global__ void k_reduce_part(const float* __restrict__ part, int nblk, int stride, int count, float* __restrict__ out,
+                              int accumulate) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    float s = 0.f;
+    for (int b = 0; b < nblk; ++b) s += part[(size_t)b * stride + k];
+    out[k] = accumulate ? out[k] + s : s;
+}
+
+// Adam with decoupled weight decay on the FP32 master weights; refreshes the bf16 copies
+// of the layer matrices.
+__global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float wd, float b1, float b2, float c1, float c2,
+                       float inv_batch, bf16* __restrict__ wbf) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float gk = g[k] * inv_batch;
+    m[k] = b1 * m[k] + (1.f - b1) * gk;
+    v[k] = b2 * v[k] + (1.f - b2) * gk * gk;
+    const float mh = m[k] / c1, vh = v[k] / c2;
+    w[k] -= lr * (mh / (sqrtf(vh) + 1e-8f) + wd * w[k]);
+    const long long off = (long long)k - (long long)OFF_L0;
+    if (off >= 0 && off < (long long)(NL * LSTRIDE)) {
+        const int l = (int)(off / LSTRIDE), q = (int)(off % LSTRIDE);
+        if (q < H * KIN) wbf[l * H * KIN + q] = __float2bfloat16(w[k]);
+    }
+}
+
+__global__ void k_w_to_bf16(const float* __restrict__ w, bf16* __restrict__ wbf) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= NL * H * KIN) return;
+    const int l = k / (H * KIN), q = k % (H * KIN);
+    wbf[k] = __float2bfloat16(w[OFF_L0 + l * LSTRIDE + q]);
+}
+
+// sample input b / |b| and target D x / |b| (float), |b|^2 in *nb2
+__global__ void k_norm2_d(long long U, const double* __restrict__ b, double* out) {
+    __shared__ double part[32];
+    double acc = 0;
+    for (long long i = threadIdx.x; i < U; i += blockDim.x) acc += b[i] * b[i];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += part[k];
+        *out = s;
+    }
+}
+
+__global__ void k_make_sample(long long U, const double* __restrict__ b, const double* __restrict__ x,
+                              const double* __restrict__ dinv, const double* nb2, float* __restrict__ r,
+                              float* __restrict__ t) {
+    const double inv = *nb2 > 0 ? 1.0 / sqrt(*nb2) : 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < U; i += (long long)gridDim.x * blockDim.x) {
+        r[i] = (float)(b[i] * inv);
+        t[i] = (float)(x[i] / dinv[i] * inv);
+    }
+}
+
+__global__ void k_d2f(long long n, const double* __restrict__ a, const int* __restrict__ map, float* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[map ? map[i] : i] = (float)a[i];
+}
+
+__global__ void k_f2d_ref(long long n, const float* __restrict__ a, const int* __restrict__ u_of_ref, double* __restrict__ out) {
+    for (long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x; rr < n; rr += (long long)gridDim.x * blockDim.x)
+        out[rr] = (double)a[u_of_ref[rr]];
+}
+
+// ---- manufactured fields ----
+__global__ void k_manufacture(long long U, const int* __restrict__ sorted_of_u, const double* __restrict__ sx,
+                              const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ prm,
+                              int nmodes, double* __restrict__ xe) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < U; u += (long long)gridDim.x * blockDim.x) {
+        const int k = sorted_of_u[u];
+        const double x = sx[k], y = sy[k], z = sz[k];
+        double p = prm[0] + prm[1] * z;
+        for (int m = 0; m < nmodes; ++m) {
+            const double* q = prm + 2 + 5 * m;
+            p += q[0] * sin(q[1] * x + q[2] * y + q[3] * z + q[4]);
+        }
+        xe[u] = p;
+    }
+}
+
+__global__ void k_rhs(long long U, const int* __restrict__ row, const int* __restrict__ col,
+                      const double* __restrict__ val, const double* __restrict__ xe, double* __restrict__ b) {
+    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    double s = 0;
+    for (int e = row[u]; e < row[u + 1]; ++e) s += val[e] * xe[col[e]];
+    b[u] = s;
+}
+
+}  // namespace
+
+// =========================================================================================
+// host side
+// =========================================================================================
+static MpnnState& state(lsmps_ctx* ctx) {
+    LSMPS_REQUIRE(ctx->mpnn != nullptr, LSMPS_ERR_STATE, "message-passing network not initialised");
+    return *ctx->mpnn;
+}
+
+bool mpnn_ready(lsmps_ctx* ctx) { return ctx->mpnn != nullptr; }
+
+void mpnn_destroy(lsmps_ctx* ctx) {
+    delete ctx->mpnn;
+    ctx->mpnn = nullptr;
+}
+
+static void upload_weights(lsmps_ctx* ctx, MpnnState& S) {
+    float* dw = S.dw.ensure<float>(NPARAM);
+    LSMPS_CUDA(cudaMemcpyAsync(dw, S.w.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    bf16* wbf = S.wbf.ensure<bf16>(NL * H * KIN);
+    k_w_to_bf16<<<blocks_for(NL * H * KIN, 256), 256, 0, ctx->stream>>>(dw, wbf);
+    LSMPS_CHECK_LAUNCH();
+}
+
+void mpnn_init(lsmps_ctx* ctx, uint32_t seed) {
+    if (!ctx->mpnn) ctx->mpnn = new MpnnState();
+    MpnnState& S = *ctx->mpnn;
+    S.w.assign(NPARAM, 0.f);
+    std::mt19937 rng(seed);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    for (int c = 0; c < H * NF; ++c) S.w[OFF_WE + c] = nd(rng) * std::sqrt(2.f / NF);
+    for (int l = 0; l < NL; ++l)
+        for (int c = 0; c < H * KIN; ++c) S.w[OFF_L0 + l * LSTRIDE + c] = 0.5f * nd(rng) * std::sqrt(2.f / KIN);
+    for (int c = 0; c < H; ++c) S.w[OFF_WD + c] = nd(rng) * std::sqrt(1.f / H);
+    S.adam_t = 0;
+    S.am.ensure<float>(NPARAM);
+    S.av.ensure<float>(NPARAM);
+    LSMPS_CUDA(cudaMemsetAsync(S.am.get<float>(), 0, NPARAM * sizeof(float), ctx->stream));
+    LSMPS_CUDA(cudaMemsetAsync(S.av.get<float>(), 0, NPARAM * sizeof(float), ctx->stream));
+    upload_weights(ctx, S);
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void mpnn_get_weights(lsmps_ctx* ctx, float* w, size_t n) {
+    MpnnState& S = state(ctx);
+    LSMPS_REQUIRE(n == NPARAM, LSMPS_ERR_ARG, "weight buffer size differs from lsmps_mpnn_param_count()");
+    LSMPS_CUDA(cudaMemcpyAsync(S.w.data(), S.dw.get<float>(), NPARAM * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(w, S.w.data(), NPARAM * sizeof(float));
+}
+
+void mpnn_set_weights(lsmps_ctx* ctx, const float* w, size_t n) {
+    if (!ctx->mpnn) mpnn_init(ctx, 0);
+    MpnnState& S = *ctx->mpnn;
+    LSMPS_REQUIRE(n == NPARAM, LSMPS_ERR_ARG, "weight buffer size differs from lsmps_mpnn_param_count()");
+    S.w.assign(w, w + NPARAM);
+    upload_weights(ctx, S);
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// Edge weights and node features of the current assembled system into g.
+static void build_graph(lsmps_ctx* ctx, MpnnGraph& g, bool copy_structure) {
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U, nnz = ctx->nnz;
+    g.U = U;
+    g.nnz = nnz;
+    if (copy_structure) {
+        int* row = g.row.ensure<int>(U + 1);
+        int* col = g.col.ensure<int>(nnz + 1);
+        LSMPS_CUDA(cudaMemcpyAsync(row, ctx->A_row.get<int>(), (U + 1) * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        LSMPS_CUDA(cudaMemcpyAsync(col, ctx->A_col.get<int>(), nnz * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        g.prow = row;
+        g.pcol = col;
+    } else {
+        g.prow = ctx->A_row.get<int>();
+        g.pcol = ctx->A_col.get<int>();
+    }
+    float* ew = g.ew.ensure<float>(nnz + 1);
+    float* feat = g.feat.ensure<float>(3 * U + 3);
+    double* mean = ctx->scratch.get<double>() + 24;
+    if (U) {
+        k_graph_ew<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_val.get<double>(),
+                                                     ctx->A_dinv.get<double>(), ew);
+        k_mean_diag<<<1, 1024, 0, s>>>(U, ctx->A_dinv.get<double>(), mean);
+        k_graph_feat<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_dinv.get<double>(),
+                                                       ctx->cls.get<uint8_t>(), ctx->sorted_of_u.get<int>(), mean, feat);
+        LSMPS_CHECK_LAUNCH();
+    }
+}
+
+static GView view(const MpnnGraph& g) {
+    return GView{g.U, g.prow, g.pcol, g.ew.get<float>(), g.feat.get<float>(), (float)std::sqrt((double)std::max(1LL, g.U))};
+}
+
+static void ensure_workspace(MpnnState& S, long long U, bool training) {
+    if (U <= S.cap && (!training || S.z[0].bytes >= (size_t)U * H * sizeof(float))) return;
+    const long long cap = std::max(U, S.cap);
+    for (int l = 0; l <= NL; ++l) S.h[l].ensure<bf16>(cap * H + 8);
+    S.y.ensure<float>(cap + 8);
+    if (training) {
+        for (int l = 0; l < NL; ++l) S.a[l].ensure<bf16>(cap * KIN + 8);
+        for (int l = 0; l <= NL; ++l) S.z[l].ensure<float>(cap * H + 8);
+        S.gh[0].ensure<float>(cap * H + 8);
+        S.gh[1].ensure<float>(cap * H + 8);
+        S.gam.ensure<float>(cap * H + 8);
+        S.gz.ensure<bf16>(cap * H + 8);
+    }
+    S.cap = cap;
+}
+
+// Forward pass over graph g for input r (float, unit norm); y in S.y.
+static void forward(lsmps_ctx* ctx, MpnnState& S, const GView& G, const float* r, bool training) {
+    cudaStream_t s = ctx->stream;
+    ensure_workspace(S, G.U, training);
+    if (!G.U) return;
+    const float* w = S.dw.get<float>();
+    const bf16* wbf = S.wbf.get<bf16>();
+    const unsigned grid = std::min<unsigned>(blocks_for(G.U, 256), 148 * 8);
+    k_enc<<<grid, 256, 0, s>>>(G, r, w, S.h[0].get<bf16>(), training ? S.z[0].get<float>() : nullptr);
+    LSMPS_CHECK_LAUNCH();
+    const unsigned lgrid = std::min<unsigned>((unsigned)((G.U + 63) / 64), 148 * 4);
+    for (int l = 0; l < NL; ++l) {
+        k_layer_fwd<<<lgrid, 128, 0, s>>>(G, S.h[l].get<bf16>(), S.h[l + 1].get<bf16>(), wbf + l * H * KIN,
+                                          w + OFF_L0 + l * LSTRIDE + H * KIN,
+                                          training ? S.a[l].get<bf16>() : nullptr,
+                                          training ? S.z[l + 1].get<float>() : nullptr);
+        LSMPS_CHECK_LAUNCH();
+    }
+    k_dec<<<grid, 256, 0, s>>>(G, S.h[NL].get<bf16>(), w, S.y.get<float>());
+    LSMPS_CHECK_LAUNCH();
+}
+
+// Loss of (g, r, t) and, when grad != nullptr, its gradient accumulated into grad (device).
+static double loss_and_grad(lsmps_ctx* ctx, MpnnState& S, const GView& G, const float* r, const float* t, double tnorm2,
+                            float* grad, bool accumulate) {
+    cudaStream_t s = ctx->stream;
+    forward(ctx, S, G, r, grad != nullptr);
+    double* lsum = S.red.ensure<double>(8);
+    k_loss<<<1, 1024, 0, s>>>(G.U, S.y.get<float>(), t, lsum);
+    LSMPS_CHECK_LAUNCH();
+    if (grad) {
+        const float* w = S.dw.get<float>();
+        const bf16* wbf = S.wbf.get<bf16>();
+        const int nb = 148 * 2;
+        float* part = S.gpart.ensure<float>((size_t)WG_BLOCKS * H * KIN + 16);
+        float* gh_next = S.gh[0].get<float>();
+        float* gh_cur = S.gh[1].get<float>();
+        // decoder
+        k_dec_bwd<<<nb, 256, 0, s>>>(G, S.y.get<float>(), t, (float)(2.0 / std::max(tnorm2, 1e-30)),
+                                     S.h[NL].get<bf16>(), w, gh_next, part);
+        LSMPS_CHECK_LAUNCH();
+        k_reduce_part<<<1, H + 1, 0, s>>>(part, nb, H + 1, H + 1, grad + OFF_WD, accumulate ? 1 : 0);
+        LSMPS_CHECK_LAUNCH();
+        const unsigned lgrid = std::min<unsigned>((unsigned)((G.U + 63) / 64), 148 * 4);
+        for (int l = NL - 1; l >= 0; --l) {
+            float* bpart = part;  // [lgrid][64]
+            k_layer_bwd_a<<<lgrid, 128, 0, s>>>(G, gh_next, S.z[l + 1].get<float>(), wbf + l * H * KIN,
+                                                S.gz.get<bf16>(), gh_cur, S.gam.get<float>(), bpart);
+            LSMPS_CHECK_LAUNCH();
+            k_reduce_part<<<1, H, 0, s>>>(bpart, (int)lgrid, H, H, grad + OFF_L0 + l * LSTRIDE + H * KIN,
+                                          accumulate ? 1 : 0);
+            LSMPS_CHECK_LAUNCH();
+            k_layer_bwd_agg<<<std::min<unsigned>(blocks_for(G.U * 32, 256), 148 * 16), 256, 0, s>>>(
+                G, S.gam.get<float>(), gh_cur);
+            LSMPS_CHECK_LAUNCH();
+            k_layer_bwd_w<<<WG_BLOCKS, 128, 0, s>>>(G, S.gz.get<bf16>(), S.a[l].get<bf16>(), part);
+            LSMPS_CHECK_LAUNCH();
+            k_reduce_part<<<blocks_for(H * KIN, 256), 256, 0, s>>>(part, WG_BLOCKS, H * KIN, H * KIN,
+                                                                   grad + OFF_L0 + l * LSTRIDE, accumulate ? 1 : 0);
+            LSMPS_CHECK_LAUNCH();
+            std::swap(gh_next, gh_cur);
+        }
+        // encoder (gh_next holds dL/dh0)
+        k_enc_bwd<<<nb, 256, 0, s>>>(G, r, gh_next, S.z[0].get<float>(), part);
+        LSMPS_CHECK_LAUNCH();
+        k_reduce_part<<<blocks_for(OFF_L0, 256), 256, 0, s>>>(part, nb, (int)OFF_L0, (int)OFF_L0, grad, accumulate ? 1 : 0);
+        LSMPS_CHECK_LAUNCH();
+    }
+    double h;
+    LSMPS_CUDA(cudaMemcpyAsync(&h, lsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    return h / std::max(tnorm2, 1e-30);
+}
+
+void mpnn_add_sample(lsmps_ctx* ctx) {
+    MpnnState& S = state(ctx);
+    LSMPS_REQUIRE(ctx->have_ppe && ctx->have_solution, LSMPS_ERR_STATE, "a training pair needs a solved system");
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    if (S.graph_gen != ctx->assembly_gen || S.graphs.empty()) {
+        S.graphs.emplace_back(new MpnnGraph());
+        build_graph(ctx, *S.graphs.back(), true);
+        S.graph_gen = ctx->assembly_gen;
+    }
+    auto smp = std::make_unique<MpnnSample>();
+    smp->graph = (int)S.graphs.size() - 1;
+    float* r = smp->r.ensure<float>(U + 1);
+    float* t = smp->t.ensure<float>(U + 1);
+    double* nb2 = ctx->scratch.get<double>() + 28;
+    k_norm2_d<<<1, 1024, 0, s>>>(U, ctx->A_b.get<double>(), nb2);
+    k_make_sample<<<1184, 256, 0, s>>>(U, ctx->A_b.get<double>(), ctx->vx.get<double>(), ctx->A_dinv.get<double>(),
+                                        nb2, r, t);
+    LSMPS_CHECK_LAUNCH();
+    // |t|^2 (for the relative loss), host-side from a small download-free reduction
+    double* tn = S.red.ensure<double>(8) + 1;
+    // reuse k_loss with y = 0: sum (0 - t)^2
+    float* zero = S.y.ensure<float>(std::max<long long>(U + 8, S.cap + 8));
+    LSMPS_CUDA(cudaMemsetAsync(zero, 0, (U + 1) * sizeof(float), s));
+    k_loss<<<1, 1024, 0, s>>>(U, zero, t, tn);
+    LSMPS_CHECK_LAUNCH();
+    LSMPS_CUDA(cudaMemcpyAsync(&smp->tnorm2, tn, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    S.samples.push_back(std::move(smp));
+}
+
+void mpnn_clear_samples(lsmps_ctx* ctx) {
+    MpnnState& S = state(ctx);
+    S.samples.clear();
+    S.graphs.clear();
+    S.graph_gen = -1;
+}
+
+int mpnn_sample_count(lsmps_ctx* ctx) { return ctx->mpnn ? (int)ctx->mpnn->samples.size() : 0; }
+
+void mpnn_grad(lsmps_ctx* ctx, int index, float* grad_host, float* loss) {
+    MpnnState& S = state(ctx);
+    LSMPS_REQUIRE(index >= 0 && index < (int)S.samples.size(), LSMPS_ERR_ARG, "sample index out of range");
+    const MpnnSample& smp = *S.samples[index];
+    float* grad = S.grad.ensure<float>(NPARAM);
+    const double L = loss_and_grad(ctx, S, view(*S.graphs[smp.graph]), smp.r.get<float>(), smp.t.get<float>(),
+                                   smp.tnorm2, grad, false);
+    if (loss) *loss = (float)L;
+    if (grad_host) {
+        LSMPS_CUDA(cudaMemcpyAsync(grad_host, grad, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+void mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* o, float* loss_out) {
+    MpnnState& S = state(ctx);
+    LSMPS_REQUIRE(!S.samples.empty(), LSMPS_ERR_STATE, "no training samples");
+    LSMPS_REQUIRE(o->steps >= 0 && o->batch >= 1, LSMPS_ERR_ARG, "training options");
+    cudaStream_t s = ctx->stream;
+    float* grad = S.grad.ensure<float>(NPARAM);
+    std::mt19937 rng(o->seed);
+    std::vector<int> order(S.samples.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    size_t cursor = order.size();
+    double last = 0;
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (int step = 0; step < o->steps; ++step) {
+        double sum = 0;
+        for (int k = 0; k < o->batch; ++k) {
+            if (cursor >= order.size()) {
+                std::shuffle(order.begin(), order.end(), rng);
+                cursor = 0;
+            }
+            const MpnnSample& smp = *S.samples[order[cursor++]];
+            sum += loss_and_grad(ctx, S, view(*S.graphs[smp.graph]), smp.r.get<float>(), smp.t.get<float>(), smp.tnorm2,
+                                 grad, k > 0);
+        }
+        ++S.adam_t;
+        const float c1 = 1.f - std::pow(b1, (float)S.adam_t), c2 = 1.f - std::pow(b2, (float)S.adam_t);
+        k_adam<<<blocks_for(NPARAM, 256), 256, 0, s>>>((int)NPARAM, S.dw.get<float>(), grad, S.am.get<float>(),
+                                                       S.av.get<float>(), o->lr, o->weight_decay, b1, b2, c1, c2,
+                                                       1.f / (float)o->batch, S.wbf.get<bf16>());
+        LSMPS_CHECK_LAUNCH();
+        last = sum / o->batch;
+    }
+    LSMPS_CUDA(cudaMemcpyAsync(S.w.data(), S.dw.get<float>(), NPARAM * sizeof(float), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    if (loss_out) *loss_out = (float)last;
+}
+
+// Network guess for the current assembled system: y = net(rhs) (sorted numbering, float).
+void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y) {
+    MpnnState& S = state(ctx);
+    if (S.infer_gen != ctx->assembly_gen) {
+        build_graph(ctx, S.infer, false);
+        S.infer_gen = ctx->assembly_gen;
+    }
+    GView G = view(S.infer);
+    forward(ctx, S, G, rhs, false);
+    LSMPS_CUDA(cudaMemcpyAsync(y, S.y.get<float>(), G.U * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+void mpnn_infer(lsmps_ctx* ctx, const double* r_ref, double* y_ref) {
+    state(ctx);
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "inference needs an assembled system");
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    double* rd = ctx->vtmp.ensure<double>(2 * U + 2);
+    float* rf = ctx->fph.ensure<float>(U + 1);
+    float* yf = ctx->fx.ensure<float>(U + 1);
+    LSMPS_CUDA(cudaMemcpyAsync(rd, r_ref, U * sizeof(double), cudaMemcpyHostToDevice, s));
+    // reference numbering -> solver numbering: rf[u_of_ref[rr]] = r[rr]
+    k_d2f<<<1184, 256, 0, s>>>(U, rd, ctx->u_of_ref.get<int>(), rf);
+    LSMPS_CHECK_LAUNCH();
+    mpnn_warm_start(ctx, rf, yf);
+    k_f2d_ref<<<1184, 256, 0, s>>>(U, yf, ctx->u_of_ref.get<int>(), rd + U);
+    LSMPS_CHECK_LAUNCH();
+    LSMPS_CUDA(cudaMemcpyAsync(y_ref, rd + U, U * sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+}
+
+void mpnn_save(lsmps_ctx* ctx, const char* path) {
+    MpnnState& S = state(ctx);
+    std::vector<float> w(NPARAM);
+    mpnn_get_weights(ctx, w.data(), NPARAM);
+    FILE* f = std::fopen(path, "wb");
+    LSMPS_REQUIRE(f, LSMPS_ERR_IO, std::string("cannot write ") + path);
+    const char magic[8] = {'L', 'S', 'M', 'P', 'N', 'N', '0', '1'};
+    const uint64_t n = NPARAM;
+    bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&n, sizeof(n), 1, f) == 1 &&
+              std::fwrite(w.data(), sizeof(float), NPARAM, f) == NPARAM;
+    std::fclose(f);
+    (void)S;
+    LSMPS_REQUIRE(ok, LSMPS_ERR_IO, std::string("short write to ") + path);
+}
+
+void mpnn_load(lsmps_ctx* ctx, const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    LSMPS_REQUIRE(f, LSMPS_ERR_IO, std::string("cannot read ") + path);
+    char magic[8];
+    uint64_t n = 0;
+    std::vector<float> w(NPARAM);
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "LSMPNN01", 8) == 0 &&
+              std::fread(&n, sizeof(n), 1, f) == 1 && n == NPARAM &&
+              std::fread(w.data(), sizeof(float), NPARAM, f) == NPARAM;
+    std::fclose(f);
+    LSMPS_REQUIRE(ok, LSMPS_ERR_IO, std::string("not a network weights file: ") + path);
+    mpnn_set_weights(ctx, w.data(), NPARAM);
+}
+
+size_t mpnn_param_count() { return NPARAM; }
+
+void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "manufactured fields need an assembled system");
+    LSMPS_REQUIRE(params && nmodes >= 0 && nmodes <= 64, LSMPS_ERR_ARG, "manufactured field parameters");
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    const int np = 2 + 5 * nmodes;
+    double* prm = ctx->scratch.get<double>() + 64;  // 512-double scratch region
+    LSMPS_CUDA(cudaMemcpyAsync(prm, params, np * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (U) {
+        k_manufacture<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), ctx->sx.get<double>(), ctx->sy.get<double>(),
+                                           ctx->sz.get<double>(), prm, nmodes, ctx->A_xexact.get<double>());
+        k_rhs<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>(),
+                                                 ctx->A_xexact.get<double>(), ctx->A_b.get<double>());
+        LSMPS_CHECK_LAUNCH();
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ctx->have_solution = false;
+}
 
 }  // namespace lsmps_gpu

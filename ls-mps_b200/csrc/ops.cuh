@@ -25,11 +25,22 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* o
 void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
 
 // mpnn.cu
+bool mpnn_ready(lsmps_ctx* ctx);
+void mpnn_destroy(lsmps_ctx* ctx);
+size_t mpnn_param_count();
 void mpnn_init(lsmps_ctx* ctx, uint32_t seed);
+void mpnn_get_weights(lsmps_ctx* ctx, float* w, size_t n);
+void mpnn_set_weights(lsmps_ctx* ctx, const float* w, size_t n);
 void mpnn_add_sample(lsmps_ctx* ctx);
+void mpnn_clear_samples(lsmps_ctx* ctx);
+int mpnn_sample_count(lsmps_ctx* ctx);
+void mpnn_grad(lsmps_ctx* ctx, int index, float* grad, float* loss);
 void mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss);
+void mpnn_infer(lsmps_ctx* ctx, const double* r, double* y);
+void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y);
 void mpnn_save(lsmps_ctx* ctx, const char* path);
 void mpnn_load(lsmps_ctx* ctx, const char* path);
+void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
 
 // Profiling hooks behind lsmps_kernel_bench (mean ms per launch, algorithmic bytes).
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);

@@ -335,6 +335,7 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     ctx->ppe_variant = o->variant;
     ctx->have_ppe = true;
     ctx->have_solution = false;
+    ctx->assembly_gen += 1;
     ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = false;
     ctx->ppe_assembly = ps;
     if (out) *out = ps;

@@ -31,8 +31,6 @@
 
 namespace lsmps_gpu {
 
-void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y);  // mpnn.cu
-bool mpnn_ready(lsmps_ctx* ctx);
 
 namespace {
 
@@ -510,6 +508,7 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restr
         if (threadIdx.x == 0) {
             S->counter[4] = 0;
             double bnorm = bnorm_override >= 0 ? bnorm_override : sqrt(bb);
+            S->bnorm = sqrt(bb);
             S->thresh = tol * fmax(1.0, bnorm);
             S->rho0 = S->alpha = S->omega = 1.0;
             S->rho = rr;
@@ -1227,8 +1226,16 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     };
     BcgScalars h{};
     read(h);
-    double rn_upd = h.rn;
     int total = 0, base = 0, replacements = 0, restarts = 0, fallback = 0;
+    if (use_nn && !warm && (!std::isfinite(h.rn) || h.rn >= h.bnorm)) {
+        // the network's guess is worse than zero: discard it and run plain Jacobi-BiCGStab
+        fallback = 1;
+        LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
+        set_scalar_caps(E, o->max_iter, 0);
+        init<double, double>(E, As, b, V, false, o->tol, -1.0);
+        read(h);
+    }
+    double rn_upd = h.rn;
     bool converged = h.done == 1, failed = h.done == 2 && h.nonfinite;
     const long long max_chunks = (long long)o->max_iter / chunk + 4 + o->max_iter;  // bounded loop
     for (long long guard = 0; !converged && !failed && guard < max_chunks; ++guard) {

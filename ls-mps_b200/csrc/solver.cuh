@@ -12,6 +12,7 @@ struct BcgScalars {
     double sn, rn;        // last |s| and |r|
     double tt;
     double best_rn;       // smallest |r| seen (stall detection)
+    double bnorm;         // |b| of the run (set by the init kernel)
     int done;             // 0 running, 1 converged, 2 breakdown, 3 iteration cap, 4 stalled
     int s_conv;           // |s| test passed this iteration
     int iters;            // completed iterations (reference bookkeeping)

@@ -109,9 +109,17 @@ SIGNATURES = {
     "lsmps_download_wls": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "lsmps_download_ppe": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
+    "lsmps_mpnn_param_count": (C.c_size_t, []),
     "lsmps_mpnn_init": (C.c_int, [_vp, C.c_uint32]),
+    "lsmps_mpnn_get_weights": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_mpnn_set_weights": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_mpnn_add_sample": (C.c_int, [_vp]),
+    "lsmps_mpnn_clear_samples": (C.c_int, [_vp]),
+    "lsmps_mpnn_sample_count": (C.c_int, [_vp]),
+    "lsmps_mpnn_grad": (C.c_int, [_vp, C.c_int, _vp, C.POINTER(C.c_float)]),
     "lsmps_mpnn_train": (C.c_int, [_vp, C.POINTER(MpnnTrainOpts), C.POINTER(C.c_float)]),
+    "lsmps_mpnn_infer": (C.c_int, [_vp, _vp, _vp]),
     "lsmps_mpnn_save": (C.c_int, [_vp, C.c_char_p]),
     "lsmps_mpnn_load": (C.c_int, [_vp, C.c_char_p]),
     "lsmps_host_generate": (C.c_int, [C.c_char_p, C.c_char_p, _vp, _vp, _vp, C.POINTER(C.c_size_t)]),
@@ -294,11 +302,43 @@ class Context:
         o = self._last_ppe
         return self.ppe(o.unknowns, o.nnz)
 
+    def ppe_manufacture(self, c0=0.0, gz=0.0, modes=()):
+        """p* = c0 + gz z + sum a sin(kx x + ky y + kz z + phi); b = A p*. modes: (a, kx, ky, kz, phi)."""
+        prm = np.array([c0, gz] + [v for m in modes for v in m], dtype=np.float64)
+        self._check(self.L.lsmps_ppe_manufacture(self.h, _p(prm), len(modes)))
+
     def mpnn_init(self, seed=0):
         self._check(self.L.lsmps_mpnn_init(self.h, seed))
 
+    def mpnn_weights(self):
+        w = np.zeros(self.L.lsmps_mpnn_param_count(), np.float32)
+        self._check(self.L.lsmps_mpnn_get_weights(self.h, _p(w), len(w)))
+        return w
+
+    def mpnn_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self.L.lsmps_mpnn_set_weights(self.h, _p(w), len(w)))
+
     def mpnn_add_sample(self):
         self._check(self.L.lsmps_mpnn_add_sample(self.h))
+
+    def mpnn_clear_samples(self):
+        self._check(self.L.lsmps_mpnn_clear_samples(self.h))
+
+    def mpnn_sample_count(self):
+        return self.L.lsmps_mpnn_sample_count(self.h)
+
+    def mpnn_grad(self, index=0):
+        g = np.zeros(self.L.lsmps_mpnn_param_count(), np.float32)
+        loss = C.c_float()
+        self._check(self.L.lsmps_mpnn_grad(self.h, index, _p(g), C.byref(loss)))
+        return loss.value, g
+
+    def mpnn_infer(self, r):
+        r = np.ascontiguousarray(r, np.float64)
+        y = np.zeros_like(r)
+        self._check(self.L.lsmps_mpnn_infer(self.h, _p(r), _p(y)))
+        return y
 
     def mpnn_train(self, steps, batch=4, lr=1e-3, weight_decay=0.0, seed=0):
         o = MpnnTrainOpts(steps=steps, batch=batch, lr=lr, weight_decay=weight_decay, seed=seed)

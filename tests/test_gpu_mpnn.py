@@ -1,0 +1,132 @@
+"""Learned preconditioner on the GPU: forward pass and gradients against the numpy oracle
+(agreement to BF16 rounding: 2e-2 relative), training, and the learned solver with its
+fallback. The network has no reference counterpart."""
+import numpy as np
+import pytest
+
+import lsmps_b200 as lib
+import mpnn_oracle as mo
+from _util import jittered_lattice
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(built):
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+def setup_system(ctx, xyz, t, field=None):
+    ctx.upload(xyz, t)
+    ctx.build_neighbors(2.1, 128, 1.0)
+    ctx.wls(2.1, 1.0, mode=1)
+    st = ctx.ppe_assemble("wls", 10**9, 2.1, 1.0, diag_shift=0.0)
+    if field:
+        ctx.ppe_manufacture(*field)
+    s = ctx.ppe_solve("jacobi", 20000, 1e-10)
+    assert s.converged
+    return st
+
+
+def oracle_graph(ctx, st):
+    row, col, val, b, xe, part = ctx.ppe(st.unknowns, st.nnz)
+    types = ctx.types()
+    G = mo.graph_from_csr(row, col, val, types[part] == lib.NEAR_WALL)
+    x = ctx.pressure(st.unknowns)
+    diag = val[row[1:] - 1]
+    nb = np.linalg.norm(b)
+    r = (b / nb).astype(np.float32).astype(np.float64)
+    t = (x * diag / nb).astype(np.float32).astype(np.float64)
+    return G, r, t
+
+
+@pytest.fixture(scope="module")
+def small(ctx):
+    xyz = jittered_lattice(11, 0.1, seed=4)
+    st = setup_system(ctx, xyz, np.zeros(len(xyz), np.uint8), (0.3, 0.05, [(1.0, 0.2, -0.1, 0.15, 0.3)]))
+    ctx.mpnn_init(7)
+    ctx.mpnn_clear_samples()
+    ctx.mpnn_add_sample()
+    return st
+
+
+def test_forward_matches_oracle(ctx, small):
+    G, r, t = oracle_graph(ctx, small)
+    w = ctx.mpnn_weights()
+    y_gpu = ctx.mpnn_infer(r)
+    y_orc, _ = mo.forward(w, G, r)
+    assert np.linalg.norm(y_gpu - y_orc) <= 2e-2 * np.linalg.norm(y_orc)
+
+
+def test_gradient_matches_oracle(ctx, small):
+    G, r, t = oracle_graph(ctx, small)
+    w = ctx.mpnn_weights()
+    loss, g = ctx.mpnn_grad(0)
+    l_orc, g_orc, _ = mo.loss_and_grad(w, G, r, t)
+    assert loss == pytest.approx(l_orc, rel=2e-2)
+    assert np.linalg.norm(g - g_orc) <= 3e-2 * np.linalg.norm(g_orc)
+    # each parameter block separately (encoder, three layers, decoder)
+    blocks = [(0, mo.OFF_L0)] + [(mo.OFF_L0 + l * mo.LSTRIDE, mo.OFF_L0 + (l + 1) * mo.LSTRIDE) for l in range(3)] + \
+             [(mo.OFF_WD, mo.NPARAM)]
+    for a, b in blocks:
+        assert np.linalg.norm(g[a:b] - g_orc[a:b]) <= 5e-2 * np.linalg.norm(g_orc[a:b]) + 1e-7
+
+
+def test_training_reduces_loss_and_helps_the_solver(ctx):
+    rng = np.random.default_rng(0)
+    ctx.mpnn_init(1)
+    ctx.mpnn_clear_samples()
+    for snap in range(3):
+        xyz, t, _ = lib.generate(None, case="rain_plate", particles=20_000, l0=1.0, seed=100 + snap)
+        ctx.upload(xyz, t)
+        ctx.build_neighbors(2.1, 128, 1.0)
+        ctx.wls(2.1, 1.0, mode=1)
+        ctx.ppe_assemble("wls", 10**9, 2.1, 1.0, diag_shift=0.0)
+        for k in range(6):
+            modes = [(rng.normal(), *(rng.uniform(-0.3, 0.3, 3)), rng.uniform(0, 6.28)) for _ in range(2)]
+            ctx.ppe_manufacture(rng.normal(), 0.1 * rng.normal(), modes)
+            assert ctx.ppe_solve("jacobi", 20000, 1e-10).converged
+            ctx.mpnn_add_sample()
+    assert ctx.mpnn_sample_count() == 18
+    l0 = np.mean([ctx.mpnn_grad(i)[0] for i in range(18)])
+    ctx.mpnn_train(steps=300, batch=2, lr=2e-3)
+    l1 = np.mean([ctx.mpnn_grad(i)[0] for i in range(18)])
+    assert l1 < 0.5 * l0, (l0, l1)
+    # held-out snapshot: the learned solver converges to the same accuracy
+    xyz, t, _ = lib.generate(None, case="rain_plate", particles=20_000, l0=1.0, seed=999)
+    ctx.upload(xyz, t)
+    ctx.build_neighbors(2.1, 128, 1.0)
+    ctx.wls(2.1, 1.0, mode=1)
+    ctx.ppe_assemble("wls", 10**9, 2.1, 1.0, diag_shift=0.0)
+    m = ctx.ppe_solve("mixed", 20000, 1e-10)
+    le = ctx.ppe_solve("learned", 20000, 1e-10)
+    assert m.converged and le.converged
+    assert le.relative_l2_error <= 1e-8 and le.fallback == 0
+    print(f"\nheld-out 20k: mixed {m.iterations} it, learned {le.iterations} it")
+
+
+def test_bad_network_falls_back(ctx):
+    xyz = jittered_lattice(14, 0.1, seed=9)
+    setup_system(ctx, xyz, np.zeros(len(xyz), np.uint8))
+    w = ctx.mpnn_weights()
+    w[mo.OFF_WD:mo.OFF_WD + 64] *= 1e6  # a guess far worse than zero
+    ctx.mpnn_set_weights(w)
+    s = ctx.ppe_solve("learned", 20000, 1e-10)
+    assert s.converged and s.fallback == 1 and s.relative_l2_error <= 1e-8
+    # the stall rule: no 1 % progress in `stall_window` iterations switches to plain Jacobi
+    ctx.mpnn_init(3)
+    s = ctx.ppe_solve("learned", 20000, 1e-10, stall_window=1)
+    assert s.converged and s.fallback == 1
+
+
+def test_weights_roundtrip(ctx, tmp_path, small):
+    ctx.mpnn_init(11)
+    w = ctx.mpnn_weights()
+    ctx.mpnn_save(str(tmp_path / "w.bin"))
+    ctx.mpnn_init(12)
+    ctx.mpnn_load(str(tmp_path / "w.bin"))
+    assert np.array_equal(ctx.mpnn_weights(), w)
+    with pytest.raises(lib.LsmpsError):
+        ctx.mpnn_load(str(tmp_path / "missing.bin"))
