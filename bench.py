@@ -52,7 +52,9 @@ def parse_args():
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--case", default="mixed")
     ap.add_argument("--seed", type=int, default=7)
-    ap.add_argument("--solver", default="mixed", choices=["mixed", "learned", "jacobi", "fp64"])
+    ap.add_argument("--solver", default="learned", choices=["learned", "mixed", "jacobi", "fp64"])
+    ap.add_argument("--weights", default=os.path.join(ROOT, "ls-mps_b200", "weights", "mpnn_rain200k.bin"),
+                    help="network weights for the learned solver (trained by ls-mps_b200/train_mpnn.py)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-iter", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -211,6 +213,8 @@ def run_mine(args, dist):
     n = len(types)
     ctx = lib.Context(dev)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    if args.solver == "learned":
+        ctx.mpnn_load(args.weights)
     ctx.upload(xyz, types)
     timings = []
     for _ in range(args.warmup):
@@ -258,7 +262,9 @@ def run_mine(args, dist):
         "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step_max,
         "value": n * dist.world / (ms_step_max * 1e-3),
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (mixed)" if args.solver == "mixed" else args.solver,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"learned": "f64 vectors + f32 matrix; bf16 network", "mixed": "f64 vectors + f32 matrix"}.get(
+            args.solver, "f64"),
         "data": "synthetic (seeded generator; no dataset)",
         "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}",
                    "particles": n, "case": args.case, "l0": L0, "re": RE_RATIO * L0, "max_neighbors": MAXN,
@@ -278,7 +284,7 @@ def run_mine(args, dist):
     # ---- the plain FP64 GPU BiCGStab (and the stages between) on the same system ----
     if not args.no_compare:
         cmp = {}
-        for name in ("fp64", "jacobi", "mixed"):
+        for name in ("fp64", "jacobi", "mixed") + (("learned",) if args.solver == "learned" else ()):
             r = ctx.ppe_solve(name, args.max_iter, args.tol)
             cmp[name] = {"solve_ms": r.solve_ms, "iterations": r.iterations, "converged": bool(r.converged),
                          "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual}
@@ -294,6 +300,7 @@ def run_mine(args, dist):
         gbs = nbytes / (ms * 1e-3) / 1e9
         kern[name] = {"ms": ms, "alg_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
     dom = "spmv32" if args.solver in ("mixed", "learned") else "spmv64"
+    # the mixed solver's SpMV: FP32 values of A D^-1, FP64 vectors
     traffic = committed_traffic().get(dom)
     result["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"], "peak": peak,
                           "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,

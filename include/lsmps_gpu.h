@@ -61,8 +61,8 @@ uint64_t lsmps_launch_count(void);
 /* Profiling hook: launches one kernel of the path `reps` times on the context stream on
  * the current data and returns its mean duration (CUDA events around the launches) and
  * its algorithmic bytes per launch (the traffic a perfect kernel would move):
- *   LSMPS_KB_SPMV64  FP64 CSR SpMV + fused dot   12 nnz + 20 U
- *   LSMPS_KB_SPMV32  FP32 CSR SpMV + fused dot    8 nnz + 16 U
+ *   LSMPS_KB_SPMV64  SELL SpMV + fused dot, FP64 values (plain FP64 solver)   12 nnz + 24.25 U
+ *   LSMPS_KB_SPMV32  SELL SpMV + fused dot, FP32 values, FP64 vectors (MIXED)  8 nnz + 24.25 U
  *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL neighbor passes   24 N + 4 N (+ 4 P + 1 N fill)
  *   LSMPS_KB_WLS     all-particle WLS            24 N + 4 P + 80 N (z, sum w, status)
  * No reference counterpart (the reference has no GPU path). */
@@ -224,7 +224,7 @@ typedef struct lsmps_mpnn_train_opts {
     float lr;                /* Adam learning rate */
     float weight_decay;      /* decoupled weight decay */
     uint32_t seed;           /* sample order */
-    int32_t reserved;
+    int32_t loss;            /* 0: error |y - t|^2 / |t|^2; 1: residual |r - A D^-1 y|^2 / |r|^2; 2: both */
 } lsmps_mpnn_train_opts;
 
 /* Initialise the weights from a seed (He-scaled normals; residual branches scaled down). */
@@ -236,8 +236,8 @@ int lsmps_mpnn_set_weights(lsmps_ctx* ctx, const float* w, size_t n);
 int lsmps_mpnn_add_sample(lsmps_ctx* ctx);
 int lsmps_mpnn_clear_samples(lsmps_ctx* ctx);
 int lsmps_mpnn_sample_count(lsmps_ctx* ctx);
-/* Loss |y - t|^2 / |t|^2 of stored sample `index` and its gradient (FP32, parameter
- * order above; grad may be NULL). */
+/* Loss of stored sample `index` (the kind last used by lsmps_mpnn_train; error loss
+ * before any training) and its gradient (FP32, parameter order above; grad may be NULL). */
 int lsmps_mpnn_grad(lsmps_ctx* ctx, int index, float* grad, float* loss);
 /* Adam on the stored samples; loss_out: mean loss of the last `batch` samples. */
 int lsmps_mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* opts, float* loss_out);

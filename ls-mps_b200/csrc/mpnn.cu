@@ -35,7 +35,7 @@ using bf16 = __nv_bfloat16;
 
 struct MpnnGraph {
     long long U = 0, nnz = 0;
-    DevBuf row, col, ew, feat;  // row/col copies (training store) or unused (inference view)
+    DevBuf row, col, ew, feat, dg;  // row/col copies (training store) or unused (inference view); dg: a_ii
     const int* prow = nullptr;
     const int* pcol = nullptr;
 };
@@ -56,7 +56,8 @@ struct MpnnState {
     MpnnGraph infer;           // graph of the current system (inference)
     long long infer_gen = -1;
     long long cap = 0;         // workspace capacity (nodes)
-    DevBuf h[NL + 1], a[NL], z[NL + 1], y, gh[2], gam, gz;
+    int loss_kind = 0;         // 0 error, 1 residual, 2 both
+    DevBuf h[NL + 1], a[NL], z[NL + 1], y, gy, ay, q, gh[2], gam, gz;
 };
 
 namespace {
@@ -125,10 +126,11 @@ __global__ void k_mean_diag(long long U, const double* __restrict__ dinv, double
 // feat[u] = [a_uu / mean - 1, NearWall, (row length - 1) / 32 - 1]
 __global__ void k_graph_feat(long long U, const int* __restrict__ row, const double* __restrict__ dinv,
                              const uint8_t* __restrict__ cls, const int* __restrict__ sorted_of_u,
-                             const double* mean, float* __restrict__ feat) {
+                             const double* mean, float* __restrict__ feat, float* __restrict__ dg) {
     long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (u >= U) return;
     const double d = dinv[u] != 0 ? 1.0 / dinv[u] : 1.0;
+    dg[u] = (float)d;
     feat[3 * u + 0] = (float)(d / *mean - 1.0);
     feat[3 * u + 1] = cls[sorted_of_u[u]] == LSMPS_NEAR_WALL ? 1.f : 0.f;
     feat[3 * u + 2] = (float)(row[u + 1] - row[u] - 1) / 32.f - 1.f;
@@ -141,6 +143,7 @@ struct GView {
     const int* col;
     const float* ew;
     const float* feat;
+    const float* dg;  // a_ii
     float sqrt_u;
 };
 
@@ -303,9 +306,39 @@ __global__ void k_loss(long long U, const float* __restrict__ y, const float* __
     }
 }
 
+// (A D^-1 y)_i = y_i - a_ii sum_j w_ij y_j / a_jj
+__global__ void k_apply_scaled(GView G, const float* __restrict__ y, float* __restrict__ ay) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= G.U) return;
+    float s = 0.f;
+    for (int e = G.row[i]; e < G.row[i + 1] - 1; ++e) s += G.ew[e] * y[G.col[e]] / G.dg[G.col[e]];
+    ay[i] = y[i] - G.dg[i] * s;
+}
+
+// dL/dy of the selected loss kind. Error: 2 (y - t) / |t|^2. Residual (|r| = 1):
+// g = -2 (r - A D^-1 y); dL/dy_k = g_k - (1 / a_kk) sum_i a_ii w_ik g_i (q holds the sum,
+// accumulated by k_scatter_res beforehand). Both: the sum.
+__global__ void k_dldy(long long U, const float* __restrict__ y, const float* __restrict__ t, const float* __restrict__ r,
+                       const float* __restrict__ ay, const float* __restrict__ q, const float* __restrict__ dg,
+                       float err_scale, int kind, float* __restrict__ gy) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= U) return;
+    float g = 0.f;
+    if (kind != 1) g += err_scale * (y[i] - t[i]);
+    if (kind != 0) g += -2.f * (r[i] - ay[i]) - q[i] / dg[i];
+    gy[i] = g;
+}
+
+// q_k += a_ii w_ik g_i with g = -2 (r - A D^-1 y) (transposed product, one thread per row)
+__global__ void k_scatter_res(GView G, const float* __restrict__ r, const float* __restrict__ ay, float* __restrict__ q) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= G.U) return;
+    const float gi = -2.f * (r[i] - ay[i]) * G.dg[i];
+    for (int e = G.row[i]; e < G.row[i + 1] - 1; ++e) atomicAdd(&q[G.col[e]], G.ew[e] * gi);
+}
+
 // go_i = dL/dy_i / sqrt(U); gh3 = go w_dec; block partials of dw_dec (64) and db_dec (1)
-__global__ void __launch_bounds__(256) k_dec_bwd(GView G, const float* __restrict__ y, const float* __restrict__ t,
-                                                 float scale2, const bf16* __restrict__ h3,
+__global__ void __launch_bounds__(256) k_dec_bwd(GView G, const float* __restrict__ gy, const bf16* __restrict__ h3,
                                                  const float* __restrict__ w, float* __restrict__ gh3,
                                                  float* __restrict__ part) {
     __shared__ float sw[H];
@@ -314,7 +347,7 @@ __global__ void __launch_bounds__(256) k_dec_bwd(GView G, const float* __restric
     if (threadIdx.x <= H) sg[threadIdx.x] = 0.f;
     __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
-        const float go = scale2 * (y[i] - t[i]) / G.sqrt_u;
+        const float go = gy[i] / G.sqrt_u;
         for (int c = 0; c < H; ++c) {
             gh3[i * H + c] = go * sw[c];
             atomicAdd(&sg[c], go * __bfloat162float(h3[i * H + c]));
@@ -675,19 +708,22 @@ static void build_graph(lsmps_ctx* ctx, MpnnGraph& g, bool copy_structure) {
     }
     float* ew = g.ew.ensure<float>(nnz + 1);
     float* feat = g.feat.ensure<float>(3 * U + 3);
+    float* dg = g.dg.ensure<float>(U + 1);
     double* mean = ctx->scratch.get<double>() + 24;
     if (U) {
         k_graph_ew<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_val.get<double>(),
                                                      ctx->A_dinv.get<double>(), ew);
         k_mean_diag<<<1, 1024, 0, s>>>(U, ctx->A_dinv.get<double>(), mean);
         k_graph_feat<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_dinv.get<double>(),
-                                                       ctx->cls.get<uint8_t>(), ctx->sorted_of_u.get<int>(), mean, feat);
+                                                       ctx->cls.get<uint8_t>(), ctx->sorted_of_u.get<int>(), mean, feat,
+                                                       dg);
         LSMPS_CHECK_LAUNCH();
     }
 }
 
 static GView view(const MpnnGraph& g) {
-    return GView{g.U, g.prow, g.pcol, g.ew.get<float>(), g.feat.get<float>(), (float)std::sqrt((double)std::max(1LL, g.U))};
+    return GView{g.U,           g.prow,         g.pcol, g.ew.get<float>(), g.feat.get<float>(), g.dg.get<float>(),
+                 (float)std::sqrt((double)std::max(1LL, g.U))};
 }
 
 static void ensure_workspace(MpnnState& S, long long U, bool training) {
@@ -734,8 +770,17 @@ static double loss_and_grad(lsmps_ctx* ctx, MpnnState& S, const GView& G, const 
     cudaStream_t s = ctx->stream;
     forward(ctx, S, G, r, grad != nullptr);
     double* lsum = S.red.ensure<double>(8);
-    k_loss<<<1, 1024, 0, s>>>(G.U, S.y.get<float>(), t, lsum);
-    LSMPS_CHECK_LAUNCH();
+    const int kind = S.loss_kind;
+    float* ay = S.ay.ensure<float>(S.cap + 8);
+    if (kind != 1) {
+        k_loss<<<1, 1024, 0, s>>>(G.U, S.y.get<float>(), t, lsum);
+        LSMPS_CHECK_LAUNCH();
+    }
+    if (kind != 0) {
+        k_apply_scaled<<<blocks_for(G.U, 256), 256, 0, s>>>(G, S.y.get<float>(), ay);
+        k_loss<<<1, 1024, 0, s>>>(G.U, ay, r, lsum + 1);  // |r - A D^-1 y|^2, |r| = 1
+        LSMPS_CHECK_LAUNCH();
+    }
     if (grad) {
         const float* w = S.dw.get<float>();
         const bf16* wbf = S.wbf.get<bf16>();
@@ -743,9 +788,17 @@ static double loss_and_grad(lsmps_ctx* ctx, MpnnState& S, const GView& G, const 
         float* part = S.gpart.ensure<float>((size_t)WG_BLOCKS * H * KIN + 16);
         float* gh_next = S.gh[0].get<float>();
         float* gh_cur = S.gh[1].get<float>();
-        // decoder
-        k_dec_bwd<<<nb, 256, 0, s>>>(G, S.y.get<float>(), t, (float)(2.0 / std::max(tnorm2, 1e-30)),
-                                     S.h[NL].get<bf16>(), w, gh_next, part);
+        // dL/dy, then the decoder
+        float* gy = S.gy.ensure<float>(S.cap + 8);
+        float* q = S.q.ensure<float>(S.cap + 8);
+        if (kind != 0) {
+            LSMPS_CUDA(cudaMemsetAsync(q, 0, G.U * sizeof(float), s));
+            k_scatter_res<<<blocks_for(G.U, 256), 256, 0, s>>>(G, r, ay, q);
+            LSMPS_CHECK_LAUNCH();
+        }
+        k_dldy<<<blocks_for(G.U, 256), 256, 0, s>>>(G.U, S.y.get<float>(), t, r, ay, q, G.dg,
+                                                    (float)(2.0 / std::max(tnorm2, 1e-30)), kind, gy);
+        k_dec_bwd<<<nb, 256, 0, s>>>(G, gy, S.h[NL].get<bf16>(), w, gh_next, part);
         LSMPS_CHECK_LAUNCH();
         k_reduce_part<<<1, H + 1, 0, s>>>(part, nb, H + 1, H + 1, grad + OFF_WD, accumulate ? 1 : 0);
         LSMPS_CHECK_LAUNCH();
@@ -774,10 +827,10 @@ static double loss_and_grad(lsmps_ctx* ctx, MpnnState& S, const GView& G, const 
         k_reduce_part<<<blocks_for(OFF_L0, 256), 256, 0, s>>>(part, nb, (int)OFF_L0, (int)OFF_L0, grad, accumulate ? 1 : 0);
         LSMPS_CHECK_LAUNCH();
     }
-    double h;
-    LSMPS_CUDA(cudaMemcpyAsync(&h, lsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    double h[2] = {0, 0};
+    LSMPS_CUDA(cudaMemcpyAsync(h, lsum, sizeof(h), cudaMemcpyDeviceToHost, s));
     LSMPS_CUDA(cudaStreamSynchronize(s));
-    return h / std::max(tnorm2, 1e-30);
+    return (kind != 1 ? h[0] / std::max(tnorm2, 1e-30) : 0.0) + (kind != 0 ? h[1] : 0.0);
 }
 
 void mpnn_add_sample(lsmps_ctx* ctx) {
@@ -837,7 +890,8 @@ void mpnn_grad(lsmps_ctx* ctx, int index, float* grad_host, float* loss) {
 void mpnn_train(lsmps_ctx* ctx, const lsmps_mpnn_train_opts* o, float* loss_out) {
     MpnnState& S = state(ctx);
     LSMPS_REQUIRE(!S.samples.empty(), LSMPS_ERR_STATE, "no training samples");
-    LSMPS_REQUIRE(o->steps >= 0 && o->batch >= 1, LSMPS_ERR_ARG, "training options");
+    LSMPS_REQUIRE(o->steps >= 0 && o->batch >= 1 && o->loss >= 0 && o->loss <= 2, LSMPS_ERR_ARG, "training options");
+    S.loss_kind = o->loss;
     cudaStream_t s = ctx->stream;
     float* grad = S.grad.ensure<float>(NPARAM);
     std::mt19937 rng(o->seed);

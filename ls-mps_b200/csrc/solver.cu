@@ -1346,6 +1346,8 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
     if (out) *out = ps;
 }
 
+// The solver's SpMV as the iterations run it: LSMPS_KB_SPMV32 is the MIXED solver's kernel
+// (FP32 A D^-1 values, FP64 vectors), LSMPS_KB_SPMV64 the plain FP64 solver's (FP64 A).
 void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes) {
     LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "SpMV bench needs an assembled PPE");
     cudaStream_t s = ctx->stream;
@@ -1357,23 +1359,19 @@ void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, doubl
     LSMPS_CUDA(cudaMemcpyAsync(E.S, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     const bool f32 = kernel == LSMPS_KB_SPMV32;
     // operands of ones: the fused dot is then nonzero, so no breakdown guard stops the kernel
-    if (f32) {
-        k_fill<float><<<1184, 256, 0, s>>>(U, ctx->fp.ensure<float>(U + 1), 1.0f);
-        k_fill<float><<<1184, 256, 0, s>>>(U, ctx->fr0.ensure<float>(U + 1), 1.0f);
-        ctx->fv.ensure<float>(U + 1);
-    } else {
-        k_fill<double><<<1184, 256, 0, s>>>(U, ctx->vp.ensure<double>(U + 1), 1.0);
-        k_fill<double><<<1184, 256, 0, s>>>(U, ctx->vr0.ensure<double>(U + 1), 1.0);
-        ctx->vv.ensure<double>(U + 1);
-    }
+    double* x = ctx->vp.ensure<double>(U + 1);
+    double* r0 = ctx->vr0.ensure<double>(U + 1);
+    double* y = ctx->vv.ensure<double>(U + 1);
+    k_fill<double><<<1184, 256, 0, s>>>(U, x, 1.0);
+    k_fill<double><<<1184, 256, 0, s>>>(U, r0, 1.0);
     LSMPS_CHECK_LAUNCH();
     Sell<float> Af{};
     Sell<double> Ad{};
     if (f32) Af = sell_scaled32(ctx);
     else Ad = sell_a64(ctx);
     auto launch = [&] {
-        if (f32) k_bcg_v<float><<<RGRID, RB, 0, s>>>(Af, ctx->fp.get<float>(), ctx->fv.get<float>(), ctx->fr0.get<float>(), E.S, E.P);
-        else k_bcg_v<double><<<RGRID, RB, 0, s>>>(Ad, ctx->vp.get<double>(), ctx->vv.get<double>(), ctx->vr0.get<double>(), E.S, E.P);
+        if (f32) k_bcg_v<double, float><<<RGRID, RB, 0, s>>>(Af, x, y, r0, E.S, E.P);
+        else k_bcg_v<double, double><<<RGRID, RB, 0, s>>>(Ad, x, y, r0, E.S, E.P);
         LSMPS_CHECK_LAUNCH();
     };
     launch();
@@ -1381,10 +1379,10 @@ void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, doubl
     for (int r = 0; r < reps; ++r) launch();
     ev_record(ctx, 15);
     *ms = ev_elapsed(ctx, 14, 15) / reps;
-    // algorithmic bytes: matrix values + columns once (nonzeros, not padding), row data,
-    // x once, y written once, r0 read once
+    // algorithmic bytes: values + columns of the nonzeros (not the padding), the x gathers
+    // counted once, y written, r0 read (FP64 vectors), slice pointers and lengths
     const double nnz = (double)ctx->nnz;
-    *bytes = f32 ? 8.0 * nnz + 16.0 * U : 12.0 * nnz + 28.0 * U;
+    *bytes = (f32 ? 8.0 : 12.0) * nnz + 24.25 * U;
     // the bench overwrote solver vectors: a warm start from them is no longer valid
     ctx->have_solution = false;
 }

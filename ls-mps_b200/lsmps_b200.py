@@ -81,7 +81,7 @@ class SolverOpts(C.Structure):
 
 class MpnnTrainOpts(C.Structure):
     _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
-                ("weight_decay", C.c_float), ("seed", C.c_uint32), ("reserved", C.c_int32)]
+                ("weight_decay", C.c_float), ("seed", C.c_uint32), ("loss", C.c_int32)]
 
 
 # Every function the header declares, with its ctypes signature.
@@ -340,8 +340,8 @@ class Context:
         self._check(self.L.lsmps_mpnn_infer(self.h, _p(r), _p(y)))
         return y
 
-    def mpnn_train(self, steps, batch=4, lr=1e-3, weight_decay=0.0, seed=0):
-        o = MpnnTrainOpts(steps=steps, batch=batch, lr=lr, weight_decay=weight_decay, seed=seed)
+    def mpnn_train(self, steps, batch=4, lr=1e-3, weight_decay=0.0, seed=0, loss=0):
+        o = MpnnTrainOpts(steps=steps, batch=batch, lr=lr, weight_decay=weight_decay, seed=seed, loss=loss)
         loss = C.c_float()
         self._check(self.L.lsmps_mpnn_train(self.h, C.byref(o), C.byref(loss)))
         return loss.value

@@ -8,8 +8,9 @@ Data: rain-on-plate snapshots of --particles (200,000) parti
 solved by the plain FP64 Jacobi-BiCGStab to relative residual 1e-10; the pair
 (b / |b|, D p / |b|) is stored on the GPU (--snapshots x --pairs = 2,000 by default).
 Training: Adam on the GPU with the library's own forward and backward kernels.
-Evaluation: held-out seeds (9000, ...) of the bench's 1M `mixed` case: iterations and solve
-time of LEARNED against MIXED (the same solver without the network), and the fallback count.
+Evaluation: held-out seeds (9000, ...) at 1M of the rain-on-plate case (the training
+distribution) and of the bench's `mixed` case: iterations and solve time of LEARNED against
+MIXED (the same solver without the network) and plain FP64, and the fallback count.
 """
 import argparse
 import json
@@ -48,10 +49,12 @@ def main():
     ap.add_argument("--particles", type=int, default=200_000)
     ap.add_argument("--snapshots", type=int, default=40)
     ap.add_argument("--pairs", type=int, default=50)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--loss", type=int, default=2, help="0 error, 1 residual |r - A D^-1 y|, 2 both (best measured)")
+    ap.add_argument("--eval-cases", default="rain_plate,mixed")
     ap.add_argument("--eval-seeds", type=int, default=3)
     ap.add_argument("--eval-particles", type=int, default=1_000_000)
     ap.add_argument("--out", default=None)
@@ -83,7 +86,7 @@ def main():
             chunk = max(1, a.steps // 20)
             for done in range(0, a.steps, chunk):
                 losses.append(ctx.mpnn_train(steps=min(chunk, a.steps - done), batch=a.batch, lr=a.lr,
-                                             seed=a.seed + done))
+                                             seed=a.seed + done, loss=a.loss))
                 print(f"step {done + chunk}: loss {losses[-1]:.4f}", flush=True)
             t2 = time.time()
             report["training"] = {"pairs": ctx.mpnn_sample_count(), "data_s": t1 - t0, "train_s": t2 - t1,
@@ -93,27 +96,35 @@ def main():
                 ctx.mpnn_save(a.out)
             ctx.mpnn_clear_samples()
         evals = []
-        for k in range(a.eval_seeds):
-            st = build(ctx, "mixed", a.eval_particles, 9000 + k)
-            res = {}
-            for name in ("mixed", "learned", "fp64"):
-                ctx.ppe_solve(name, 20000, 1e-10)  # warm
-                s = ctx.ppe_solve(name, 20000, 1e-10)
-                res[name] = {"iterations": s.iterations, "solve_ms": s.solve_ms, "rel_l2": s.relative_l2_error,
-                             "converged": bool(s.converged), "fallback": s.fallback}
-            evals.append(res)
-            print(f"seed {9000 + k}: " + ", ".join(f"{n} {r['iterations']} it {r['solve_ms']:.1f} ms" for n, r in res.items()),
-                  flush=True)
+        for case in a.eval_cases.split(","):
+            for k in range(a.eval_seeds):
+                build(ctx, case, a.eval_particles, 9000 + k)
+                res = {"case": case}
+                for name in ("mixed", "learned", "fp64"):
+                    ctx.ppe_solve(name, 20000, 1e-10)  # warm
+                    s = ctx.ppe_solve(name, 20000, 1e-10)
+                    res[name] = {"iterations": s.iterations, "solve_ms": s.solve_ms, "rel_l2": s.relative_l2_error,
+                                 "converged": bool(s.converged), "fallback": s.fallback}
+                evals.append(res)
+                print(f"{case} seed {9000 + k}: " + ", ".join(
+                    f"{n} {r['iterations']} it {r['solve_ms']:.1f} ms" for n, r in res.items() if n != "case"),
+                      flush=True)
         report["eval"] = evals
-        if evals:
-            m = np.mean([e["mixed"]["solve_ms"] for e in evals])
-            le = np.mean([e["learned"]["solve_ms"] for e in evals])
-            p = np.mean([e["fp64"]["solve_ms"] for e in evals])
-            report["summary"] = {"mixed_ms": m, "learned_ms": le, "plain_fp64_ms": p,
-                                 "learned_vs_mixed": m / le, "learned_vs_plain_fp64": p / le,
-                                 "mixed_it": np.mean([e["mixed"]["iterations"] for e in evals]),
-                                 "learned_it": np.mean([e["learned"]["iterations"] for e in evals])}
-            print(json.dumps(report["summary"]))
+        summary = {}
+        for case in a.eval_cases.split(","):
+            ev = [e for e in evals if e["case"] == case]
+            if not ev:
+                continue
+            m = np.mean([e["mixed"]["solve_ms"] for e in ev])
+            le = np.mean([e["learned"]["solve_ms"] for e in ev])
+            p = np.mean([e["fp64"]["solve_ms"] for e in ev])
+            summary[case] = {"mixed_ms": m, "learned_ms": le, "plain_fp64_ms": p,
+                             "learned_vs_mixed": m / le, "learned_vs_plain_fp64": p / le,
+                             "mixed_it": np.mean([e["mixed"]["iterations"] for e in ev]),
+                             "learned_it": np.mean([e["learned"]["iterations"] for e in ev]),
+                             "fallbacks": int(sum(e["learned"]["fallback"] for e in ev))}
+        report["summary"] = summary
+        print(json.dumps(summary))
     if a.report:
         with open(a.report, "w") as f:
             json.dump(report, f, indent=1, default=float)

@@ -57,7 +57,14 @@ def graph_from_csr(row, col, val, nearwall):
     deg = np.diff(row) - 1
     feat = np.stack([diag / diag.mean() - 1.0, nearwall.astype(np.float64), deg / 32.0 - 1.0], 1)
     return dict(U=U, src=np.array(src), dst=np.array(dst), w=np.array(w, np.float64),
-                feat=feat.astype(np.float32).astype(np.float64))
+                feat=feat.astype(np.float32).astype(np.float64), d=diag.astype(np.float32).astype(np.float64))
+
+
+def apply_scaled(G, y):
+    """(A D^-1 y)_i = y_i - a_ii sum_j w_ij y_j / a_jj."""
+    s = np.zeros_like(y)
+    np.add.at(s, G["src"], G["w"] * y[G["dst"]] / G["d"][G["dst"]])
+    return y - G["d"] * s
 
 
 def aggregate(G, h):
@@ -92,13 +99,25 @@ def forward(w, G, r, round_bf16=True):
     return y, dict(x=x, hs=hs, zs=zs, As=As, su=su)
 
 
-def loss_and_grad(w, G, r, t, round_bf16=True):
+def loss_and_grad(w, G, r, t, round_bf16=True, kind=0):
+    """kind 0: |y - t|^2 / |t|^2; 1: |r - A D^-1 y|^2 (|r| = 1); 2: both."""
     p = unpack(w)
     y, c = forward(w, G, r, round_bf16)
     tn2 = float(np.sum(np.float64(t) ** 2))
-    loss = float(np.sum((y - t) ** 2)) / tn2
+    loss = 0.0
+    gy = np.zeros_like(y)
+    if kind != 1:
+        loss += float(np.sum((y - t) ** 2)) / tn2
+        gy += 2.0 * (y - t) / tn2
+    if kind != 0:
+        res = r - apply_scaled(G, y)
+        loss += float(np.sum(res ** 2))
+        gg = -2.0 * res
+        q = np.zeros_like(y)
+        np.add.at(q, G["dst"], G["d"][G["src"]] * G["w"] * gg[G["src"]])
+        gy += gg - q / G["d"]
     g = np.zeros(NPARAM)
-    go = 2.0 * (y - t) / tn2 / float(c["su"])
+    go = gy / float(c["su"])
     g[OFF_WD:OFF_WD + 64] = c["hs"][-1].T @ go
     g[OFF_BD] = go.sum()
     gh = go[:, None] * p["wd"][None, :]

@@ -74,6 +74,17 @@ def test_gradient_matches_oracle(ctx, small):
         assert np.linalg.norm(g[a:b] - g_orc[a:b]) <= 5e-2 * np.linalg.norm(g_orc[a:b]) + 1e-7
 
 
+def test_residual_loss_gradient_matches_oracle(ctx, small):
+    G, r, t = oracle_graph(ctx, small)
+    ctx.mpnn_train(steps=0, loss=1)  # selects the residual loss, no update
+    w = ctx.mpnn_weights()
+    loss, g = ctx.mpnn_grad(0)
+    l_orc, g_orc, _ = mo.loss_and_grad(w, G, r, t, kind=1)
+    ctx.mpnn_train(steps=0, loss=0)
+    assert loss == pytest.approx(l_orc, rel=2e-2)
+    assert np.linalg.norm(g - g_orc) <= 3e-2 * np.linalg.norm(g_orc)
+
+
 def test_training_reduces_loss_and_helps_the_solver(ctx):
     rng = np.random.default_rng(0)
     ctx.mpnn_init(1)

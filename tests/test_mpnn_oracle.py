@@ -19,14 +19,18 @@ def small_graph(n=60, seed=0):
     return mo.graph_from_csr(row, col, val, rng.random(n) < 0.2)
 
 
-def test_oracle_gradient_finite_differences():
+import pytest
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_oracle_gradient_finite_differences(kind):
     rng = np.random.default_rng(1)
     G = small_graph()
     w = rng.normal(0, 0.3, mo.NPARAM)
     r = rng.normal(size=G["U"])
     r /= np.linalg.norm(r)
     t = rng.normal(size=G["U"]) * 0.1
-    loss, g, _ = mo.loss_and_grad(w, G, r, t, round_bf16=False)
+    loss, g, _ = mo.loss_and_grad(w, G, r, t, round_bf16=False, kind=kind)
     idx = np.concatenate([rng.choice(np.arange(0, 320), 12, replace=False),
                           rng.choice(np.arange(320, mo.OFF_WD), 24, replace=False),
                           np.arange(mo.OFF_WD, mo.NPARAM)[::9]])
@@ -35,7 +39,7 @@ def test_oracle_gradient_finite_differences():
         wp, wm = w.copy(), w.copy()
         wp[k] += eps
         wm[k] -= eps
-        fd = (mo.loss_and_grad(wp, G, r, t, False)[0] - mo.loss_and_grad(wm, G, r, t, False)[0]) / (2 * eps)
+        fd = (mo.loss_and_grad(wp, G, r, t, False, kind)[0] - mo.loss_and_grad(wm, G, r, t, False, kind)[0]) / (2 * eps)
         assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(fd)), (k, fd, g[k])
 
 
