@@ -120,7 +120,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     lsmps_gpu::DevBuf* bufs[] = {&ctx->dflags, &ctx->scratch, &ctx->scan_tmp, &ctx->host_dummy, &ctx->pos,
                                  &ctx->type_in, &ctx->cell_of, &ctx->slot, &ctx->cell_count, &ctx->cell_start,
                                  &ctx->perm, &ctx->iperm, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->stype,
-                                 &ctx->scell, &ctx->cls, &ctx->nbr_cnt, &ctx->nbr_row, &ctx->nbr_col,
+                                 &ctx->scell, &ctx->cls, &ctx->nbr_cnt, &ctx->nbr_row, &ctx->nbr_col, &ctx->seg_list,
                                  &ctx->nbr_stats, &ctx->wls_status, &ctx->wls_z, &ctx->wls_wsum, &ctx->wls_x,
                                  &ctx->wls_stats, &ctx->wls_sample, &ctx->ref_rank, &ctx->u_of_sorted,
                                  &ctx->sorted_of_u, &ctx->ref_of_u, &ctx->u_of_ref, &ctx->A_row, &ctx->A_col,

@@ -51,9 +51,10 @@ struct lsmps_ctx {
     bool have_neighbors = false, have_classes = false;
     uint64_t pairs = 0, truncated = 0;
     int max_cell_occupancy = 0;
+    int nsegs = 0;  // non-empty 12-cell segments of the grid (neighbor passes)
     lsmps_gpu::DevBuf cell_of, slot, cell_count, cell_start, perm, iperm;
     lsmps_gpu::DevBuf sx, sy, sz, stype, scell, cls;
-    lsmps_gpu::DevBuf nbr_cnt, nbr_row, nbr_col, nbr_stats;
+    lsmps_gpu::DevBuf nbr_cnt, nbr_row, nbr_col, nbr_stats, seg_list;
 
     // ---- WLS ----
     bool have_wls = false;

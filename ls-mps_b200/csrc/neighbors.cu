@@ -6,9 +6,10 @@
 //   2. a counting sort of particles into a dense cell grid (atomic slots, scan), then
 //      each cell's members sorted by particle index, so that every 3-cell x-row of the grid
 //      is one contiguous, index-ascending range of the sorted arrays;
-//   3. a count pass and a fill pass, one warp per particle: the warp tests the 9 contiguous
-//      row ranges 32 candidates at a time, and a ballot gives each accepted candidate its
-//      position. Scanning the 9 rows in (dz, dy) order with candidates in sorted order is
+//   3. a count pass and a fill pass, one block per segment of 4 cells along x, one warp per
+//      particle: the block stages its 9 cell rows' candidates in shared memory, a warp tests
+//      a particle's 9 contiguous row ranges 32 candidates at a time (FP32 guard band, exact
+//      FP64 near the cutoff), and a ballot gives each accepted candidate its position. Scanning the 9 rows in (dz, dy) order with candidates in sorted order is
 //      exactly the reference's order (27 cells dz, dy, dx; ascending index in a cell), so
 //      the sorted column indices of a row ascend and the first max_neighbors are the ones
 //      the reference keeps. The fill pass fuses the classification over the kept list.
@@ -202,51 +203,36 @@ __device__ __forceinline__ uint8_t classify_rule(uint8_t tin, int kept, unsigned
     return LSMPS_INTERIOR;
 }
 
-__global__ void __launch_bounds__(NB_WARPS * 32) k_count(GridView g, const double* __restrict__ sx,
-                                                       const double* __restrict__ sy,
-                                                       const double* __restrict__ sz,
-                                                       const int* __restrict__ scell, int n, double re2,
-                                                       int maxn, int* __restrict__ cnt,
-                                                       unsigned long long* trunc_total) {
-    int k = blockIdx.x * NB_WARPS + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    unsigned long long tr = 0;
-    if (k < n) {
-        int lin = scell[k];
-        int cx = lin % g.nx, t = lin / g.nx, cy = t % g.ny, cz = t / g.ny;
-        double xi = sx[k], yi = sy[k], zi = sz[k];
-        int count = 0;
-        for (int dz = -1; dz <= 1; ++dz)
-            for (int dy = -1; dy <= 1; ++dy) {
-                int beg, end;
-                if (!row_range(g, cx, cy, cz, dy, dz, beg, end)) continue;
-                for (int mb = beg; mb < end; mb += 32) {
-                    int m = mb + lane;
-                    bool ok = false;
-                    if (m < end && m != k)
-                        ok = xnorm2(xsub(sx[m], xi), xsub(sy[m], yi), xsub(sz[m], zi)) < re2;
-                    count += __popc(__ballot_sync(0xffffffffu, ok));
-                }
+// Global-memory form of one query (one warp): count / fill the accepted candidates of
+// sorted particle k; used by the staged kernels when a segment's neighborhood does not fit
+// in shared memory.
+__device__ __forceinline__ int count_query_global(const GridView& g, const double* __restrict__ sx,
+                                                  const double* __restrict__ sy, const double* __restrict__ sz,
+                                                  const int* __restrict__ scell, int k, double re2, int lane) {
+    int lin = scell[k];
+    int cx = lin % g.nx, t = lin / g.nx, cy = t % g.ny, cz = t / g.ny;
+    double xi = sx[k], yi = sy[k], zi = sz[k];
+    int count = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy) {
+            int beg, end;
+            if (!row_range(g, cx, cy, cz, dy, dz, beg, end)) continue;
+            for (int mb = beg; mb < end; mb += 32) {
+                int m = mb + lane;
+                bool ok = false;
+                if (m < end && m != k) ok = xnorm2(xsub(sx[m], xi), xsub(sy[m], yi), xsub(sz[m], zi)) < re2;
+                count += __popc(__ballot_sync(0xffffffffu, ok));
             }
-        if (lane == 0) {
-            cnt[k] = min(count, maxn);
-            tr = count > maxn ? (unsigned long long)(count - maxn) : 0ull;
         }
-    }
-    if (lane == 0 && tr) atomicAdd(trunc_total, tr);
+    return count;
 }
 
-__global__ void __launch_bounds__(NB_WARPS * 32) k_fill(GridView g, const double* __restrict__ sx,
-                                                      const double* __restrict__ sy,
-                                                      const double* __restrict__ sz,
-                                                      const int* __restrict__ scell,
-                                                      const uint8_t* __restrict__ stype, int n,
-                                                      double re2, int maxn, double l0, int classify,
-                                                      const int* __restrict__ row,
-                                                      int* __restrict__ col, uint8_t* __restrict__ cls) {
-    int k = blockIdx.x * NB_WARPS + (threadIdx.x >> 5);
-    if (k >= n) return;
-    int lane = threadIdx.x & 31;
+__device__ __forceinline__ void fill_query_global(const GridView& g, const double* __restrict__ sx,
+                                                  const double* __restrict__ sy, const double* __restrict__ sz,
+                                                  const int* __restrict__ scell, const uint8_t* __restrict__ stype,
+                                                  int k, double re2, int maxn, double l0, int classify,
+                                                  const int* __restrict__ row, int* __restrict__ col,
+                                                  uint8_t* __restrict__ cls, int lane) {
     unsigned lt = (1u << lane) - 1u;
     int lin = scell[k];
     int cx = lin % g.nx, t = lin / g.nx, cy = t % g.ny, cz = t / g.ny;
@@ -283,6 +269,211 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_fill(GridView g, const double
     if (classify) {
         sec = __reduce_or_sync(0xffffffffu, sec);
         if (lane == 0) cls[k] = classify_rule(stype[k], min(written, maxn), sec, zi, l0);
+    }
+}
+
+// ---- staged passes: one block per segment of SEG cells along x, one thread per particle -----
+// The block copies the candidates of its 9 cell rows (cells cx0-1 .. cx1+1 of rows (cy+dy,
+// cz+dz)) into shared memory once, as FP32 positions relative to the segment's corner, plus
+// the row pointers of its own particles (a contiguous range of the sorted arrays). Each
+// thread then walks one particle's 9 row ranges (cells cx-1 .. cx+1 of each row, contiguous
+// in the sorted order) candidate by candidate, so its kept list comes out in the reference's
+// order without any cross-lane bookkeeping. Cells whose box is farther than re (plus a 1e-4
+// relative margin) are skipped. A candidate is accepted when its FP32 distance^2 is below
+// re^2 (1 - 2e-5) and rejected above re^2 (1 + 2e-5); in between the exact FP64 test on the
+// global positions decides. Coordinates lie within (SEG + 2) re of the corner, so the FP32
+// distance^2 is within 1e-5 re^2 of the exact one and the kept lists are the reference's bit
+// for bit. The sector bits of the classification use the FP32 differences when every sign
+// and |d| comparison they need is separated by more than 4e-6 re, else the exact FP64 ones.
+constexpr int SEG = 12;
+constexpr int SEG_THREADS = 128;
+constexpr int SEG_MAXC = 1536;  // staged candidates (24 KB)
+constexpr int SEG_MAXQ = 512;   // queries per segment
+
+struct SegGrid {
+    GridView g;
+    int3 g0;   // grid origin cell
+    double re;
+    int nsegx;
+};
+
+__device__ __forceinline__ bool sector_bits_f32(float dx, float dy, float dz, float margin, unsigned& bits) {
+    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    if (fminf(fminf(ax, ay), az) <= margin || fabsf(ax - ay) <= margin || fabsf(ax - az) <= margin ||
+        fabsf(ay - az) <= margin)
+        return false;
+    const int s = (ax >= ay && ax >= az) ? (dx >= 0 ? 0 : 1) : ((ay >= ax && ay >= az) ? (dy >= 0 ? 2 : 3) : (dz >= 0 ? 4 : 5));
+    const int o = 6 + (dx >= 0) + 2 * (dy >= 0) + 4 * (dz >= 0);
+    bits = (1u << s) | (1u << o);
+    return true;
+}
+
+// Non-empty segments of the grid, listed in any order (each segment's outputs are addressed
+// by its own particles, so the order does not affect the result).
+__global__ void k_list_segments(SegGrid G, long long nseg, int* __restrict__ list, int* __restrict__ count) {
+    const long long seg = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool nonempty = false;
+    if (seg < nseg) {
+        const int sxi = (int)(seg % G.nsegx);
+        const long long tt = seg / G.nsegx;
+        const int cy = (int)(tt % G.g.ny), cz = (int)(tt / G.g.ny);
+        const int cx0 = sxi * SEG, cx1 = min(cx0 + SEG, G.g.nx) - 1;
+        const int rowlin = (cz * G.g.ny + cy) * G.g.nx;
+        nonempty = G.g.cell_start[rowlin + cx0] != G.g.cell_start[rowlin + cx1 + 1];
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, nonempty);
+    int base = 0;
+    if ((threadIdx.x & 31) == 0 && bal) base = atomicAdd(count, __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (nonempty) list[base + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u))] = (int)seg;
+}
+
+// One accepted-or-band candidate of the thread's query (the rare path of the scan).
+template <bool FILL>
+__device__ __forceinline__ void seg_accept(float d2, float lo_th, float dx, float dy, float dz, int m, int k,
+                                           const double* __restrict__ sx, const double* __restrict__ sy,
+                                           const double* __restrict__ sz, double re2, int maxn, int room, int out0,
+                                           int classify, float margin, int* __restrict__ col, int& written,
+                                           unsigned& sec) {
+    if (m == k) return;
+    if (d2 >= lo_th && !(xnorm2(xsub(sx[m], sx[k]), xsub(sy[m], sy[k]), xsub(sz[m], sz[k])) < re2)) return;
+    if (FILL && written < maxn && written < room) {
+        col[out0 + written] = m;
+        if (classify) {
+            unsigned bb;
+            if (!sector_bits_f32(dx, dy, dz, margin, bb))
+                bb = sector_bits(xsub(sx[m], sx[k]), xsub(sy[m], sy[k]), xsub(sz[m], sz[k]));
+            sec |= bb;
+        }
+    }
+    ++written;
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_pass(SegGrid G, const int* __restrict__ seg_list,
+                                                            const double* __restrict__ sx,
+                                                            const double* __restrict__ sy,
+                                                            const double* __restrict__ sz,
+                                                            const int* __restrict__ scell,
+                                                            const uint8_t* __restrict__ stype, double re2,
+                                                            int maxn, double l0, int classify,
+                                                            int* __restrict__ cnt,
+                                                            unsigned long long* trunc_total,
+                                                            const int* __restrict__ row, int* __restrict__ col,
+                                                            uint8_t* __restrict__ cls) {
+    __shared__ float4 cf[SEG_MAXC];
+    __shared__ int qrow[SEG_MAXQ + 1];
+    __shared__ int rbase[10], rfirst[9], rcs[9][SEG + 3];
+    const float re_f = (float)G.re;
+    const float re2f = (float)re2;
+    const float lo_th = re2f * (1.f - 2e-5f), hi_th = re2f * (1.f + 2e-5f);
+    const float cull = re2f * (1.f + 1e-4f);
+    const float margin = 4e-6f * re_f;
+    const int seg = seg_list[blockIdx.x];
+    const int sxi = seg % G.nsegx, tt = seg / G.nsegx, cy = tt % G.g.ny, cz = tt / G.g.ny;
+    const int cx0 = sxi * SEG, cx1 = min(cx0 + SEG, G.g.nx) - 1;
+    const int lo = max(cx0 - 1, 0), hi = min(cx1 + 1, G.g.nx - 1);
+    const int rowlin = (cz * G.g.ny + cy) * G.g.nx;
+    const int q0 = G.g.cell_start[rowlin + cx0], q1 = G.g.cell_start[rowlin + cx1 + 1];
+    for (int t = threadIdx.x; t < 9 * (SEG + 3); t += blockDim.x) {
+        const int r = t / (SEG + 3), c = lo + t % (SEG + 3);
+        const int y = cy + (r % 3 - 1), z = cz + (r / 3 - 1);
+        int v = 0;
+        if (y >= 0 && y < G.g.ny && z >= 0 && z < G.g.nz && c <= hi + 1) v = G.g.cell_start[(z * G.g.ny + y) * G.g.nx + c];
+        rcs[r][c - lo] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rbase[0] = 0;
+        for (int r = 0; r < 9; ++r) {
+            rfirst[r] = rcs[r][0];
+            rbase[r + 1] = rbase[r] + (rcs[r][hi + 1 - lo] - rcs[r][0]);
+        }
+    }
+    __syncthreads();
+    const int total = rbase[9];
+    if (total > SEG_MAXC || q1 - q0 > SEG_MAXQ) {
+        // crowded neighborhood: the global-memory form, one query per warp
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int k = q0 + warp; k < q1; k += SEG_THREADS / 32) {
+            if (FILL) {
+                fill_query_global(G.g, sx, sy, sz, scell, stype, k, re2, maxn, l0, classify, row, col, cls, lane);
+            } else {
+                int c = count_query_global(G.g, sx, sy, sz, scell, k, re2, lane);
+                if (lane == 0) {
+                    cnt[k] = min(c, maxn);
+                    if (c > maxn) atomicAdd(trunc_total, (unsigned long long)(c - maxn));
+                }
+            }
+        }
+        return;
+    }
+    const double ox = (G.g0.x + cx0) * G.re, oy = (G.g0.y + cy) * G.re, oz = (G.g0.z + cz) * G.re;
+    for (int r = 0; r < 9; ++r) {  // row by row: consecutive threads load consecutive particles
+        const int n_r = rbase[r + 1] - rbase[r], f = rfirst[r], b = rbase[r];
+        for (int i = threadIdx.x; i < n_r; i += blockDim.x)
+            cf[b + i] = make_float4((float)(sx[f + i] - ox), (float)(sy[f + i] - oy), (float)(sz[f + i] - oz), 0.f);
+    }
+    if (FILL)
+        for (int i = threadIdx.x; i <= q1 - q0; i += blockDim.x) qrow[i] = row[q0 + i];
+    __syncthreads();
+    for (int k = q0 + threadIdx.x; k < q1; k += blockDim.x) {
+        int ck = cx0;
+        while (ck < cx1 && k >= rcs[4][ck + 1 - lo]) ++ck;
+        const float4 qf = cf[rbase[4] + (k - rfirst[4])];  // the query is staged in the centre row
+        const float qx = qf.x - (ck - cx0) * re_f;          // position inside its own cell (x)
+        int written = 0, out0 = 0, room = 0;
+        unsigned sec = 0;
+        if (FILL) {
+            out0 = qrow[k - q0];
+            room = qrow[k - q0 + 1] - out0;
+        }
+        for (int r = 0; r < 9; ++r) {
+            const int dy = r % 3 - 1, dz = r / 3 - 1;
+            const float gy = dy < 0 ? qf.y : (dy > 0 ? re_f - qf.y : 0.f);
+            const float gz = dz < 0 ? qf.z : (dz > 0 ? re_f - qf.z : 0.f);
+            const float gyz = gy * gy + gz * gz;
+            if (gyz > cull) continue;
+            // cells ck-1 .. ck+1 of this row, each kept when its box is within re
+            int clo = max(ck - 1, lo), chi = min(ck + 1, hi);
+            if (clo < ck && gyz + qx * qx > cull) clo = ck;
+            if (chi > ck && gyz + (re_f - qx) * (re_f - qx) > cull) chi = ck;
+            const int gb = rcs[r][clo - lo], ge = rcs[r][chi + 1 - lo];
+            const int sb = rbase[r] + (gb - rfirst[r]);
+            const int se = sb + (ge - gb);
+            const int mshift = rfirst[r] - rbase[r];  // global index = staged index + mshift
+            int si = sb;
+            for (; si + 4 <= se; si += 4) {
+                float d2[4], ddx[4], ddy[4], ddz[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float4 cj = cf[si + u];
+                    ddx[u] = cj.x - qf.x;
+                    ddy[u] = cj.y - qf.y;
+                    ddz[u] = cj.z - qf.z;
+                    d2[u] = ddx[u] * ddx[u] + ddy[u] * ddy[u] + ddz[u] * ddz[u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (d2[u] <= hi_th)
+                        seg_accept<FILL>(d2[u], lo_th, ddx[u], ddy[u], ddz[u], si + u + mshift, k, sx, sy, sz, re2,
+                                         maxn, room, out0, classify, margin, col, written, sec);
+            }
+            for (; si < se; ++si) {
+                const float4 cj = cf[si];
+                const float dx = cj.x - qf.x, dyf = cj.y - qf.y, dzf = cj.z - qf.z;
+                const float d2 = dx * dx + dyf * dyf + dzf * dzf;
+                if (d2 <= hi_th)
+                    seg_accept<FILL>(d2, lo_th, dx, dyf, dzf, si + mshift, k, sx, sy, sz, re2, maxn, room, out0,
+                                     classify, margin, col, written, sec);
+            }
+        }
+        if (FILL) {
+            if (classify) cls[k] = classify_rule(stype[k], min(written, maxn), sec, sz[k], l0);
+        } else {
+            cnt[k] = min(written, maxn);
+            if (written > maxn) atomicAdd(trunc_total, (unsigned long long)(written - maxn));
+        }
     }
 }
 
@@ -494,9 +685,23 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     unsigned long long* trunc_d = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 16);
     LSMPS_CUDA(cudaMemsetAsync(trunc_d, 0, sizeof(unsigned long long), s));
     GridView gv{cstart, gd.x, gd.y, gd.z};
-    unsigned nb_blocks = (unsigned)((n + NB_WARPS - 1) / NB_WARPS);
-    if (n) {
-        k_count<<<nb_blocks, NB_WARPS * 32, 0, s>>>(gv, sx, sy, sz, scell, (int)n, ctx->re2, maxn, cnt, trunc_d);
+    SegGrid sg{gv, g0, re, (gd.x + SEG - 1) / SEG};
+    const long long nseg = (long long)sg.nsegx * gd.y * gd.z;
+    LSMPS_REQUIRE(nseg < (1ll << 31), LSMPS_ERR_GRID, "too many cell segments");
+    int* seg_list = ctx->seg_list.ensure<int>(nseg + 1);
+    int* seg_count = ctx->scratch.get<int>() + 40;
+    LSMPS_CUDA(cudaMemsetAsync(seg_count, 0, sizeof(int), s));
+    k_list_segments<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(sg, nseg, seg_list, seg_count);
+    LSMPS_CHECK_LAUNCH();
+    int hsegs = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&hsegs, seg_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ctx->nsegs = hsegs;
+    const unsigned seg_grid = (unsigned)std::max(hsegs, 1);
+    if (n && hsegs) {
+        k_seg_pass<false><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
+                                                             ctx->re2, maxn, l0, 0, cnt, trunc_d, nullptr, nullptr,
+                                                             nullptr);
         LSMPS_CHECK_LAUNCH();
     }
     scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
@@ -514,9 +719,10 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     int* col = ctx->nbr_col.ensure<int>((size_t)hpairs + 1);
     uint8_t* cls = ctx->cls.ensure<uint8_t>(n);
     const int do_cls = (flags & LSMPS_NBR_CLASSIFY) ? 1 : 0;
-    if (n) {
-        k_fill<<<nb_blocks, NB_WARPS * 32, 0, s>>>(gv, sx, sy, sz, scell, stype, (int)n, ctx->re2, maxn, l0,
-                                                 do_cls, row, col, cls);
+    if (n && hsegs) {
+        k_seg_pass<true><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
+                                                            ctx->re2, maxn, l0, do_cls, nullptr, nullptr, row, col,
+                                                            cls);
         LSMPS_CHECK_LAUNCH();
     }
     ctx->have_neighbors = true;
@@ -531,27 +737,32 @@ void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* b
     cudaStream_t s = ctx->stream;
     int n = (int)ctx->n;
     GridView gv{ctx->cell_start.get<int>(), ctx->gdim[0], ctx->gdim[1], ctx->gdim[2]};
-    unsigned nb_blocks = (unsigned)((n + NB_WARPS - 1) / NB_WARPS);
+    SegGrid sg{gv, make_int3(ctx->gmin[0], ctx->gmin[1], ctx->gmin[2]), ctx->re, (ctx->gdim[0] + SEG - 1) / SEG};
     auto* trunc_d = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 16);
+    const int* seg_list = ctx->seg_list.get<int>();
+    const unsigned seg_grid = (unsigned)std::max(ctx->nsegs, 1);
     auto launch = [&] {
         if (kernel == LSMPS_KB_NBR_COUNT)
-            k_count<<<nb_blocks, NB_WARPS * 32, 0, s>>>(gv, ctx->sx.get<double>(), ctx->sy.get<double>(),
-                                                        ctx->sz.get<double>(), ctx->scell.get<int>(), n, ctx->re2,
-                                                        ctx->maxn, ctx->nbr_cnt.get<int>(), trunc_d);
+            k_seg_pass<false><<<seg_grid, SEG_THREADS, 0, s>>>(
+                sg, seg_list, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(), ctx->scell.get<int>(),
+                ctx->stype.get<uint8_t>(), ctx->re2, ctx->maxn, ctx->l0, 0, ctx->nbr_cnt.get<int>(), trunc_d, nullptr,
+                nullptr, nullptr);
         else
-            k_fill<<<nb_blocks, NB_WARPS * 32, 0, s>>>(gv, ctx->sx.get<double>(), ctx->sy.get<double>(),
-                                                       ctx->sz.get<double>(), ctx->scell.get<int>(),
-                                                       ctx->stype.get<uint8_t>(), n, ctx->re2, ctx->maxn, ctx->l0,
-                                                       ctx->have_classes ? 1 : 0, ctx->nbr_row.get<int>(),
-                                                       ctx->nbr_col.get<int>(), ctx->cls.get<uint8_t>());
+            k_seg_pass<true><<<seg_grid, SEG_THREADS, 0, s>>>(
+                sg, seg_list, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(), ctx->scell.get<int>(),
+                ctx->stype.get<uint8_t>(), ctx->re2, ctx->maxn, ctx->l0, ctx->have_classes ? 1 : 0, nullptr, nullptr,
+                ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), ctx->cls.get<uint8_t>());
         LSMPS_CHECK_LAUNCH();
     };
-    if (n == 0) { *ms = 0; *bytes = 0; return; }
+    if (n == 0 || ctx->nsegs == 0) { *ms = 0; *bytes = 0; return; }
     launch();  // warm
     ev_record(ctx, 14);
     for (int r = 0; r < reps; ++r) launch();
     ev_record(ctx, 15);
     *ms = ev_elapsed(ctx, 14, 15) / reps;
+    // algorithmic bytes: positions (24 B) and cell (4 B) of every particle once, cell starts;
+    // the count pass writes 4 B per particle, the fill pass reads types and row pointers and
+    // writes the columns and classes
     double N = (double)n, P = (double)ctx->pairs, cells = (double)ctx->ncells;
     *bytes = kernel == LSMPS_KB_NBR_COUNT ? 32.0 * N + 4.0 * cells : 34.0 * N + 4.0 * P + 4.0 * cells;
 }
