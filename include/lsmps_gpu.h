@@ -204,6 +204,25 @@ int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
  * (a, kx, ky, kz, phi). No reference counterpart beyond the fixed p* of the variants. */
 int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
 
+/* ---- residual check that allocates nothing ------------------------------------------ */
+/* No counterpart in the reference. out[v] = |b - A p_v|_2 for the nvec (1..8) device
+ * vectors p_v = d_p + v * ld (U doubles each, the reference's unknown numbering), and
+ * out[nvec] = |b|_2, written to the device buffer d_out (nvec + 1 doubles), over the
+ * assembled system. Enqueued on the context stream (lsmps_stream) and returns without
+ * waiting: order the producer of d_p before it and read d_out after lsmps_sync.
+ * It allocates nothing: no cudaMalloc / cudaFree and no context buffer growth. It is for
+ * callers that keep the pressure in their own device memory and check it inside a time
+ * loop that overlaps work on other streams, where an allocation would synchronise the
+ * device, or whose device memory is already in their own pool. The reduction scratch is
+ * one static device array of 42,880 bytes per device (partial sums of at most 592 blocks
+ * for at most 8 vectors); nvec outside 1..8 fails with LSMPS_ERR_ARG. Its ticket word must
+ * start at zero: each call clears it on the stream before the launch. The first call on a
+ * device resolves the array's address (cudaGetSymbolAddress, checked; it may load the
+ * module), so make that first call before any stream capture begins. The scratch is shared
+ * by every context on the device: calls whose executions overlap in time (two contexts, two
+ * streams, two threads) race on it and must be serialised by the caller. */
+int lsmps_ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
+
 /* ---- learned preconditioner (message-passing network over the PPE graph) ----------- */
 /* No reference counterpart. Nodes are the PPE unknowns, edges the
  * off-diagonal entries with weight -a_ij / a_ii. Input features per node: residual

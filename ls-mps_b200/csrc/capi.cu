@@ -284,6 +284,10 @@ int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
     return guarded(ctx, [&] { ppe_manufacture(ctx, params, nmodes); });
 }
 
+int lsmps_ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out) {
+    return guarded(ctx, [&] { ppe_residual_static(ctx, d_p, ld, nvec, d_out); });
+}
+
 size_t lsmps_mpnn_param_count(void) { return mpnn_param_count(); }
 
 int lsmps_mpnn_init(lsmps_ctx* ctx, uint32_t seed) {

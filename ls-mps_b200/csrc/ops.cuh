@@ -41,6 +41,7 @@ void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y);
 void mpnn_save(lsmps_ctx* ctx, const char* path);
 void mpnn_load(lsmps_ctx* ctx, const char* path);
 void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
+void ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
 
 // Profiling hooks behind lsmps_kernel_bench (mean ms per launch, algorithmic bytes).
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);

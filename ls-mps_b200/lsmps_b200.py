@@ -110,6 +110,7 @@ SIGNATURES = {
     "lsmps_download_ppe": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
+    "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
     "lsmps_mpnn_param_count": (C.c_size_t, []),
     "lsmps_mpnn_init": (C.c_int, [_vp, C.c_uint32]),
     "lsmps_mpnn_get_weights": (C.c_int, [_vp, _vp, C.c_size_t]),
