@@ -66,8 +66,26 @@ uint64_t lsmps_launch_count(void);
  *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL neighbor passes   24 N + 4 N (+ 4 P + 1 N fill)
  *   LSMPS_KB_WLS     all-particle WLS            24 N + 4 P + 80 N (z, sum w, status)
  * No reference counterpart (the reference has no GPU path). */
-enum { LSMPS_KB_SPMV64 = 0, LSMPS_KB_SPMV32 = 1, LSMPS_KB_NBR_COUNT = 2, LSMPS_KB_NBR_FILL = 3, LSMPS_KB_WLS = 4 };
+enum {
+    LSMPS_KB_SPMV64 = 0,
+    LSMPS_KB_SPMV32 = 1,
+    LSMPS_KB_NBR_COUNT = 2,
+    LSMPS_KB_NBR_FILL = 3,
+    LSMPS_KB_WLS = 4,
+    LSMPS_KB_MPNN_LAYER = 5 /* one message-passing layer (aggregation + 64x128 tensor-core GEMM) of the
+                               loaded network over the assembled PPE graph: 256 U + 8 Z */
+};
 int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
+
+/* Launch-shape autotuner. Kernels whose launch shapes (grid size, block size, loads in
+ * flight) all give the same bits time each shape once on the live data at their first use
+ * per problem-size class (floor(log2 n)) and keep the fastest for the context: the network's
+ * message-passing layer and the all-particle WLS. mode 0: off (fixed default shapes), 1: on
+ * (default), 2: on and forget earlier choices. No reference counterpart. */
+int lsmps_set_autotune(lsmps_ctx* ctx, int mode);
+/* The tuner's table as text, one line per candidate: "kernel n~2^k<TAB>shape<TAB>ms[<TAB>best]".
+ * Writes at most cap bytes (NUL-terminated) to buf; *needed gets the full size + 1. */
+int lsmps_autotune_report(lsmps_ctx* ctx, char* buf, size_t cap, size_t* needed);
 
 /* ---- particles -------------------------------------------------------------------- */
 /* xyz: n x 3 doubles (x, y, z interleaved, as the reference's Particle::r); type: n

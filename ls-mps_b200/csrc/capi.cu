@@ -164,8 +164,30 @@ int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_laun
             nb_kernel_bench(ctx, kernel, reps, ms_per_launch, bytes_per_launch);
         else if (kernel == LSMPS_KB_WLS)
             wls_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
+        else if (kernel == LSMPS_KB_MPNN_LAYER)
+            mpnn_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
         else
             throw Error{LSMPS_ERR_ARG, "unknown kernel id"};
+    });
+}
+
+int lsmps_set_autotune(lsmps_ctx* ctx, int mode) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(mode >= 0 && mode <= 2, LSMPS_ERR_ARG, "autotune mode must be 0, 1 or 2");
+        ctx->tuner.enabled = mode != 0;
+        if (mode == 2) ctx->tuner.table.clear();
+    });
+}
+
+int lsmps_autotune_report(lsmps_ctx* ctx, char* buf, size_t cap, size_t* needed) {
+    return guarded(ctx, [&] {
+        const std::string r = autotune_report(ctx);
+        if (needed) *needed = r.size() + 1;
+        if (buf && cap) {
+            const size_t k = std::min(cap - 1, r.size());
+            std::memcpy(buf, r.data(), k);
+            buf[k] = 0;
+        }
     });
 }
 

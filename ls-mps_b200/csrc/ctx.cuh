@@ -17,6 +17,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -24,7 +25,19 @@
 
 namespace lsmps_gpu {
 struct MpnnState;
-}
+
+// Autotuner table of one context: per "kernel n~2^k" key, the candidate launch shapes,
+// their measured ms per launch and the chosen one.
+struct TuneResult {
+    std::vector<std::string> names;
+    std::vector<float> ms;
+    int best = 0;
+};
+struct Tuner {
+    bool enabled = true;
+    std::map<std::string, TuneResult> table;
+};
+}  // namespace lsmps_gpu
 
 struct lsmps_ctx {
     int device = 0;
@@ -83,6 +96,8 @@ struct lsmps_ctx {
     // ---- learned preconditioner (weights, training store, workspace) ----
     lsmps_gpu::MpnnState* mpnn = nullptr;
     long long assembly_gen = 0;  // bumped by every PPE assembly
+
+    lsmps_gpu::Tuner tuner;  // launch shapes chosen by the autotuner
 
     void* pinned = nullptr;
     size_t pinned_bytes = 0;

@@ -99,26 +99,47 @@ __device__ __forceinline__ unsigned a_addr(const bf16* tile, int ld, int k0, int
 }
 
 // ---- graph construction from the assembled PPE ---------------------------------------
+// warp per row (grid-stride), lanes over the row's entries
 __global__ void k_graph_ew(long long U, const int* __restrict__ row, const double* __restrict__ val,
                            const double* __restrict__ dinv, float* __restrict__ ew) {
-    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (u >= U) return;
-    const int e0 = row[u], e1 = row[u + 1];
-    const double di = dinv[u];
-    for (int e = e0; e < e1 - 1; ++e) ew[e] = (float)(-val[e] * di);
-    ew[e1 - 1] = 0.f;  // the diagonal is the row's last entry
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long u = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; u < U; u += nw) {
+        const int e0 = row[u], e1 = row[u + 1];
+        const double di = dinv[u];
+        for (int e = e0 + lane; e < e1; e += 32) ew[e] = e < e1 - 1 ? (float)(-val[e] * di) : 0.f;  // diagonal last
+    }
 }
 
-__global__ void k_mean_diag(long long U, const double* __restrict__ dinv, double* out) {
-    __shared__ double part[32];
+constexpr int MEAN_BLOCKS = 592;
+
+// mean of a_uu = 1 / dinv_u (1 where dinv is 0): per-block sums, then one block adds them
+// in block order (deterministic)
+__global__ void k_diag_partials(long long U, const double* __restrict__ dinv, double* part) {
+    __shared__ double ws[8];
     double acc = 0;
-    for (long long i = threadIdx.x; i < U; i += blockDim.x) acc += dinv[i] != 0 ? 1.0 / dinv[i] : 1.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < U; i += (long long)gridDim.x * blockDim.x)
+        acc += dinv[i] != 0 ? 1.0 / dinv[i] : 1.0;
     acc = warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += ws[k];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_mean_finish(long long U, const double* __restrict__ part, int nparts, double* out) {
+    __shared__ double ws[8];
+    double acc = 0;
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) acc += part[k];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += ws[k];
         *out = U ? t / (double)U : 1.0;
     }
 }
@@ -183,6 +204,8 @@ __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ 
 //      staged with h_i as the bf16 A tile [h | m] (16 x 128) in shared memory;
 //   2. z = [h | m] W^T on the tensor cores (8 k-steps x 8 n-tiles of m16n8k16);
 //   3. h_out = h + ReLU(z + b) (bf16), with [h | m] and z kept for the backward pass.
+// 2 NB neighbor-row gathers in flight per warp (a launch-shape parameter: same bits for every NB)
+template <int NB>
 __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out,
                                                    const bf16* __restrict__ Wl, const float* __restrict__ bl,
                                                    bf16* __restrict__ a_save, float* __restrict__ z_save) {
@@ -201,31 +224,79 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
     const long long ntiles = (G.U + 15) / 16;
     for (long long tile = blockIdx.x * 4LL + warp; tile < ntiles; tile += gridDim.x * 4LL) {
         const long long base = tile * 16;
+        // row pointers of the tile's 16 nodes in one load (row has U + 1 entries)
+        const int rp = lane <= 16 ? G.row[min(base + lane, G.U)] : 0;
+        // (col, weight) of up to 32 edges of node t, one per lane; the diagonal (the row's last
+        // entry) has no edge
+        auto fetch = [&](int t, int& cj, float& wj, int& ne, int& e0) {
+            e0 = __shfl_sync(0xffffffffu, rp, t);
+            ne = max(__shfl_sync(0xffffffffu, rp, t + 1) - 1 - e0, 0);
+            cj = 0;
+            wj = 0.f;
+            if (lane < min(ne, 32)) {
+                cj = G.col[e0 + lane];
+                wj = G.ew[e0 + lane];
+            }
+        };
+        const int half = lane >> 4, sub = lane & 15;  // half-warp per neighbor row, 4 features per lane
+        int cj, ne, e0;
+        float wj;
+        fetch(0, cj, wj, ne, e0);
         for (int t = 0; t < 16; ++t) {
             const long long i = base + t;
+            int cjn = 0, nen = 0, e0n = 0;
+            float wjn = 0.f;
+            if (t < 15) fetch(t + 1, cjn, wjn, nen, e0n);  // in flight during node t's gathers
             __nv_bfloat162 own = __floats2bfloat162_rn(0.f, 0.f);
-            float m0 = 0.f, m1 = 0.f;
-            if (i < G.U) {
-                own = *reinterpret_cast<const __nv_bfloat162*>(h_in + i * H + 2 * lane);
-                const int e0 = G.row[i], e1 = G.row[i + 1] - 1;  // the diagonal (last) has no edge
-                int e = e0;
-                for (; e + 2 <= e1; e += 2) {
-                    const int j0 = G.col[e], j1 = G.col[e + 1];
-                    const float w0 = G.ew[e], w1 = G.ew[e + 1];
-                    const float2 a0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)j0 * H + 2 * lane));
-                    const float2 a1 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)j1 * H + 2 * lane));
-                    m0 += w0 * a0.x + w1 * a1.x;
-                    m1 += w0 * a0.y + w1 * a1.y;
+            if (i < G.U) own = *reinterpret_cast<const __nv_bfloat162*>(h_in + i * H + 2 * lane);
+            float m[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int eb = 0; eb < ne; eb += 32) {
+                if (eb) {  // rows of more than 32 edges
+                    cj = 0;
+                    wj = 0.f;
+                    if (lane < min(ne - eb, 32)) {
+                        cj = G.col[e0 + eb + lane];
+                        wj = G.ew[e0 + eb + lane];
+                    }
                 }
-                if (e < e1) {
-                    const float w0 = G.ew[e];
-                    const float2 a0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(h_in + (long long)G.col[e] * H + 2 * lane));
-                    m0 += w0 * a0.x;
-                    m1 += w0 * a0.y;
+                const int nb = min(32, ne - eb);
+                for (int k = 0; k < nb; k += 2 * NB) {
+                    uint2 a[NB];
+                    float w[NB];
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) {
+                        const int edge = k + 2 * q + half;
+                        const int src = min(edge, nb - 1);
+                        const int j = __shfl_sync(0xffffffffu, cj, src);
+                        const float wq = __shfl_sync(0xffffffffu, wj, src);
+                        w[q] = edge < nb ? wq : 0.f;
+                        a[q] = *reinterpret_cast<const uint2*>(h_in + (long long)j * H + 4 * sub);
+                    }
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) {
+                        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a[q].x));
+                        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a[q].y));
+                        m[0] += w[q] * lo.x;
+                        m[1] += w[q] * lo.y;
+                        m[2] += w[q] * hi.x;
+                        m[3] += w[q] * hi.y;
+                    }
                 }
             }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) m[c] += __shfl_xor_sync(0xffffffffu, m[c], 16);  // even + odd edges
             *reinterpret_cast<__nv_bfloat162*>(A + t * LDA + 2 * lane) = own;
-            *reinterpret_cast<__nv_bfloat162*>(A + t * LDA + H + 2 * lane) = __floats2bfloat162_rn(m0, m1);
+            if (half == 0) {
+                __nv_bfloat162 p0 = __floats2bfloat162_rn(m[0], m[1]), p1 = __floats2bfloat162_rn(m[2], m[3]);
+                uint2 pk;
+                pk.x = *reinterpret_cast<unsigned*>(&p0);
+                pk.y = *reinterpret_cast<unsigned*>(&p1);
+                *reinterpret_cast<uint2*>(A + t * LDA + H + 4 * sub) = pk;
+            }
+            cj = cjn;
+            wj = wjn;
+            ne = nen;
+            e0 = e0n;
         }
         __syncwarp();
         float acc[8][4];
@@ -710,10 +781,13 @@ static void build_graph(lsmps_ctx* ctx, MpnnGraph& g, bool copy_structure) {
     float* feat = g.feat.ensure<float>(3 * U + 3);
     float* dg = g.dg.ensure<float>(U + 1);
     double* mean = ctx->scratch.get<double>() + 24;
+    double* part = ctx->scratch.get<double>() + 1024;  // MEAN_BLOCKS doubles of the 2048-double scratch
     if (U) {
-        k_graph_ew<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_val.get<double>(),
-                                                     ctx->A_dinv.get<double>(), ew);
-        k_mean_diag<<<1, 1024, 0, s>>>(U, ctx->A_dinv.get<double>(), mean);
+        k_graph_ew<<<148 * 8, 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_val.get<double>(),
+                                          ctx->A_dinv.get<double>(), ew);
+        k_diag_partials<<<MEAN_BLOCKS, 256, 0, s>>>(U, ctx->A_dinv.get<double>(), part);
+        k_mean_finish<<<1, 256, 0, s>>>(U, part, MEAN_BLOCKS, mean);
+        note_launches(2);
         k_graph_feat<<<blocks_for(U, 256), 256, 0, s>>>(U, ctx->A_row.get<int>(), ctx->A_dinv.get<double>(),
                                                        ctx->cls.get<uint8_t>(), ctx->sorted_of_u.get<int>(), mean, feat,
                                                        dg);
@@ -742,24 +816,52 @@ static void ensure_workspace(MpnnState& S, long long U, bool training) {
     S.cap = cap;
 }
 
+// Launch shapes of the message-passing layer: gathers in flight x blocks per SM (4 warps each).
+constexpr int LAYER_NB[3] = {2, 4, 8};
+constexpr int LAYER_BPS[4] = {2, 3, 4, 6};
+
+static void launch_layer(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool training, int c, int l) {
+    const unsigned lgrid = std::min<unsigned>((unsigned)((G.U + 63) / 64), 148u * LAYER_BPS[c % 4]);
+    const float* w = S.dw.get<float>();
+    const bf16* wbf = S.wbf.get<bf16>();
+    const bf16* hin = S.h[l].get<bf16>();
+    bf16* hout = S.h[l + 1].get<bf16>();
+    const bf16* W = wbf + l * H * KIN;
+    const float* b = w + OFF_L0 + l * LSTRIDE + H * KIN;
+    bf16* as = training ? S.a[l].get<bf16>() : nullptr;
+    float* zs = training ? S.z[l + 1].get<float>() : nullptr;
+    cudaStream_t s = ctx->stream;
+    switch (LAYER_NB[c / 4]) {
+        case 2: k_layer_fwd<2><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
+        case 4: k_layer_fwd<4><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
+        default: k_layer_fwd<8><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
+    }
+    LSMPS_CHECK_LAUNCH();
+}
+
+// The autotuned launch shape of the layer for this graph size (layer 0 is the timed launch:
+// it reads h[0] and writes h[1], so repeating it is harmless).
+static int layer_shape(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool training) {
+    static const std::vector<std::string> names = [] {
+        std::vector<std::string> v;
+        for (int nb : LAYER_NB)
+            for (int bps : LAYER_BPS) v.push_back("gathers" + std::to_string(nb) + "/blocks" + std::to_string(bps) + "xSM");
+        return v;
+    }();
+    return autotune(ctx, "mpnn_layer_fwd", G.U, names, 2, [&](int c) { launch_layer(ctx, S, G, training, c, 0); });
+}
+
 // Forward pass over graph g for input r (float, unit norm); y in S.y.
 static void forward(lsmps_ctx* ctx, MpnnState& S, const GView& G, const float* r, bool training) {
     cudaStream_t s = ctx->stream;
     ensure_workspace(S, G.U, training);
     if (!G.U) return;
     const float* w = S.dw.get<float>();
-    const bf16* wbf = S.wbf.get<bf16>();
     const unsigned grid = std::min<unsigned>(blocks_for(G.U, 256), 148 * 8);
     k_enc<<<grid, 256, 0, s>>>(G, r, w, S.h[0].get<bf16>(), training ? S.z[0].get<float>() : nullptr);
     LSMPS_CHECK_LAUNCH();
-    const unsigned lgrid = std::min<unsigned>((unsigned)((G.U + 63) / 64), 148 * 4);
-    for (int l = 0; l < NL; ++l) {
-        k_layer_fwd<<<lgrid, 128, 0, s>>>(G, S.h[l].get<bf16>(), S.h[l + 1].get<bf16>(), wbf + l * H * KIN,
-                                          w + OFF_L0 + l * LSTRIDE + H * KIN,
-                                          training ? S.a[l].get<bf16>() : nullptr,
-                                          training ? S.z[l + 1].get<float>() : nullptr);
-        LSMPS_CHECK_LAUNCH();
-    }
+    const int c = layer_shape(ctx, S, G, training);
+    for (int l = 0; l < NL; ++l) launch_layer(ctx, S, G, training, c, l);
     k_dec<<<grid, 256, 0, s>>>(G, S.h[NL].get<bf16>(), w, S.y.get<float>());
     LSMPS_CHECK_LAUNCH();
 }
@@ -934,6 +1036,28 @@ void mpnn_warm_start(lsmps_ctx* ctx, const float* rhs, float* y) {
     GView G = view(S.infer);
     forward(ctx, S, G, rhs, false);
     LSMPS_CUDA(cudaMemcpyAsync(y, S.y.get<float>(), G.U * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+// One message-passing layer (layer 0, the tuned shape) on the current assembled system with
+// the loaded weights; input features from the unit right-hand side b / |b|.
+void mpnn_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes) {
+    MpnnState& S = state(ctx);
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "layer bench needs an assembled system");
+    const long long U = ctx->U;
+    if (U == 0) { *ms = 0; *bytes = 0; return; }
+    float* rf = ctx->fph.ensure<float>(U + 1);
+    float* yf = ctx->fx.ensure<float>(U + 1);
+    std::vector<float> ones((size_t)U, (float)(1.0 / std::sqrt((double)U)));
+    LSMPS_CUDA(cudaMemcpyAsync(rf, ones.data(), U * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    mpnn_warm_start(ctx, rf, yf);  // graph, h[0], tuned shape
+    GView G = view(S.infer);
+    const int c = layer_shape(ctx, S, G, false);
+    launch_layer(ctx, S, G, false, c, 0);
+    ev_record(ctx, 14);
+    for (int r = 0; r < reps; ++r) launch_layer(ctx, S, G, false, c, 0);
+    ev_record(ctx, 15);
+    *ms = ev_elapsed(ctx, 14, 15) / reps;
+    *bytes = 256.0 * U + 8.0 * ctx->nnz;
 }
 
 void mpnn_infer(lsmps_ctx* ctx, const double* r_ref, double* y_ref) {

@@ -1,5 +1,7 @@
 // Internal entry points of the library's phases (called by the C ABI in capi.cu).
 #pragma once
+#include <functional>
+
 #include "ctx.cuh"
 
 namespace lsmps_gpu {
@@ -47,8 +49,19 @@ void ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec,
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
 void wls_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
 void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
+void mpnn_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
 
 // Timing helpers: record event `slot` on the context stream.
+// Launch-shape autotuner. For a kernel whose candidate launch shapes all compute the same
+// bits and whose launches are idempotent: at the first call for (kernel, size class of n =
+// floor(log2 n)) each candidate is launched once to warm and `reps` times between CUDA events
+// on the context stream, and the fastest is kept in the context. Returns the candidate to
+// launch. With tuning off or while the stream is captured it returns the stored choice if
+// any, else `fallback`. launch(c) enqueues candidate c on the context stream.
+int autotune(lsmps_ctx* ctx, const char* kernel, long long n, const std::vector<std::string>& names, int fallback,
+             const std::function<void(int)>& launch, int reps = 2);
+std::string autotune_report(lsmps_ctx* ctx);
+
 void ev_record(lsmps_ctx* ctx, int slot);
 double ev_elapsed(lsmps_ctx* ctx, int a, int b);
 

@@ -743,18 +743,19 @@ __global__ void __launch_bounds__(RB, 6) k_replace_residual(Sell<double> A, cons
     }
 }
 
-// |b|^2 into scal[0]: one block, fixed order (once per learned solve)
-__global__ void k_norm2_one_block(long long n, const double* __restrict__ b, double* scal) {
-    __shared__ double part[32];
+// |b|^2 into scal[0], fixed-order partials (once per learned solve)
+__global__ void __launch_bounds__(RB) k_norm2(long long n, const double* __restrict__ b, double* scal, Partials P,
+                                              unsigned int* counter) {
     double acc = 0;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc += b[i] * b[i];
-    acc = warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tot += part[k];
-        scal[0] = tot;
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB)
+        acc += b[i] * b[i];
+    if (block_partials(acc, 0.0, P, counter)) {
+        double tot, unused;
+        final_sum(P, &tot, &unused);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            scal[0] = tot;
+        }
     }
 }
 
@@ -1198,7 +1199,7 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         float* rhs = ctx->fph.ensure<float>(U + 1);
         float* yf = ctx->fx.ensure<float>(U + 1);
         double* scal = engine_scalars(ctx);
-        k_norm2_one_block<<<1, 1024, 0, s>>>(U, b, scal);
+        k_norm2<<<RGRID, RB, 0, s>>>(U, b, scal, E.P, &E.S->counter[5]);
         k_rhs_unit<<<1184, 256, 0, s>>>(U, b, rhs, scal);  // network input: b / |b| in FP32
         LSMPS_CHECK_LAUNCH();
         mpnn_warm_start(ctx, rhs, yf);

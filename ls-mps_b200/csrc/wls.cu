@@ -510,15 +510,28 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
     }
 }
 
+// Block sizes the autotuner chooses from (one particle per thread: same bits for each).
+constexpr int WLS_BLOCK[3] = {32, 64, 128};
+
 template <int NRHS, int PREC>
 void launch_all(lsmps_ctx* ctx, const WlsParams& P, unsigned long long* gcnt, double* gsum) {
     int n = (int)ctx->n;
     if (!n) return;
-    k_wls_all<NRHS, PREC><<<blocks_for(n, 128), 128, 0, ctx->stream>>>(
-        P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
-        ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), ctx->wls_status.get<int>(), ctx->wls_z.get<double>(),
-        ctx->wls_wsum.get<double>(), ctx->wls_x.get<double>(), gcnt, gsum);
-    LSMPS_CHECK_LAUNCH();
+    auto go = [&](int c) {
+        const int t = WLS_BLOCK[c];
+        k_wls_all<NRHS, PREC><<<blocks_for(n, t), t, 0, ctx->stream>>>(
+            P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
+            ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), ctx->wls_status.get<int>(), ctx->wls_z.get<double>(),
+            ctx->wls_wsum.get<double>(), ctx->wls_x.get<double>(), gcnt, gsum);
+        LSMPS_CHECK_LAUNCH();
+    };
+    static const std::vector<std::string> names = {"block32", "block64", "block128"};
+    const std::string key = "wls_all nrhs" + std::to_string(NRHS) + (PREC ? " mixed" : " fp64");
+    const size_t tuned_before = ctx->tuner.table.size();
+    const int c = autotune(ctx, key.c_str(), n, names, 2, go);
+    if (ctx->tuner.table.size() != tuned_before)  // the timed launches added to the statistics
+        LSMPS_CUDA(cudaMemsetAsync(gcnt, 0, 16 * sizeof(double), ctx->stream));
+    go(c);
 }
 
 // Back to caller order (wls arrays are kept in sorted order).

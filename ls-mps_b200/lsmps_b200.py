@@ -22,7 +22,7 @@ INTERIOR, FREE_SURFACE, SPLASH, NEAR_WALL, WALL = range(5)
 NBR_CLASSIFY = 1
 PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
 SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED, SOLVER_MIXED_F32 = range(6)
-KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS = range(5)
+KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER = range(6)
 SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4, "mixed_f32": 5}
 VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}
 
@@ -111,6 +111,8 @@ SIGNATURES = {
     "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
+    "lsmps_set_autotune": (C.c_int, [_vp, C.c_int]),
+    "lsmps_autotune_report": (C.c_int, [_vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "lsmps_mpnn_param_count": (C.c_size_t, []),
     "lsmps_mpnn_init": (C.c_int, [_vp, C.c_uint32]),
     "lsmps_mpnn_get_weights": (C.c_int, [_vp, _vp, C.c_size_t]),
@@ -215,6 +217,22 @@ class Context:
         ms, nb = C.c_double(), C.c_double()
         self._check(self.L.lsmps_kernel_bench(self.h, kernel, reps, C.byref(ms), C.byref(nb)))
         return ms.value, nb.value
+
+    def set_autotune(self, mode):
+        """0 off (fixed default launch shapes), 1 on, 2 on and forget earlier choices."""
+        self._check(self.L.lsmps_set_autotune(self.h, mode))
+
+    def autotune_report(self):
+        """[(key, shape, ms, is_best)] of every candidate the autotuner timed on this context."""
+        need = C.c_size_t()
+        self._check(self.L.lsmps_autotune_report(self.h, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value)
+        self._check(self.L.lsmps_autotune_report(self.h, buf, need.value, C.byref(need)))
+        out = []
+        for line in buf.value.decode().splitlines():
+            f = line.split("\t")
+            out.append((f[0], f[1], float(f[2]), len(f) > 3))
+        return out
 
     def upload(self, xyz, types):
         self._xyz = np.ascontiguousarray(xyz, dtype=np.float64)
