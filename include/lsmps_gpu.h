@@ -119,6 +119,23 @@ int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l
 /* classify() (src/lsmps.cpp:27) over the current neighbor lists, standalone. */
 int lsmps_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
 
+/* Neighbor lists with a skin (Verlet lists), for step series that move an unchanged particle
+ * set. lsmps_build_neighbors_skin builds candidate lists of radius re + skin (at most
+ * max_candidates per particle; LSMPS_ERR_ARG if any would be dropped) and from them the exact
+ * lists of radius re, as lsmps_build_neighbors does. Then, per step, lsmps_update_positions
+ * (same particles, same order) and lsmps_refresh_neighbors re-derive the exact lists by
+ * filtering the candidates with the build's own test (src/lsmps.cpp:26): the same neighbor
+ * sets as a fresh build, rows in ascending index of the candidate build's numbering.
+ * refresh returns LSMPS_ERR_STATE once a particle has moved more than skin / 2 since the
+ * candidate build (rebuild then); lsmps_max_displacement reports that distance. No reference
+ * counterpart (the reference's cnl_rebuild_interval key is not parsed by it). */
+int lsmps_build_neighbors_skin(lsmps_ctx* ctx, double re, double skin, int max_neighbors, int max_candidates,
+                               double l0, int flags, lsmps_neighbor_stats* out);
+int lsmps_update_positions(lsmps_ctx* ctx, const double* xyz, size_t n);
+int lsmps_update_positions_device(lsmps_ctx* ctx, const double* d_xyz, size_t n);
+int lsmps_refresh_neighbors(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out);
+int lsmps_max_displacement(lsmps_ctx* ctx, double* out);
+
 /* ---- WLS -------------------------------------------------------------------------- */
 typedef struct lsmps_wls_opts {
     double re, l0;
@@ -214,6 +231,17 @@ int lsmps_download_ppe(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, 
                        double* x_exact, int32_t* unknown_particle);
 /* Solution of the last solve (U, reference numbering). */
 int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+
+/* Per-particle pressure (n values, caller order) for step series whose unknowns change from
+ * step to step. set_initial_pressure: the next lsmps_ppe_solve with warm_start = 1 starts from
+ * these values at the unknowns (call after lsmps_ppe_assemble). download_pressure_particles:
+ * the last solution at the unknowns' particles, `fill` at the others (NaN: the others keep the
+ * values the buffer holds). No reference counterpart (the reference solves one snapshot from
+ * zero, src/lsmps.cpp:67). */
+int lsmps_set_initial_pressure(lsmps_ctx* ctx, const double* p, size_t n);
+int lsmps_set_initial_pressure_device(lsmps_ctx* ctx, const double* d_p, size_t n);
+int lsmps_download_pressure_particles(lsmps_ctx* ctx, double* p, size_t n, double fill);
+int lsmps_download_pressure_particles_device(lsmps_ctx* ctx, double* d_p, size_t n, double fill);
 
 /* ---- manufactured right-hand sides ------------------------------------------------ */
 /* p* = c0 + sum_m a_m sin(kx_m x + ky_m y + kz_m z + phi_m) + gz z over the unknowns'

@@ -56,6 +56,29 @@ __global__ void k_pack_particles(const double* __restrict__ xyz, size_t n, doubl
 }
 }  // namespace
 
+void particles_upload(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n, bool device) {
+    LSMPS_REQUIRE(n == 0 || (xyz && type), LSMPS_ERR_ARG, "null particle buffers");
+    LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
+    ev_record(ctx, 0);
+    double* pos = ctx->pos.ensure<double>(3 * n + 1);
+    uint8_t* t = ctx->type_in.ensure<uint8_t>(n + 1);
+    if (n) {
+        if (device) {
+            k_pack_particles<<<blocks_for(3 * n, 256), 256, 0, ctx->stream>>>(xyz, n, pos);
+            LSMPS_CHECK_LAUNCH();
+            LSMPS_CUDA(cudaMemcpyAsync(t, type, n, cudaMemcpyDeviceToDevice, ctx->stream));
+        } else {
+            LSMPS_CUDA(cudaMemcpyAsync(pos, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            LSMPS_CUDA(cudaMemcpyAsync(t, type, n, cudaMemcpyHostToDevice, ctx->stream));
+        }
+    }
+    ev_record(ctx, 1);
+    ctx->n = n;
+    ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+    ctx->have_candidates = false;
+    ctx->timings[0] = ev_elapsed(ctx, 0, 1);
+}
+
 }  // namespace lsmps_gpu
 
 using namespace lsmps_gpu;
@@ -121,6 +144,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->type_in, &ctx->cell_of, &ctx->slot, &ctx->cell_count, &ctx->cell_start,
                                  &ctx->perm, &ctx->iperm, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->stype,
                                  &ctx->scell, &ctx->cls, &ctx->nbr_cnt, &ctx->nbr_row, &ctx->nbr_col, &ctx->seg_list,
+                                 &ctx->cand_row, &ctx->cand_col, &ctx->ref_sx, &ctx->ref_sy, &ctx->ref_sz,
                                  &ctx->nbr_stats, &ctx->wls_status, &ctx->wls_z, &ctx->wls_wsum, &ctx->wls_x,
                                  &ctx->wls_stats, &ctx->wls_sample, &ctx->ref_rank, &ctx->u_of_sorted,
                                  &ctx->sorted_of_u, &ctx->ref_of_u, &ctx->u_of_ref, &ctx->A_row, &ctx->A_col,
@@ -192,40 +216,11 @@ int lsmps_autotune_report(lsmps_ctx* ctx, char* buf, size_t cap, size_t* needed)
 }
 
 int lsmps_upload_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n) {
-    return guarded(ctx, [&] {
-        LSMPS_REQUIRE(n == 0 || (xyz && type), LSMPS_ERR_ARG, "null particle buffers");
-        LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
-        ev_record(ctx, 0);
-        double* pos = ctx->pos.ensure<double>(3 * n + 1);
-        uint8_t* t = ctx->type_in.ensure<uint8_t>(n + 1);
-        if (n) {
-            LSMPS_CUDA(cudaMemcpyAsync(pos, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-            LSMPS_CUDA(cudaMemcpyAsync(t, type, n, cudaMemcpyHostToDevice, ctx->stream));
-        }
-        ev_record(ctx, 1);
-        ctx->n = n;
-        ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
-        ctx->timings[0] = ev_elapsed(ctx, 0, 1);
-    });
+    return guarded(ctx, [&] { particles_upload(ctx, xyz, type, n, false); });
 }
 
 int lsmps_upload_particles_device(lsmps_ctx* ctx, const double* d_xyz, const uint8_t* d_type, size_t n) {
-    return guarded(ctx, [&] {
-        LSMPS_REQUIRE(n == 0 || (d_xyz && d_type), LSMPS_ERR_ARG, "null particle buffers");
-        LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
-        ev_record(ctx, 0);
-        double* pos = ctx->pos.ensure<double>(3 * n + 1);
-        uint8_t* t = ctx->type_in.ensure<uint8_t>(n + 1);
-        if (n) {
-            k_pack_particles<<<blocks_for(3 * n, 256), 256, 0, ctx->stream>>>(d_xyz, n, pos);
-            LSMPS_CHECK_LAUNCH();
-            LSMPS_CUDA(cudaMemcpyAsync(t, d_type, n, cudaMemcpyDeviceToDevice, ctx->stream));
-        }
-        ev_record(ctx, 1);
-        ctx->n = n;
-        ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
-        ctx->timings[0] = ev_elapsed(ctx, 0, 1);
-    });
+    return guarded(ctx, [&] { particles_upload(ctx, d_xyz, d_type, n, true); });
 }
 
 int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l0, int flags,
@@ -235,6 +230,40 @@ int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l
         nb_build(ctx, re, max_neighbors, l0, flags, out);
         ev_record(ctx, 3);
         ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+    });
+}
+
+int lsmps_build_neighbors_skin(lsmps_ctx* ctx, double re, double skin, int max_neighbors, int max_candidates,
+                               double l0, int flags, lsmps_neighbor_stats* out) {
+    return guarded(ctx, [&] {
+        ev_record(ctx, 2);
+        nb_build_skin(ctx, re, skin, max_neighbors, max_candidates, l0, flags, out);
+        ev_record(ctx, 3);
+        ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+    });
+}
+
+int lsmps_update_positions(lsmps_ctx* ctx, const double* xyz, size_t n) {
+    return guarded(ctx, [&] { nb_update_positions(ctx, xyz, n, false); });
+}
+
+int lsmps_update_positions_device(lsmps_ctx* ctx, const double* d_xyz, size_t n) {
+    return guarded(ctx, [&] { nb_update_positions(ctx, d_xyz, n, true); });
+}
+
+int lsmps_refresh_neighbors(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out) {
+    return guarded(ctx, [&] {
+        ev_record(ctx, 2);
+        nb_refresh(ctx, flags, out);
+        ev_record(ctx, 3);
+        ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+    });
+}
+
+int lsmps_max_displacement(lsmps_ctx* ctx, double* out) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(out, LSMPS_ERR_ARG, "null output");
+        *out = nb_max_displacement(ctx);
     });
 }
 
@@ -300,6 +329,19 @@ int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
         ev_record(ctx, 13);
         ctx->timings[6] = ev_elapsed(ctx, 12, 13);
     });
+}
+
+int lsmps_set_initial_pressure(lsmps_ctx* ctx, const double* p, size_t n) {
+    return guarded(ctx, [&] { ppe_set_initial_particles(ctx, p, n, false); });
+}
+int lsmps_set_initial_pressure_device(lsmps_ctx* ctx, const double* d_p, size_t n) {
+    return guarded(ctx, [&] { ppe_set_initial_particles(ctx, d_p, n, true); });
+}
+int lsmps_download_pressure_particles(lsmps_ctx* ctx, double* p, size_t n, double fill) {
+    return guarded(ctx, [&] { ppe_pressure_particles(ctx, p, n, fill, false); });
+}
+int lsmps_download_pressure_particles_device(lsmps_ctx* ctx, double* d_p, size_t n, double fill) {
+    return guarded(ctx, [&] { ppe_pressure_particles(ctx, d_p, n, fill, true); });
 }
 
 int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {

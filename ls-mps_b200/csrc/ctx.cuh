@@ -68,6 +68,12 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf cell_of, slot, cell_count, cell_start, perm, iperm;
     lsmps_gpu::DevBuf sx, sy, sz, stype, scell, cls;
     lsmps_gpu::DevBuf nbr_cnt, nbr_row, nbr_col, nbr_stats, seg_list;
+    // candidate lists of radius re + skin (sorted numbering) and the sorted positions they
+    // were built at, for refreshes of an unchanged particle set
+    bool have_candidates = false;
+    double skin = 0, cand_re = 0;
+    uint64_t cand_pairs = 0;
+    lsmps_gpu::DevBuf cand_row, cand_col, ref_sx, ref_sy, ref_sz;
 
     // ---- WLS ----
     bool have_wls = false;

@@ -612,6 +612,7 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     ctx->maxn = maxn;
     ctx->have_neighbors = ctx->have_classes = false;
     ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+    ctx->have_candidates = false;  // the sorted numbering changes
     int* dflag = ctx->dflags.get<int>();
 
     // 1. cell coordinates + bounds

@@ -7,11 +7,17 @@
 namespace lsmps_gpu {
 
 // neighbors.cu
+void particles_upload(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n, bool device);
 void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_neighbor_stats* out);
 void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
 void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out);
 void nb_download(lsmps_ctx* ctx, int32_t* row_ptr, int32_t* col, size_t col_cap);
 void nb_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);
+void nb_build_skin(lsmps_ctx* ctx, double re, double skin, int maxn, int maxc, double l0, int flags,
+                   lsmps_neighbor_stats* out);
+void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out);
+double nb_max_displacement(lsmps_ctx* ctx);
+void nb_update_positions(lsmps_ctx* ctx, const double* xyz, size_t n, bool device);
 
 // wls.cu
 void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
@@ -25,6 +31,8 @@ void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, doubl
 // solver.cu
 void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out);
 void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool device);
+void ppe_pressure_particles(lsmps_ctx* ctx, double* pp, size_t n, double fill, bool device);
 
 // mpnn.cu
 bool mpnn_ready(lsmps_ctx* ctx);

@@ -773,6 +773,34 @@ __global__ void k_y_from_net(long long n, const float* __restrict__ yf, const do
         y[i] = nb * (double)yf[i];
 }
 
+// y += |r0| net(r0 / |r0|) (network correction of a warm start), keeping y in keep
+__global__ void k_y_add_net(long long n, const float* __restrict__ yf, const double* scal, double* __restrict__ y,
+                            double* __restrict__ keep) {
+    const double nr = sqrt(scal[0]);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        keep[i] = y[i];
+        y[i] += nr * (double)yf[i];
+    }
+}
+
+// initial guess of the unknowns from a per-particle field (caller order): unknown u is
+// particle perm[sorted_of_u[u]]
+__global__ void k_guess_from_particles(long long U, const int* __restrict__ sorted_of_u, const int* __restrict__ perm,
+                                       const double* __restrict__ pp, double* __restrict__ x) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < U; u += (long long)gridDim.x * blockDim.x)
+        x[u] = pp[perm[sorted_of_u[u]]];
+}
+
+__global__ void k_fill_value(size_t n, double v, double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) out[i] = v;
+}
+
+__global__ void k_solution_to_particles(long long U, const int* __restrict__ sorted_of_u, const int* __restrict__ perm,
+                                        const double* __restrict__ x, double* __restrict__ pp) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < U; u += (long long)gridDim.x * blockDim.x)
+        pp[perm[sorted_of_u[u]]] = x[u];
+}
+
 // ---------------------------------------------------------------------------------------
 // host side of the engine
 // ---------------------------------------------------------------------------------------
@@ -1192,9 +1220,25 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     Sell<float> Af = sell_scaled32(ctx);
     set_scalar_caps(E, o->max_iter, use_nn ? stall : 0);
     bool have_start = warm;
+    double warm_rn = 0;  // |b - A x0| of a warm start the network corrected
     if (warm) {  // the iteration works on y = D x
         k_scale_by_diag<<<1184, 256, 0, s>>>(U, V.x, dinv);
         LSMPS_CHECK_LAUNCH();
+        if (use_nn) {  // the network corrects the warm start: y += |r0| net(r0 / |r0|), r0 = b - A D^-1 y
+            float* rhs = ctx->fph.ensure<float>(U + 1);
+            float* yf = ctx->fx.ensure<float>(U + 1);
+            double* scal = engine_scalars(ctx);
+            residual64(E, As, b, V.x, V.r, scal);
+            k_rhs_unit<<<1184, 256, 0, s>>>(U, V.r, rhs, scal);
+            LSMPS_CHECK_LAUNCH();
+            mpnn_warm_start(ctx, rhs, yf);
+            k_y_add_net<<<1184, 256, 0, s>>>(U, yf, scal, V.x, V.p);  // the warm start kept in p
+            LSMPS_CHECK_LAUNCH();
+            double r2 = 0;
+            LSMPS_CUDA(cudaMemcpyAsync(&r2, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+            LSMPS_CUDA(cudaStreamSynchronize(s));
+            warm_rn = std::sqrt(r2);
+        }
     } else if (use_nn) {
         float* rhs = ctx->fph.ensure<float>(U + 1);
         float* yf = ctx->fx.ensure<float>(U + 1);
@@ -1234,6 +1278,13 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
         set_scalar_caps(E, o->max_iter, 0);
         init<double, double>(E, As, b, V, false, o->tol, -1.0);
+        read(h);
+    } else if (use_nn && warm && (!std::isfinite(h.rn) || h.rn >= warm_rn)) {
+        // the correction made the warm start worse: go back to it
+        fallback = 1;
+        LSMPS_CUDA(cudaMemcpyAsync(V.x, V.p, U * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        set_scalar_caps(E, o->max_iter, 0);
+        init<double, double>(E, As, b, V, true, o->tol, -1.0);
         read(h);
     }
     double rn_upd = h.rn;
@@ -1294,6 +1345,47 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     ps->converged = converged;
     ps->fallback = fallback;
     ps->solve_ms = ev_elapsed(ctx, 10, 11);
+}
+
+void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool device) {
+    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "initial guess needs an assembled system");
+    LSMPS_REQUIRE(n == ctx->n && (n == 0 || pp), LSMPS_ERR_ARG, "initial guess must hold one value per particle");
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    double* x = ctx->vx.ensure<double>(U + 1);
+    const double* src = pp;
+    if (!device && n) {
+        double* tmp = ctx->vtmp.ensure<double>(n + 1);
+        LSMPS_CUDA(cudaMemcpyAsync(tmp, pp, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        src = tmp;
+    }
+    if (U) {
+        k_guess_from_particles<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), ctx->perm.get<int>(), src, x);
+        LSMPS_CHECK_LAUNCH();
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    ctx->have_solution = true;
+}
+
+void ppe_pressure_particles(lsmps_ctx* ctx, double* pp, size_t n, double fill, bool device) {
+    LSMPS_REQUIRE(ctx->have_solution, LSMPS_ERR_STATE, "no solution: lsmps_ppe_solve first");
+    LSMPS_REQUIRE(n == ctx->n && (n == 0 || pp), LSMPS_ERR_ARG, "output must hold one value per particle");
+    cudaStream_t s = ctx->stream;
+    const long long U = ctx->U;
+    double* dst = device ? pp : ctx->vtmp.ensure<double>(n + 1);
+    if (n && std::isnan(fill)) {  // keep the other particles' values
+        if (!device) LSMPS_CUDA(cudaMemcpyAsync(dst, pp, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    } else if (n) {
+        k_fill_value<<<std::min<unsigned>(blocks_for(n, 256), 1184), 256, 0, s>>>(n, fill, dst);
+        LSMPS_CHECK_LAUNCH();
+    }
+    if (U) {
+        k_solution_to_particles<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), ctx->perm.get<int>(),
+                                                     ctx->vx.get<double>(), dst);
+        LSMPS_CHECK_LAUNCH();
+    }
+    if (!device && n) LSMPS_CUDA(cudaMemcpyAsync(pp, dst, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
 }
 
 void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out) {

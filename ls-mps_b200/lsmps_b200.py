@@ -15,6 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "liblsmps_b200.so")
+DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "mpnn_rain200k.bin")
 CLI_PATH = os.path.join(HERE, "bin", "lsmps-bench")
 
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_GRID, ERR_OVERFLOW, ERR_NONFINITE, ERR_TIMEOUT, ERR_IO = range(10)
@@ -101,6 +102,12 @@ SIGNATURES = {
     "lsmps_build_neighbors": (C.c_int, [_vp, C.c_double, C.c_int, C.c_double, C.c_int,
                                         C.POINTER(NeighborStats)]),
     "lsmps_classify": (C.c_int, [_vp, C.c_double, C.POINTER(NeighborStats)]),
+    "lsmps_build_neighbors_skin": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
+                                             C.POINTER(NeighborStats)]),
+    "lsmps_update_positions": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_update_positions_device": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_refresh_neighbors": (C.c_int, [_vp, C.c_int, C.POINTER(NeighborStats)]),
+    "lsmps_max_displacement": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lsmps_wls": (C.c_int, [_vp, C.POINTER(WlsOpts), C.POINTER(WlsStats)]),
     "lsmps_ppe_assemble": (C.c_int, [_vp, C.POINTER(PpeOpts), C.POINTER(PpeStats)]),
     "lsmps_ppe_solve": (C.c_int, [_vp, C.POINTER(SolverOpts), C.POINTER(PpeStats)]),
@@ -111,6 +118,10 @@ SIGNATURES = {
     "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
+    "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_set_initial_pressure_device": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_download_pressure_particles": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
+    "lsmps_download_pressure_particles_device": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
     "lsmps_set_autotune": (C.c_int, [_vp, C.c_int]),
     "lsmps_autotune_report": (C.c_int, [_vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "lsmps_mpnn_param_count": (C.c_size_t, []),
@@ -251,6 +262,29 @@ class Context:
         self._check(self.L.lsmps_classify(self.h, l0, C.byref(st)))
         return st
 
+    def build_neighbors_skin(self, re, skin, max_neighbors, max_candidates, l0, classify=True):
+        """Candidate lists of radius re + skin, then the exact lists of radius re."""
+        st = NeighborStats()
+        self._check(self.L.lsmps_build_neighbors_skin(self.h, re, skin, max_neighbors, max_candidates, l0,
+                                                      NBR_CLASSIFY if classify else 0, C.byref(st)))
+        return st
+
+    def update_positions(self, xyz):
+        """New positions of the same particles (n x 3, caller order)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self._check(self.L.lsmps_update_positions(self.h, _p(xyz), len(xyz)))
+
+    def refresh_neighbors(self, classify=True):
+        """Exact lists from the candidates at the current positions (LsmpsError once beyond skin / 2)."""
+        st = NeighborStats()
+        self._check(self.L.lsmps_refresh_neighbors(self.h, NBR_CLASSIFY if classify else 0, C.byref(st)))
+        return st
+
+    def max_displacement(self):
+        d = C.c_double()
+        self._check(self.L.lsmps_max_displacement(self.h, C.byref(d)))
+        return d.value
+
     def wls(self, re, l0, mode=1, wls_samples=4096, coef=None, precision=0, store=False, reg=1e-8):
         coef = REF_QUADRATIC[None, :] if coef is None else np.atleast_2d(coef)
         self._coef = np.ascontiguousarray(coef, dtype=np.float64)
@@ -307,6 +341,17 @@ class Context:
     def pressure(self, unknowns):
         p = np.zeros(unknowns)
         self._check(self.L.lsmps_download_pressure(self.h, _p(p), unknowns))
+        return p
+
+    def set_initial_pressure(self, p_particles):
+        """Warm start of the next solve (warm_start=True) from one value per particle (caller order)."""
+        p = np.ascontiguousarray(p_particles, dtype=np.float64)
+        self._check(self.L.lsmps_set_initial_pressure(self.h, _p(p), len(p)))
+
+    def pressure_particles(self, n, fill=0.0):
+        """The last solution per particle (caller order); `fill` where a particle is not an unknown."""
+        p = np.zeros(n)
+        self._check(self.L.lsmps_download_pressure_particles(self.h, _p(p), n, fill))
         return p
 
     def pressure_into(self, out):
