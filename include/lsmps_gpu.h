@@ -269,6 +269,71 @@ int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
  * streams, two threads) race on it and must be serialised by the caller. */
 int lsmps_ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
 
+/* ---- step series (rain-on-plate proxy) ------------------------------------------------ */
+/* A 3-D step series on one context: wall fixed, droplets fall droplet_speed l0 per step and
+ * join the film at film_thickness l0 above the plate, the film slides film_speed l0 per step
+ * down the plate (angle theta_deg, plate frame of the rain_plate generator), particles past
+ * the plate's lower edge (the outflow plane) leave, injected_per_step particles arrive per
+ * step as droplets of droplet_radius l0 at heights inject_hmin..inject_hmax l0 above the
+ * plate. Every step runs neighbor lists (lsmps_build_neighbors_skin every
+ * cnl_rebuild_interval steps or when the skin no longer covers the motion, the refresh in
+ * between), classification, all-particle WLS, the WLS-Laplacian PPE and the solve, warm-started
+ * from the previous step's pressure per particle. Injected droplets join and flagged
+ * outflow particles leave at rebuild steps. The fluid count is taken on the device each step
+ * and compared with initial + injected - deleted (mass_balance, 0 when conserved). The
+ * reference's series is the 2-D python/rain_plate_cpu.py baseline (inject:67-87,
+ * remove_outflow:146-154); its C++ benchmark ignores these keys of config/rain_injection.cfg. */
+typedef struct lsmps_series lsmps_series;
+typedef struct lsmps_series_params {
+    int32_t steps;                /* informational: steps the caller will run */
+    int32_t injected_per_step;    /* config key injected_per_step */
+    int32_t cnl_rebuild_interval; /* config key cnl_rebuild_interval */
+    int32_t solver;               /* LSMPS_SOLVER_FP64 .. LSMPS_SOLVER_MIXED_F32 */
+    double l0, re;                /* spacing; support radius in l0 (re_ratio) */
+    double skin;                  /* candidate skin in l0 */
+    double droplet_speed;         /* l0 per step */
+    double film_speed;            /* l0 per step */
+    double theta_deg;             /* plate angle */
+    double film_thickness;        /* l0 */
+    double droplet_radius;        /* l0 */
+    double inject_hmin, inject_hmax; /* l0 above the plate */
+    double tol;                   /* PPE tolerance as lsmps_solver_opts.tol */
+    int32_t max_iter;
+    int32_t max_neighbors;
+    int32_t max_candidates;
+    int32_t wls_precision;        /* 0 FP64, 1 FP32 + FP64 refinement */
+    int32_t warm_start;           /* 1: start each solve from the previous pressure */
+    uint32_t seed;                /* injection positions */
+} lsmps_series_params;
+
+typedef struct lsmps_series_stats {
+    int32_t step, rebuilt, forced_rebuild, converged;
+    uint64_t particles;           /* the set the PPE sees */
+    uint64_t in_flight;           /* injected, joining at the next rebuild */
+    uint64_t flagged;             /* past the outflow plane, leaving at the next rebuild */
+    uint64_t injected_total, deleted_total;
+    uint64_t fluid_particles;     /* counted on the device: set + in flight, not wall */
+    int64_t mass_balance;         /* fluid_particles - (initial fluid + injected - deleted) */
+    uint64_t pairs, unknowns, nnz;
+    int32_t iterations, outer_iterations, fallback, reserved;
+    double fluid_volume;          /* fluid_particles x l0^3 */
+    double max_displacement;      /* since the last candidate build */
+    double relative_l2_error;     /* |x - p*| / |p*| of this step's PPE */
+    double relative_residual;
+    double neighbor_ms, wls_ms, assembly_ms, solve_ms, step_ms;
+} lsmps_series_stats;
+
+/* xyz / type: the initial particles (host, as lsmps_upload_particles; Wall marks the plate).
+ * The series borrows ctx (and its network for LSMPS_SOLVER_LEARNED) until destroyed. */
+int lsmps_series_create(lsmps_ctx* ctx, const lsmps_series_params* params, const double* xyz, const uint8_t* type,
+                        size_t n, lsmps_series** out);
+int lsmps_series_step(lsmps_series* series, lsmps_series_stats* out);
+/* The current particle set (host): positions n x 3, material (0 wall, 1 film, 2 droplet),
+ * pressure; any pointer may be NULL; *n gets the count. */
+int lsmps_series_particles(lsmps_series* series, double* xyz, uint8_t* material, double* pressure, size_t cap,
+                           size_t* n);
+void lsmps_series_destroy(lsmps_series* series);
+
 /* ---- learned preconditioner (message-passing network over the PPE graph) ----------- */
 /* No reference counterpart. Nodes are the PPE unknowns, edges the
  * off-diagonal entries with weight -a_ij / a_ii. Input features per node: residual

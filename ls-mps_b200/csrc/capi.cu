@@ -344,6 +344,29 @@ int lsmps_download_pressure_particles_device(lsmps_ctx* ctx, double* d_p, size_t
     return guarded(ctx, [&] { ppe_pressure_particles(ctx, d_p, n, fill, true); });
 }
 
+static_assert(sizeof(lsmps_series_params) == 128, "lsmps_series_params layout");
+static_assert(sizeof(lsmps_series_stats) == 184, "lsmps_series_stats layout");
+
+int lsmps_series_create(lsmps_ctx* ctx, const lsmps_series_params* params, const double* xyz, const uint8_t* type,
+                        size_t n, lsmps_series** out) {
+    return guarded(ctx, [&] { series_create(ctx, params, xyz, type, n, out); });
+}
+
+int lsmps_series_step(lsmps_series* series, lsmps_series_stats* out) {
+    return guarded(series_context(series), [&] { series_step(series, out); });
+}
+
+int lsmps_series_particles(lsmps_series* series, double* xyz, uint8_t* material, double* pressure, size_t cap,
+                           size_t* n) {
+    return guarded(series_context(series), [&] { series_particles(series, xyz, material, pressure, cap, n); });
+}
+
+void lsmps_series_destroy(lsmps_series* series) {
+    if (!series) return;
+    cudaSetDevice(series_context(series)->device);
+    series_destroy(series);
+}
+
 int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
     return guarded(ctx, [&] { ppe_manufacture(ctx, params, nmodes); });
 }

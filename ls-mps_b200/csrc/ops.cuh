@@ -8,6 +8,12 @@ namespace lsmps_gpu {
 
 // neighbors.cu
 void particles_upload(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n, bool device);
+void series_create(lsmps_ctx* ctx, const lsmps_series_params* p, const double* xyz, const uint8_t* type, size_t n,
+                   lsmps_series** out);
+void series_step(lsmps_series* s, lsmps_series_stats* out);
+void series_particles(lsmps_series* s, double* xyz, uint8_t* material, double* pressure, size_t cap, size_t* n);
+void series_destroy(lsmps_series* s);
+lsmps_ctx* series_context(lsmps_series* s);
 void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_neighbor_stats* out);
 void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
 void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out);

@@ -63,6 +63,37 @@ class PpeOpts(C.Structure):
                 ("re", C.c_double), ("l0", C.c_double), ("diag_shift", C.c_double)]
 
 
+class SeriesParams(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("injected_per_step", C.c_int32), ("cnl_rebuild_interval", C.c_int32),
+                ("solver", C.c_int32), ("l0", C.c_double), ("re", C.c_double), ("skin", C.c_double),
+                ("droplet_speed", C.c_double), ("film_speed", C.c_double), ("theta_deg", C.c_double),
+                ("film_thickness", C.c_double), ("droplet_radius", C.c_double), ("inject_hmin", C.c_double),
+                ("inject_hmax", C.c_double), ("tol", C.c_double), ("max_iter", C.c_int32),
+                ("max_neighbors", C.c_int32), ("max_candidates", C.c_int32), ("wls_precision", C.c_int32),
+                ("warm_start", C.c_int32), ("seed", C.c_uint32)]
+
+
+class SeriesStats(C.Structure):
+    _fields_ = [("step", C.c_int32), ("rebuilt", C.c_int32), ("forced_rebuild", C.c_int32), ("converged", C.c_int32),
+                ("particles", C.c_uint64), ("in_flight", C.c_uint64), ("flagged", C.c_uint64),
+                ("injected_total", C.c_uint64), ("deleted_total", C.c_uint64), ("fluid_particles", C.c_uint64),
+                ("mass_balance", C.c_int64), ("pairs", C.c_uint64), ("unknowns", C.c_uint64), ("nnz", C.c_uint64),
+                ("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("fallback", C.c_int32),
+                ("reserved", C.c_int32), ("fluid_volume", C.c_double), ("max_displacement", C.c_double),
+                ("relative_l2_error", C.c_double), ("relative_residual", C.c_double), ("neighbor_ms", C.c_double),
+                ("wls_ms", C.c_double), ("assembly_ms", C.c_double), ("solve_ms", C.c_double),
+                ("step_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+SERIES_DEFAULTS = dict(steps=200, injected_per_step=2000, cnl_rebuild_interval=10, solver="learned", l0=1.0, re=2.1,
+                       skin=1.0, droplet_speed=0.05, film_speed=0.02, theta_deg=20.0, film_thickness=4.0,
+                       droplet_radius=3.0, inject_hmin=10.0, inject_hmax=40.0, tol=3e-11, max_iter=20000,
+                       max_neighbors=128, max_candidates=512, wls_precision=None, warm_start=1, seed=23)
+
+
 class PpeStats(C.Structure):
     _fields_ = [("unknowns", C.c_uint64), ("nnz", C.c_uint64), ("dirichlet", C.c_uint64),
                 ("neumann", C.c_uint64), ("failed_rows", C.c_uint64), ("iterations", C.c_int32),
@@ -119,6 +150,10 @@ SIGNATURES = {
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
     "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_series_create": (C.c_int, [_vp, C.POINTER(SeriesParams), _vp, _vp, C.c_size_t, C.POINTER(_vp)]),
+    "lsmps_series_step": (C.c_int, [_vp, C.POINTER(SeriesStats)]),
+    "lsmps_series_particles": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "lsmps_series_destroy": (None, [_vp]),
     "lsmps_set_initial_pressure_device": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_download_pressure_particles": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
     "lsmps_download_pressure_particles_device": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
@@ -425,3 +460,51 @@ def struct_dict(s):
             v = list(v)
         out[name] = v
     return out
+
+
+class Series:
+    """A rain-on-plate step series on a context (lsmps_series_*). Keyword arguments override
+    SERIES_DEFAULTS; `solver` is a name of SOLVERS; wls_precision defaults to mixed for the
+    mixed / learned solvers and FP64 otherwise."""
+
+    def __init__(self, ctx, xyz, types, **kw):
+        p = dict(SERIES_DEFAULTS)
+        p.update(kw)
+        solver = SOLVERS.get(p["solver"], p["solver"])
+        if p["wls_precision"] is None:
+            p["wls_precision"] = 1 if solver in (SOLVERS["mixed"], SOLVERS["learned"], SOLVERS["mixed_f32"]) else 0
+        p["solver"] = solver
+        self.params = SeriesParams(**p)
+        self.ctx = ctx
+        self.h = None
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        types = np.ascontiguousarray(types, dtype=np.uint8)
+        h = _vp()
+        ctx._check(ctx.L.lsmps_series_create(ctx.h, C.byref(self.params), _p(xyz), _p(types), len(types), C.byref(h)))
+        self.h = h
+
+    def step(self):
+        st = SeriesStats()
+        self.ctx._check(self.ctx.L.lsmps_series_step(self.h, C.byref(st)))
+        return st
+
+    def particles(self):
+        """(xyz, material, pressure) of the current particle set (material: 0 wall, 1 film, 2 droplet)."""
+        n = C.c_size_t()
+        self.ctx._check(self.ctx.L.lsmps_series_particles(self.h, None, None, None, 0, C.byref(n)))
+        xyz = np.zeros((n.value, 3))
+        mat = np.zeros(n.value, np.uint8)
+        pres = np.zeros(n.value)
+        self.ctx._check(self.ctx.L.lsmps_series_particles(self.h, _p(xyz), _p(mat), _p(pres), n.value, C.byref(n)))
+        return xyz, mat, pres
+
+    def close(self):
+        if self.h:
+            self.ctx.L.lsmps_series_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,126 @@
+"""Rain-on-plate step series and the skin (Verlet) neighbor lists it uses.
+
+* Refreshed lists (candidates of radius re + skin filtered at the current positions) hold
+  the same neighbor sets and classes as a fresh build at those positions; the refresh
+  refuses once a particle moved more than skin / 2.
+* Per-particle warm start: a solve started from its own solution (set per particle) stops
+  at once, and the per-particle download puts the unknowns' values at their particles.
+* Series: the device fluid count matches initial + injected - deleted at every step (mass
+  balance 0); candidate rebuilds at step 1 and every interval steps; every PPE reaches
+  relative L2 <= 1e-8 against p*; the warm start needs fewer iterations than the cold first
+  solve; the learned and plain FP64 series see the same particles.
+"""
+import numpy as np
+import pytest
+
+import lsmps_b200 as lib
+
+pytestmark = pytest.mark.gpu
+SMALL = dict(steps=25, injected_per_step=400, cnl_rebuild_interval=10, tol=3e-11, seed=5)
+
+
+@pytest.fixture(scope="module")
+def plate():
+    xyz, t, _ = lib.generate(None, case="rain_plate", particles=60_000, l0=1.0, seed=3)
+    return xyz, t
+
+
+def _rows(row, col):
+    return [np.sort(col[row[i]:row[i + 1]]) for i in range(len(row) - 1)]
+
+
+def _same_lists(a, b):
+    (ra, ca), (rb, cb) = a, b
+    assert np.array_equal(np.diff(ra), np.diff(rb))
+    for x, y in zip(_rows(ra, ca), _rows(rb, cb)):
+        assert np.array_equal(x, y)
+
+
+def test_refresh_equals_fresh_build(built, plate):
+    xyz, t = plate
+    rng = np.random.default_rng(0)
+    with lib.Context(0) as a, lib.Context(0) as b:
+        a.upload(xyz, t)
+        st = a.build_neighbors_skin(2.1, 0.6, 128, 512, 1.0)
+        b.upload(xyz, t)
+        sb = b.build_neighbors(2.1, 128, 1.0)
+        assert st.pairs == sb.pairs
+        _same_lists(a.neighbors(st.pairs), b.neighbors(sb.pairs))
+        moved = xyz + rng.uniform(-0.17, 0.17, xyz.shape)  # |d| <= 0.17 sqrt(3) < 0.3 = skin / 2
+        a.update_positions(moved)
+        assert a.max_displacement() <= 0.3
+        st = a.refresh_neighbors()
+        b.upload(moved, t)
+        sb = b.build_neighbors(2.1, 128, 1.0)
+        assert st.pairs == sb.pairs and list(st.type_count) == list(sb.type_count)
+        _same_lists(a.neighbors(st.pairs), b.neighbors(sb.pairs))
+        assert np.array_equal(a.types(), b.types())
+        a.update_positions(xyz + np.array([0.4, 0.0, 0.0]) * (np.arange(len(t)) % 2)[:, None])
+        with pytest.raises(lib.LsmpsError) as e:
+            a.refresh_neighbors()
+        assert e.value.code == lib.ERR_STATE
+
+
+def test_particle_warm_start(built, plate):
+    xyz, t = plate
+    with lib.Context(0) as c:
+        c.upload(xyz, t)
+        c.build_neighbors(2.1, 128, 1.0)
+        c.wls(2.1, 1.0, mode=1)
+        ps = c.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
+        cold = c.ppe_solve("fp64", 20000, 3e-11)
+        pp = c.pressure_particles(len(t), fill=-7.0)
+        row, col, val, b, xe, part = c.ppe(ps.unknowns, ps.nnz)
+        p_ref = c.pressure(ps.unknowns)
+        assert np.array_equal(pp[part], p_ref)  # unknown rank -> its particle
+        others = np.ones(len(t), bool)
+        others[part] = False
+        assert np.all(pp[others] == -7.0)
+        c.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
+        c.set_initial_pressure(pp)
+        warm = c.ppe_solve("fp64", 20000, 3e-11, warm_start=True)
+        assert warm.converged and warm.iterations <= 2 < cold.iterations
+
+
+@pytest.fixture(scope="module")
+def series_runs(built, plate):
+    xyz, t = plate
+    out = {}
+    with lib.Context(0) as ctx:
+        ctx.mpnn_load(lib.DEFAULT_WEIGHTS)
+        for solver in ("learned", "fp64"):
+            with lib.Series(ctx, xyz, t, solver=solver, **SMALL) as s:
+                rows = [s.step() for _ in range(SMALL["steps"])]
+                out[solver] = (rows, s.particles())
+    return out
+
+
+def test_series_mass_balance_and_cadence(series_runs):
+    rows, _ = series_runs["fp64"]
+    for r in rows:
+        assert r.mass_balance == 0
+        assert r.injected_total == SMALL["injected_per_step"] * r.step
+        assert r.forced_rebuild == 0
+        assert bool(r.rebuilt) == (r.step == 1 or r.step % SMALL["cnl_rebuild_interval"] == 0)
+        if r.rebuilt:
+            assert r.in_flight == 0  # injected droplets join at rebuilds
+        else:
+            assert r.max_displacement <= 0.5 * 1.0
+    assert rows[-1].deleted_total > 0  # the film reaches the outflow edge
+
+
+def test_series_accuracy_and_warm_start(series_runs):
+    for solver in ("learned", "fp64"):
+        rows, _ = series_runs[solver]
+        for r in rows:
+            assert r.converged, (solver, r.step)
+            assert r.relative_l2_error <= 1e-8, (solver, r.step, r.relative_l2_error)
+        warm = np.mean([r.iterations for r in rows[1:]])
+        assert warm < rows[0].iterations, (solver, warm, rows[0].iterations)
+
+
+def test_series_same_particles_for_both_solvers(series_runs):
+    (ra, (xa, ma, _)), (rb, (xb, mb, _)) = series_runs["learned"], series_runs["fp64"]
+    assert [r.particles for r in ra] == [r.particles for r in rb]
+    assert [r.unknowns for r in ra] == [r.unknowns for r in rb]
+    assert np.array_equal(xa, xb) and np.array_equal(ma, mb)
