@@ -46,7 +46,7 @@ L0, RE_RATIO, MAXN = 1.0, 2.1, 128
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--particles", type=int, default=1_000_000)
@@ -55,7 +55,8 @@ def parse_args():
     ap.add_argument("--solver", default="learned", choices=["learned", "mixed", "jacobi", "fp64"])
     ap.add_argument("--weights", default=os.path.join(ROOT, "ls-mps_b200", "weights", "mpnn_rain200k.bin"),
                     help="network weights for the learned solver (trained by ls-mps_b200/train_mpnn.py)")
-    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--tol", type=float, default=3e-11,
+                    help="relative residual; 3e-11 brings every compared solver to PPE relative L2 <= 1e-8")
     ap.add_argument("--max-iter", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 comparison solves")
@@ -123,7 +124,7 @@ class ClockSampler:
         try:
             self.err_path = self.path + ".err"
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=open(self.err_path, "w"))
         except OSError:
             self.proc = None
@@ -290,12 +291,15 @@ def run_mine(args, dist):
                          "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual}
         result["ppe_compare"] = cmp
         result["speedup_vs_plain_fp64"] = cmp["fp64"]["solve_ms"] / result["ppe"]["solve_ms"]
+        result["l2_target"] = {"bound": 1e-8, "met": bool(rel_l2 <= 1e-8 and all(
+            c["converged"] and c["relative_l2_error"] <= 1e-8 for c in cmp.values()))}
 
     # ---- roofline of the dominant kernel (the solver's SpMV) and the other kernels ----
     peak, peak_kind = measured_hbm_peak()
     kern = {}
     for name, kid in (("spmv32", lib.KB_SPMV32), ("spmv64", lib.KB_SPMV64), ("nbr_count", lib.KB_NBR_COUNT),
-                      ("nbr_fill", lib.KB_NBR_FILL), ("wls", lib.KB_WLS)):
+                      ("nbr_fill", lib.KB_NBR_FILL), ("wls", lib.KB_WLS)) + (
+                          (("mpnn_layer", lib.KB_MPNN_LAYER),) if args.solver == "learned" else ()):
         ms, nbytes = ctx.kernel_bench(kid, 20)
         gbs = nbytes / (ms * 1e-3) / 1e9
         kern[name] = {"ms": ms, "alg_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
