@@ -57,6 +57,7 @@ def main():
     ap.add_argument("--eval-cases", default="rain_plate,mixed")
     ap.add_argument("--eval-seeds", type=int, default=3)
     ap.add_argument("--eval-particles", type=int, default=1_000_000)
+    ap.add_argument("--eval-tol", type=float, default=3e-11, help="relative residual of the evaluation solves")
     ap.add_argument("--out", default=None)
     ap.add_argument("--load", default=None, help="skip training, evaluate these weights")
     ap.add_argument("--report", default=None, help="write the evaluation as JSON here")
@@ -101,8 +102,8 @@ def main():
                 build(ctx, case, a.eval_particles, 9000 + k)
                 res = {"case": case}
                 for name in ("mixed", "learned", "fp64"):
-                    ctx.ppe_solve(name, 20000, 1e-10)  # warm
-                    s = ctx.ppe_solve(name, 20000, 1e-10)
+                    ctx.ppe_solve(name, 20000, a.eval_tol)  # warm
+                    s = ctx.ppe_solve(name, 20000, a.eval_tol)
                     res[name] = {"iterations": s.iterations, "solve_ms": s.solve_ms, "rel_l2": s.relative_l2_error,
                                  "converged": bool(s.converged), "fallback": s.fallback}
                 evals.append(res)
@@ -122,7 +123,11 @@ def main():
                              "learned_vs_mixed": m / le, "learned_vs_plain_fp64": p / le,
                              "mixed_it": np.mean([e["mixed"]["iterations"] for e in ev]),
                              "learned_it": np.mean([e["learned"]["iterations"] for e in ev]),
-                             "fallbacks": int(sum(e["learned"]["fallback"] for e in ev))}
+                             "fallbacks": int(sum(e["learned"]["fallback"] for e in ev)),
+                             "seeds": len(ev),
+                             "max_rel_l2": max(e[n]["rel_l2"] for e in ev for n in ("mixed", "learned", "fp64")),
+                             "learned_fewer_iterations": int(sum(e["learned"]["iterations"] < e["mixed"]["iterations"]
+                                                                 for e in ev))}
         report["summary"] = summary
         print(json.dumps(summary))
     if a.report:
