@@ -207,7 +207,12 @@ typedef struct lsmps_solver_opts {
     int32_t max_iter;        /* total BiCGStab iterations (inner ones for MIXED / LEARNED) */
     double tol;              /* converged when |r| <= tol * max(1, |b|) (src/lsmps.cpp:67) */
     int32_t warm_start;      /* start from the last solution held by the context */
-    int32_t use_graph;       /* capture the iteration in a CUDA graph (FP64 / JACOBI / MIXED) */
+    int32_t use_graph;       /* FP64 / JACOBI / MIXED / LEARNED: 1 (default) the whole iteration loop as one
+                                CUDA graph whose WHILE node repeats check_every iterations and the
+                                replacement / restart / stop decisions on the device (no host round
+                                trip per solve); 2 graphs of check_every iterations launched from a
+                                host loop that makes the decisions; 0 eager launches, same host loop.
+                                All three run the same kernels in the same order (same bits). */
     double inner_tol;        /* MIXED / LEARNED: residual drop between FP64 residual replacements
                                 (default 0.01); MIXED_F32: the same (default 0.1) */
     int32_t inner_max_iter;  /* reserved */

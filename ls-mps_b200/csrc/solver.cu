@@ -20,6 +20,7 @@
 // reads the status once per graph launch.
 #include <algorithm>
 #include <cmath>
+#include <climits>
 #include <cstring>
 #include <tuple>
 #include <utility>
@@ -486,7 +487,9 @@ template <class T, class TM = T>
 __global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restrict__ b, const T* __restrict__ x,
                                                  int use_x, T* __restrict__ r, T* __restrict__ r0,
                                                  T* __restrict__ p, T* __restrict__ v, BcgScalars* S,
-                                                 Partials P, double tol, double bnorm_override) {
+                                                 Partials P, double tol, double bnorm_override,
+                                                 const int* gate = nullptr, int want = 0) {
+    if (gate && *gate != want) return;  // device-driven loop: runs only when the control chose it
     double abb = 0, arr = 0;
     SELL_LOOP(A) {
         double ax = use_x ? sell_row(A, s, lane, x) : 0.0;
@@ -713,7 +716,8 @@ __global__ void k_start_rhs(long long n, const double* __restrict__ r64, const d
 __global__ void __launch_bounds__(RB, 6) k_replace_residual(Sell<double> A, const double* __restrict__ b,
                                                             const double* __restrict__ y, double* __restrict__ r,
                                                             const double* __restrict__ r0, BcgScalars* S,
-                                                            Partials P) {
+                                                            Partials P, const int* gate = nullptr, int want = 0) {
+    if (gate && *gate != want) return;  // device-driven loop: runs only when the control chose it
     double arr = 0, ar0r = 0;
     SELL_LOOP(A) {
         double ay = sell_row(A, s, lane, y);
@@ -802,6 +806,99 @@ __global__ void k_solution_to_particles(long long U, const int* __restrict__ sor
 }
 
 // ---------------------------------------------------------------------------------------
+// device-driven solve loop: the host loop's decisions (residual replacement, restart, stop)
+// made by single-thread kernels between the iteration chunks of a conditional WHILE graph
+// node, so that a whole solve is one graph launch with no host round trip
+// ---------------------------------------------------------------------------------------
+struct LoopCtl {
+    double rn_upd;      // |r| at the last replacement or restart
+    double delta;       // replacement when |r| fell below delta rn_upd
+    int total;          // iterations so far (over restarts)
+    int base;           // S->iters at the last accounting
+    int replacements, restarts, fallback;
+    int act;            // 0 none, 1 replace, 2 restart: gates the replacement and init kernels
+    int final_replace;  // the pending replacement ends the solve (iteration cap)
+    int state;          // 0 running, 1 converged, 2 failed, 3 iteration cap
+    int trips, max_trips, max_iter, use_nn;
+};
+
+// as set_scalar_caps on the host: a fresh scalar block with the remaining iteration budget
+__device__ void restart_caps(BcgScalars* S, int max_iter) {
+    BcgScalars z{};
+    z.max_iter = max_iter;
+    z.stall_window = 0;
+    *S = z;
+}
+
+__global__ void k_mix_after_chunk(BcgScalars* S, LoopCtl* C) {
+    C->total += S->iters - C->base;
+    C->base = S->iters;
+    C->act = 0;
+    if (!S->done && S->rn > C->delta * C->rn_upd) return;  // keep iterating
+    const int why = S->done;
+    if (why == 3 || C->total >= C->max_iter) {
+        C->act = 1;
+        C->final_replace = 1;
+        return;
+    }
+    if (why == 0) {
+        C->act = 1;
+        C->final_replace = 0;
+        return;
+    }
+    if (why == 4 && C->use_nn) C->fallback = 1;
+    if (S->nonfinite) {
+        C->state = 2;
+        return;
+    }
+    restart_caps(S, C->max_iter - C->total);
+    C->act = 2;
+}
+
+__global__ void k_mix_after_replace(BcgScalars* S, LoopCtl* C) {
+    if (C->act != 1) return;
+    C->act = 0;
+    if (C->final_replace) {
+        C->state = S->done == 1 ? 1 : 3;
+        return;
+    }
+    C->replacements += 1;
+    C->rn_upd = S->rn;
+    if (S->done == 1) {
+        C->state = 1;
+        return;
+    }
+    if (S->done == 0) return;
+    if (S->nonfinite) {  // breakdown after the replacement: restart, unless non-finite
+        C->state = 2;
+        return;
+    }
+    restart_caps(S, C->max_iter - C->total);
+    C->act = 2;
+}
+
+__global__ void k_mix_after_restart(BcgScalars* S, LoopCtl* C) {
+    if (C->act != 2) return;
+    C->act = 0;
+    C->restarts += 1;
+    C->base = 0;
+    C->rn_upd = S->rn;
+    if (S->done == 1) C->state = 1;
+    else if (S->done) C->state = 2;
+}
+
+// plain loop (FP64 / Jacobi): stop when the iteration stopped
+__global__ void k_plain_after_chunk(const BcgScalars* S, LoopCtl* C) {
+    if (S->done) C->state = S->done == 1 ? 1 : 2;
+}
+
+// the WHILE condition; trips are bounded whatever the control state says
+__global__ void k_loop_continue(LoopCtl* C, cudaGraphConditionalHandle h) {
+    C->trips += 1;
+    cudaGraphSetConditional(h, (C->state == 0 && C->trips < C->max_trips) ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------------------
 // host side of the engine
 // ---------------------------------------------------------------------------------------
 struct Engine {
@@ -826,6 +923,51 @@ Engine make_engine(lsmps_ctx* ctx) {
 
 double* engine_scalars(lsmps_ctx* ctx) { return ctx->red.get<double>() + 2 * RGRID + 128; }
 
+LoopCtl* engine_loop_ctl(lsmps_ctx* ctx) {
+    return reinterpret_cast<LoopCtl*>(ctx->red.get<double>() + 2 * RGRID + 160);
+}
+static_assert(sizeof(BcgScalars) <= 128 * sizeof(double) && sizeof(LoopCtl) <= 96 * sizeof(double),
+              "engine scalar layout");
+
+// A graph whose one node is a WHILE conditional: its body (captured from stream s by `body`,
+// then k_loop_continue) runs until the control clears the condition.
+template <class F>
+cudaGraphExec_t build_while_graph(cudaStream_t s, LoopCtl* C, F&& body) {
+    cudaGraph_t g = nullptr;
+    LSMPS_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphExec_t exec = nullptr;
+    try {
+        cudaGraphConditionalHandle h;
+        LSMPS_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        LSMPS_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+        LSMPS_CUDA(cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+        body();
+        k_loop_continue<<<1, 1, 0, s>>>(C, h);
+        cudaGraph_t captured = nullptr;
+        LSMPS_CUDA(cudaStreamEndCapture(s, &captured));
+        LSMPS_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    } catch (...) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(s, &tmp);
+            if (tmp) cudaGraphDestroy(tmp);
+        }
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        throw;
+    }
+    cudaGraphDestroy(g);
+    return exec;
+}
+
 template <class T, class TM = T>
 void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V) {
     note_launches(5);
@@ -847,13 +989,40 @@ void residual64(Engine& E, const Sell<double>& A, const double* b, const double*
     LSMPS_CHECK_LAUNCH();
 }
 
-// Runs the iteration until done, as a CUDA graph of `chunk` iterations when requested.
-// Returns the final scalars.
+// Runs the iteration until done. mode 1: one graph whose WHILE node repeats `chunk`
+// iterations until the scalars say done (no host round trip); mode 2: a graph of `chunk`
+// iterations launched from a host loop that reads the scalars after each; mode 0: eager
+// launches with the same host loop. Returns the final scalars.
 template <class T>
-BcgScalars run_loop(Engine& E, const Sell<T>& A, const Vecs<T>& V, int chunk, bool use_graph) {
+BcgScalars run_loop(Engine& E, const Sell<T>& A, const Vecs<T>& V, int chunk, int mode) {
     BcgScalars h{};
+    LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, E.s));
+    LSMPS_CUDA(cudaStreamSynchronize(E.s));
+    // the iteration cap bounds the loop; two extra chunks cover the final no-op kernels
+    const long long max_chunks = (h.max_iter + chunk - 1) / chunk + 2;
+    if (h.done) return h;
+    if (mode == 1) {
+        LoopCtl* C = engine_loop_ctl(E.ctx);
+        LoopCtl c0{};
+        c0.max_trips = (int)std::min<long long>(max_chunks, INT_MAX);
+        LSMPS_CUDA(cudaMemcpyAsync(C, &c0, sizeof(c0), cudaMemcpyHostToDevice, E.s));
+        cudaGraphExec_t exec = build_while_graph(E.s, C, [&] {
+            for (int c = 0; c < chunk; ++c) iteration<T>(E, A, V);
+            k_plain_after_chunk<<<1, 1, 0, E.s>>>(E.S, C);
+        });
+        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        cudaError_t e = cudaGraphLaunch(exec, E.s);
+        LoopCtl hc{};
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, C, sizeof(hc), cudaMemcpyDeviceToHost, E.s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, E.s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(E.s);
+        cudaGraphExecDestroy(exec);
+        LSMPS_CUDA(e);
+        note_launches((uint64_t)hc.trips * (5 * (uint64_t)chunk + 2));
+        return h;
+    }
     cudaGraphExec_t exec = nullptr;
-    if (use_graph) {
+    if (mode == 2) {
         cudaGraph_t graph;
         LSMPS_CUDA(cudaStreamBeginCapture(E.s, cudaStreamCaptureModeThreadLocal));
         for (int c = 0; c < chunk; ++c) iteration<T>(E, A, V);
@@ -863,12 +1032,8 @@ BcgScalars run_loop(Engine& E, const Sell<T>& A, const Vecs<T>& V, int chunk, bo
         LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         cudaGraphDestroy(graph);
     }
-    LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, E.s));
-    LSMPS_CUDA(cudaStreamSynchronize(E.s));
-    // the iteration cap bounds the loop; two extra chunks cover the final no-op kernels
-    const long long max_chunks = (h.max_iter + chunk - 1) / chunk + 2;
     for (long long c = 0; c < max_chunks && !h.done; ++c) {
-        if (use_graph) {
+        if (exec) {
             LSMPS_CUDA(cudaGraphLaunch(exec, E.s));
             note_launches(5 * (uint64_t)chunk);
         } else {
@@ -1059,7 +1224,7 @@ static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_s
     }
     init<double>(E, Aop, ctx->A_b.get<double>(), V, warm, o->tol, -1.0);
     int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
-    BcgScalars h = run_loop<double>(E, Aop, V, chunk, o->use_graph != 0);
+    BcgScalars h = run_loop<double>(E, Aop, V, chunk, o->use_graph);
     if (jacobi) {
         k_unscale<<<1184, 256, 0, s>>>(U, V.x, dinv);
         LSMPS_CHECK_LAUNCH();
@@ -1255,7 +1420,7 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     }
     init<double, double>(E, As, b, V, have_start, o->tol, -1.0);
     cudaGraphExec_t exec = nullptr;
-    if (o->use_graph) {
+    if (o->use_graph == 2) {
         cudaGraph_t graph;
         LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
@@ -1290,7 +1455,42 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     double rn_upd = h.rn;
     bool converged = h.done == 1, failed = h.done == 2 && h.nonfinite;
     const long long max_chunks = (long long)o->max_iter / chunk + 4 + o->max_iter;  // bounded loop
-    for (long long guard = 0; !converged && !failed && guard < max_chunks; ++guard) {
+    if (o->use_graph == 1 && !converged && !failed) {
+        // the loop below, decided on the device: one graph launch for the whole solve
+        LoopCtl* C = engine_loop_ctl(ctx);
+        LoopCtl c0{};
+        c0.rn_upd = rn_upd;
+        c0.delta = delta;
+        c0.fallback = fallback;
+        c0.max_trips = (int)std::min<long long>(max_chunks, INT_MAX);
+        c0.max_iter = o->max_iter;
+        c0.use_nn = use_nn ? 1 : 0;
+        LSMPS_CUDA(cudaMemcpyAsync(C, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
+        cudaGraphExec_t wexec = build_while_graph(s, C, [&] {
+            for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
+            k_mix_after_chunk<<<1, 1, 0, s>>>(E.S, C);
+            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P, &C->act, 1);
+            k_mix_after_replace<<<1, 1, 0, s>>>(E.S, C);
+            k_bcg_init<double, double><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P, o->tol,
+                                                            -1.0, &C->act, 2);
+            k_mix_after_restart<<<1, 1, 0, s>>>(E.S, C);
+        });
+        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        cudaError_t e = cudaGraphLaunch(wexec, s);
+        LoopCtl hc{};
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, C, sizeof(hc), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaGraphExecDestroy(wexec);
+        LSMPS_CUDA(e);
+        note_launches((uint64_t)hc.trips * (5 * (uint64_t)chunk + 6));
+        total = hc.total;
+        replacements = hc.replacements;
+        restarts = hc.restarts;
+        fallback = hc.fallback;
+        converged = hc.state == 1;
+        failed = hc.state == 2;
+    }
+    for (long long guard = 0; o->use_graph != 1 && !converged && !failed && guard < max_chunks; ++guard) {
         if (!h.done) {
             if (exec) {
                 LSMPS_CUDA(cudaGraphLaunch(exec, s));

@@ -342,7 +342,7 @@ class Context:
     def ppe_solve(self, solver, max_iter, tol, warm_start=False, use_graph=True, inner_tol=0.0,
                   inner_max_iter=0, stall_window=0, check_every=0):
         o = SolverOpts(solver=SOLVERS.get(solver, solver), max_iter=int(max_iter), tol=tol,
-                       warm_start=1 if warm_start else 0, use_graph=1 if use_graph else 0,
+                       warm_start=1 if warm_start else 0, use_graph=int(use_graph),
                        inner_tol=inner_tol, inner_max_iter=inner_max_iter, stall_window=stall_window,
                        check_every=check_every)
         st = PpeStats()

@@ -110,3 +110,30 @@ def test_warm_start(ctx, lattice_system):
     assert b.converged and b.iterations <= 2
     c = ctx.ppe_solve("jacobi", 5000, 1e-10, warm_start=True)
     assert c.converged and c.iterations <= 2
+
+
+@pytest.fixture(scope="module")
+def plate_system(built):
+    c = lib.Context(0)
+    xyz, t, _ = lib.generate(None, case="rain_plate", particles=200_000, l0=1.0, seed=21)
+    c.upload(xyz, t)
+    c.build_neighbors(2.1, 128, 1.0)
+    c.wls(2.1, 1.0, mode=1)
+    st = c.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
+    c.mpnn_load(lib.DEFAULT_WEIGHTS)
+    yield c, st.unknowns
+    c.close()
+
+
+@pytest.mark.parametrize("solver", ["fp64", "jacobi", "mixed", "learned"])
+def test_device_driven_loop_matches_host_loops(plate_system, solver):
+    """use_graph 1 (one graph, WHILE node, decisions on the device) runs the same kernels in the
+    same order as the host loops over chunk graphs (2) and eager launches (0): same bits."""
+    c, U = plate_system
+    out = {}
+    for mode in (1, 2, 0):
+        st = c.ppe_solve(solver, 20000, 3e-11, use_graph=mode)
+        out[mode] = (st.iterations, st.outer_iterations, st.converged, st.fallback,
+                     float(st.final_residual).hex(), float(st.relative_l2_error).hex(), c.pressure(U).tobytes())
+    assert out[1][2] and out[1][5] and float.fromhex(out[1][5]) <= 1e-8
+    assert out[1] == out[2] == out[0]
