@@ -274,6 +274,35 @@ int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
  * streams, two threads) race on it and must be serialised by the caller. */
 int lsmps_ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
 
+/* ---- WLS of caller fields, pressure projection ------------------------------------ */
+/* The all-particle WLS (mode 1 moments, FP64) of nfields (1..3) per-particle fields given in
+ * device memory (n x nfields, caller order): out (n x nfields x 9, caller order) holds per
+ * particle and field the WLS solution (df/dx, df/dy, df/dz, l0 d2f/dx2, l0 d2f/dy2,
+ * l0 d2f/dz2, l0 d2f/dxdy, l0 d2f/dxdz, l0 d2f/dydz), as the reference's wls_test solves for
+ * its quadratic (src/lsmps.cpp:28), with f_j - f_i from the array; zeros where the WLS is
+ * skipped (wall, splash) or failed. Needs neighbor lists and classes. */
+int lsmps_wls_fields(lsmps_ctx* ctx, const double* d_fields, int nfields, double* d_out);
+
+typedef struct lsmps_projection_stats {
+    uint64_t unknowns;       /* PPE unknowns */
+    uint64_t measured;       /* particles the divergence statistics cover (the unknowns) */
+    double div_before_rms, div_before_max;  /* div u* */
+    double div_after_rms, div_after_max;    /* div u after the correction */
+    int32_t iterations, converged;
+    double relative_residual, solve_ms, total_ms;
+    uint64_t core;           /* Interior unknowns at least 3 neighbor hops from any other particle */
+    double div_core_before_rms, div_core_after_rms;  /* over the core */
+} lsmps_projection_stats;
+
+/* One pressure projection (the reference's 2-D python/rain_plate_lsmps_cpu.py:202-260 in
+ * 3-D): div u* from lsmps_wls_fields of the velocity, the assembled WLS-Laplacian PPE (variant
+ * LSMPS_PPE_WLS; free-surface / splash Dirichlet p = 0) solved with opts for
+ * lap p = rho / dt div u* (b = -rho / dt div u*, as A ~ -lap), and u = u* - dt / rho grad p
+ * (walls keep u*). d_vel / d_vel_out: n x 3 device arrays, caller order; d_pressure: n values,
+ * 0 off the unknowns. Overwrites the assembled b (and p* with 0). */
+int lsmps_projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* opts,
+                          double* d_vel_out, double* d_pressure, lsmps_projection_stats* out);
+
 /* ---- step series (rain-on-plate proxy) ------------------------------------------------ */
 /* A 3-D step series on one context: wall fixed, droplets fall droplet_speed l0 per step and
  * join the film at film_thickness l0 above the plate, the film slides film_speed l0 per step

@@ -146,6 +146,9 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->scell, &ctx->cls, &ctx->nbr_cnt, &ctx->nbr_row, &ctx->nbr_col, &ctx->seg_list,
                                  &ctx->cand_row, &ctx->cand_col, &ctx->ref_sx, &ctx->ref_sy, &ctx->ref_sz,
                                  &ctx->nbr_stats, &ctx->wls_status, &ctx->wls_z, &ctx->wls_wsum, &ctx->wls_x,
+                                 &ctx->wf_in, &ctx->wf_x, &ctx->wf_status, &ctx->wf_z, &ctx->wf_wsum, &ctx->wf_stats,
+                                 &ctx->pj_grad, &ctx->pj_gradp, &ctx->pj_div, &ctx->pj_mask, &ctx->pj_stats,
+                                 &ctx->pj_hop,
                                  &ctx->wls_stats, &ctx->wls_sample, &ctx->ref_rank, &ctx->u_of_sorted,
                                  &ctx->sorted_of_u, &ctx->ref_of_u, &ctx->u_of_ref, &ctx->A_row, &ctx->A_col,
                                  &ctx->A_val, &ctx->A_valf, &ctx->A_b, &ctx->A_xexact, &ctx->A_dinv,
@@ -365,6 +368,15 @@ void lsmps_series_destroy(lsmps_series* series) {
     if (!series) return;
     cudaSetDevice(series_context(series)->device);
     series_destroy(series);
+}
+
+int lsmps_wls_fields(lsmps_ctx* ctx, const double* d_fields, int nfields, double* d_out) {
+    return guarded(ctx, [&] { wls_fields(ctx, d_fields, nfields, d_out); });
+}
+
+int lsmps_projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* opts,
+                          double* d_vel_out, double* d_pressure, lsmps_projection_stats* out) {
+    return guarded(ctx, [&] { projection_step(ctx, d_vel, dt, rho, opts, d_vel_out, d_pressure, out); });
 }
 
 int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {

@@ -80,6 +80,10 @@ struct lsmps_ctx {
     int wls_nrhs = 0;
     bool wls_stored = false;
     lsmps_gpu::DevBuf wls_status, wls_z, wls_wsum, wls_x, wls_stats, wls_sample;
+    // WLS of caller fields (gradients for the projection step): inputs, solutions, scratch
+    lsmps_gpu::DevBuf wf_in, wf_x, wf_status, wf_z, wf_wsum, wf_stats;
+    // projection step: WLS solutions of u and p, divergence, unknown mask, statistics
+    lsmps_gpu::DevBuf pj_grad, pj_gradp, pj_div, pj_mask, pj_stats, pj_hop;
 
     // ---- PPE ----
     bool have_ppe = false;

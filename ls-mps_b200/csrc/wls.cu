@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                                                  const int* __restrict__ col, int* __restrict__ status,
                                                  double* __restrict__ zout, double* __restrict__ wsum,
                                                  double* __restrict__ xout, unsigned long long* gcnt,
-                                                 double* gsum) {
+                                                 double* gsum, const double* __restrict__ fvals) {
     __shared__ unsigned long long s_cnt[8];
     __shared__ double s_sum[4];
     if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
@@ -389,9 +389,12 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                     for (int f = 0; f < NRHS; ++f)
 #pragma unroll
                         for (int a = 0; a < K; ++a) B[f][a] = 0;
+                    // field values: per-particle array (sorted order, NRHS per particle) or the
+                    // analytic quadratics
                     double fi[NRHS];
 #pragma unroll
-                    for (int f = 0; f < NRHS; ++f) fi[f] = quad_fast(P.coef + 10 * f, xi, yi, zi);
+                    for (int f = 0; f < NRHS; ++f)
+                        fi[f] = fvals ? fvals[(size_t)k * NRHS + f] : quad_fast(P.coef + 10 * f, xi, yi, zi);
                     for (int e = row[k]; e < row[k + 1]; ++e) {
                         int m = col[e];
                         double xm = sx[m], ym = sy[m], zm = sz[m];
@@ -405,7 +408,8 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                         basis_fast(dx, dy, dz, ir, l0inv, q);
 #pragma unroll
                         for (int f = 0; f < NRHS; ++f) {
-                            double df = (quad_fast(P.coef + 10 * f, xm, ym, zm) - fi[f]) * w * ir;
+                            const double fm = fvals ? fvals[(size_t)m * NRHS + f] : quad_fast(P.coef + 10 * f, xm, ym, zm);
+                            double df = (fm - fi[f]) * w * ir;
 #pragma unroll
                             for (int a = 0; a < K; ++a) B[f][a] += q[a] * df;
                         }
@@ -462,6 +466,10 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                     for (int a = 0; a < K; ++a) zout[(size_t)k * K + a] = z[a];
 #pragma unroll
                     for (int f = 0; f < NRHS; ++f) {
+                        if (P.store)
+#pragma unroll
+                            for (int a = 0; a < K; ++a) xout[((size_t)k * NRHS + f) * K + a] = B[f][a];
+                        if (fvals) continue;  // no analytic field to measure against
                         const double* c = P.coef + 10 * f;
                         double gx = c[1] + 2 * c[4] * xi + c[7] * yi + c[8] * zi;
                         double gy = c[2] + 2 * c[5] * yi + c[7] * xi + c[9] * zi;
@@ -474,9 +482,6 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                         se_l += le * le;
                         mx_g = fmax(mx_g, ge);
                         mx_l = fmax(mx_l, le);
-                        if (P.store)
-#pragma unroll
-                            for (int a = 0; a < K; ++a) xout[((size_t)k * NRHS + f) * K + a] = B[f][a];
                     }
                 }
             }
@@ -513,16 +518,25 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
 // Block sizes the autotuner chooses from (one particle per thread: same bits for each).
 constexpr int WLS_BLOCK[3] = {32, 64, 128};
 
+// Outputs of one all-particle WLS launch (sorted order).
+struct WlsOut {
+    int* status;
+    double *z, *wsum, *x;
+};
+
 template <int NRHS, int PREC>
-void launch_all(lsmps_ctx* ctx, const WlsParams& P, unsigned long long* gcnt, double* gsum) {
+void launch_all(lsmps_ctx* ctx, const WlsParams& P, unsigned long long* gcnt, double* gsum,
+                const double* fvals = nullptr, const WlsOut* dst = nullptr) {
     int n = (int)ctx->n;
     if (!n) return;
+    const WlsOut o = dst ? *dst
+                         : WlsOut{ctx->wls_status.get<int>(), ctx->wls_z.get<double>(), ctx->wls_wsum.get<double>(),
+                                  ctx->wls_x.get<double>()};
     auto go = [&](int c) {
         const int t = WLS_BLOCK[c];
         k_wls_all<NRHS, PREC><<<blocks_for(n, t), t, 0, ctx->stream>>>(
             P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
-            ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), ctx->wls_status.get<int>(), ctx->wls_z.get<double>(),
-            ctx->wls_wsum.get<double>(), ctx->wls_x.get<double>(), gcnt, gsum);
+            ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), o.status, o.z, o.wsum, o.x, gcnt, gsum, fvals);
         LSMPS_CHECK_LAUNCH();
     };
     static const std::vector<std::string> names = {"block32", "block64", "block128"};
@@ -632,6 +646,60 @@ void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* o, lsmps_wls_stats* out) {
     ctx->wls_stored = P.store != 0;
     ctx->have_ppe = ctx->have_solution = false;
     if (out) *out = st;
+}
+
+namespace {
+// caller order (n x nrhs) -> sorted order, and the solutions back
+__global__ void k_fields_to_sorted(const int* __restrict__ perm, size_t n, int nrhs, const double* __restrict__ in,
+                                   double* __restrict__ out) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = (size_t)perm[k];
+        for (int f = 0; f < nrhs; ++f) out[k * nrhs + f] = in[i * nrhs + f];
+    }
+}
+__global__ void k_solutions_to_caller(const int* __restrict__ iperm, size_t n, int nrhs, const double* __restrict__ x,
+                                      double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = (size_t)iperm[i];
+        for (int a = 0; a < nrhs * K; ++a) out[i * nrhs * K + a] = x[k * nrhs * K + a];
+    }
+}
+}  // namespace
+
+void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out) {
+    LSMPS_REQUIRE(ctx->have_neighbors && ctx->have_classes, LSMPS_ERR_STATE,
+                  "WLS of fields needs neighbor lists and classification first");
+    LSMPS_REQUIRE(nrhs >= 1 && nrhs <= 3, LSMPS_ERR_ARG, "WLS of fields takes 1..3 fields");
+    const size_t n = ctx->n;
+    LSMPS_REQUIRE(n == 0 || (d_fields && d_out), LSMPS_ERR_ARG, "null field or output buffer");
+    cudaStream_t s = ctx->stream;
+    WlsParams P{};
+    P.re = ctx->re;
+    P.l0 = ctx->l0;
+    P.reg = 1e-8;
+    P.nrhs = nrhs;
+    P.precision = 0;
+    P.store = 1;
+    double* fs = ctx->wf_in.ensure<double>(n * nrhs + 1);
+    WlsOut o{ctx->wf_status.ensure<int>(n + 1), ctx->wf_z.ensure<double>(n * K + 1), ctx->wf_wsum.ensure<double>(n + 1),
+             ctx->wf_x.ensure<double>(n * nrhs * K + 1)};
+    auto* gcnt = reinterpret_cast<unsigned long long*>(ctx->wf_stats.ensure<double>(16));
+    double* gsum = reinterpret_cast<double*>(gcnt + 8);
+    LSMPS_CUDA(cudaMemsetAsync(gcnt, 0, 16 * sizeof(double), s));
+    if (n) {
+        LSMPS_CUDA(cudaMemsetAsync(o.x, 0, n * nrhs * K * sizeof(double), s));  // failed rows stay 0
+        k_fields_to_sorted<<<std::min<unsigned>(blocks_for(n, 256), 1184), 256, 0, s>>>(ctx->perm.get<int>(), n, nrhs,
+                                                                                      d_fields, fs);
+        LSMPS_CHECK_LAUNCH();
+    }
+    if (nrhs == 1) launch_all<1, 0>(ctx, P, gcnt, gsum, fs, &o);
+    else if (nrhs == 2) launch_all<2, 0>(ctx, P, gcnt, gsum, fs, &o);
+    else launch_all<3, 0>(ctx, P, gcnt, gsum, fs, &o);
+    if (n) {
+        k_solutions_to_caller<<<std::min<unsigned>(blocks_for(n, 256), 1184), 256, 0, s>>>(ctx->iperm.get<int>(), n,
+                                                                                         nrhs, o.x, d_out);
+        LSMPS_CHECK_LAUNCH();
+    }
 }
 
 void wls_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes) {

@@ -63,6 +63,14 @@ class PpeOpts(C.Structure):
                 ("re", C.c_double), ("l0", C.c_double), ("diag_shift", C.c_double)]
 
 
+class ProjectionStats(C.Structure):
+    _fields_ = [("unknowns", C.c_uint64), ("measured", C.c_uint64), ("div_before_rms", C.c_double),
+                ("div_before_max", C.c_double), ("div_after_rms", C.c_double), ("div_after_max", C.c_double),
+                ("iterations", C.c_int32), ("converged", C.c_int32), ("relative_residual", C.c_double),
+                ("solve_ms", C.c_double), ("total_ms", C.c_double), ("core", C.c_uint64),
+                ("div_core_before_rms", C.c_double), ("div_core_after_rms", C.c_double)]
+
+
 class SeriesParams(C.Structure):
     _fields_ = [("steps", C.c_int32), ("injected_per_step", C.c_int32), ("cnl_rebuild_interval", C.c_int32),
                 ("solver", C.c_int32), ("l0", C.c_double), ("re", C.c_double), ("skin", C.c_double),
@@ -150,6 +158,9 @@ SIGNATURES = {
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
     "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_wls_fields": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "lsmps_projection_step": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.POINTER(SolverOpts), _vp, _vp,
+                                        C.POINTER(ProjectionStats)]),
     "lsmps_series_create": (C.c_int, [_vp, C.POINTER(SeriesParams), _vp, _vp, C.c_size_t, C.POINTER(_vp)]),
     "lsmps_series_step": (C.c_int, [_vp, C.POINTER(SeriesStats)]),
     "lsmps_series_particles": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -377,6 +388,37 @@ class Context:
         p = np.zeros(unknowns)
         self._check(self.L.lsmps_download_pressure(self.h, _p(p), unknowns))
         return p
+
+    def wls_fields(self, fields):
+        """WLS solutions (n x k x 9) of k per-particle fields (torch CUDA tensor or array, n x k;
+        caller order): gradient, l0 x second derivatives (lsmps_wls_fields)."""
+        import torch
+
+        f = torch.as_tensor(fields, dtype=torch.float64, device="cuda")
+        f = f.reshape(f.shape[0], -1).contiguous()
+        out = torch.zeros((f.shape[0], f.shape[1], 9), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        self._check(self.L.lsmps_wls_fields(self.h, C.c_void_p(f.data_ptr()), f.shape[1],
+                                            C.c_void_p(out.data_ptr())))
+        self.sync()
+        return out
+
+    def projection_step(self, vel, dt, rho, solver="mixed", max_iter=20000, tol=1e-10, warm_start=False):
+        """One pressure projection of velocity vel (n x 3, caller order) on the assembled
+        WLS-Laplacian PPE: (corrected velocity, pressure per particle, ProjectionStats)."""
+        import torch
+
+        u = torch.as_tensor(vel, dtype=torch.float64, device="cuda").reshape(-1, 3).contiguous()
+        out = torch.empty_like(u)
+        p = torch.zeros(u.shape[0], dtype=torch.float64, device="cuda")
+        o = SolverOpts(solver=SOLVERS.get(solver, solver), max_iter=int(max_iter), tol=tol,
+                       warm_start=1 if warm_start else 0, use_graph=1)
+        st = ProjectionStats()
+        torch.cuda.synchronize()
+        self._check(self.L.lsmps_projection_step(self.h, C.c_void_p(u.data_ptr()), dt, rho, C.byref(o),
+                                                 C.c_void_p(out.data_ptr()), C.c_void_p(p.data_ptr()), C.byref(st)))
+        self.sync()
+        return out, p, st
 
     def set_initial_pressure(self, p_particles):
         """Warm start of the next solve (warm_start=True) from one value per particle (caller order)."""

@@ -222,9 +222,15 @@ void orc_classify(const double* xyz, const uint8_t* type_in, size_t n, const int
 // and sum w (wsum_out[i]), from which the WLS Laplacian operator is
 //   lap_i(f) = sum_j c_ij (f_j - f_i),  c_ij = w_ij q_ij . z_i / (r_ij sum_w l0).
 // status: 0 ok, 1 regularised, 2 skipped type, 3 sum w <= 0, 4 Cholesky failed.
-void orc_wls(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr,
-             const int* col, double re, double l0, double reg, int nrhs, const double* coef,
-             double* x_out, int* status, double* z_out, double* wsum_out) {
+// Field values either from the quadratics coef (nrhs x 10) or from the array fields
+// (n x nrhs, per particle).
+static void wls_impl(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr, const int* col,
+                     double re, double l0, double reg, int nrhs, const double* coef, const double* fields,
+                     double* x_out, int* status, double* z_out, double* wsum_out) {
+    auto fval = [&](int k, size_t p) {
+        return fields ? fields[p * nrhs + k]
+                      : quad_eval(coef + 10 * k, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2]);
+    };
     std::vector<double> bb((size_t)nrhs * K);
     for (size_t i = 0; i < n; ++i) {
         if (x_out) std::fill(x_out + i * nrhs * K, x_out + (i + 1) * nrhs * K, 0.0);
@@ -244,9 +250,7 @@ void orc_wls(const double* xyz, const uint8_t* type, size_t n, const int* row_pt
             basis(dx, dy, dz, r, l0, q);
             ws += w;
             for (int k = 0; k < nrhs; ++k) {
-                const double* c = coef + 10 * k;
-                double df = quad_eval(c, xyz[3 * j], xyz[3 * j + 1], xyz[3 * j + 2]) -
-                            quad_eval(c, xi, yi, zi);
+                double df = fval(k, (size_t)j) - fval(k, i);
                 for (int a = 0; a < K; ++a) bb[k * K + a] += w * q[a] * df / r;
             }
             for (int a = 0; a < K; ++a)
@@ -266,6 +270,20 @@ void orc_wls(const double* xyz, const uint8_t* type, size_t n, const int* row_pt
             chol_solve(M, e, z_out + i * K);
         }
     }
+}
+
+void orc_wls(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr,
+             const int* col, double re, double l0, double reg, int nrhs, const double* coef,
+             double* x_out, int* status, double* z_out, double* wsum_out) {
+    wls_impl(xyz, type, n, row_ptr, col, re, l0, reg, nrhs, coef, nullptr, x_out, status, z_out, wsum_out);
+}
+
+// The same WLS for per-particle fields (n x nrhs): the solutions a projection step's
+// gradients come from (lsmps_wls_fields).
+void orc_wls_fields(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr, const int* col,
+                    double re, double l0, double reg, int nrhs, const double* fields, double* x_out,
+                    int* status) {
+    wls_impl(xyz, type, n, row_ptr, col, re, l0, reg, nrhs, nullptr, fields, x_out, status, nullptr, nullptr);
 }
 
 // Pressure-Poisson assembly. Unknowns are Interior or NearWall particles in index order,

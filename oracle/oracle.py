@@ -200,6 +200,8 @@ class Oracle:
             L.orc_classify.argtypes = [_dp, _up, C.c_size_t, _ip, _ip, C.c_double, _up]
             L.orc_wls.argtypes = [_dp, _up, C.c_size_t, _ip, _ip, C.c_double, C.c_double, C.c_double,
                                   C.c_int, _dp, C.c_void_p, _ip, C.c_void_p, C.c_void_p]
+            L.orc_wls_fields.argtypes = [_dp, _up, C.c_size_t, _ip, _ip, C.c_double, C.c_double, C.c_double,
+                                         C.c_int, _dp, _dp, _ip]
             L.orc_ppe_assemble.restype = C.c_longlong
             L.orc_ppe_assemble.argtypes = [C.c_int, _dp, _up, C.c_size_t, _ip, _ip, C.c_double,
                                            C.c_double, C.c_longlong, C.c_double, C.c_void_p,
@@ -242,6 +244,17 @@ class Oracle:
                           np.ascontiguousarray(types, dtype=np.uint8), n, row, col, re, l0, reg,
                           nrhs, coef, _ptr(x), st, _ptr(z), _ptr(ws))
         return x, st, z, ws
+
+    @classmethod
+    def wls_fields(cls, xyz, types, row, col, re, l0, fields, reg=1e-8):
+        """WLS solutions (n x nfields x 9) of per-particle fields (n x nfields), and the status."""
+        fields = np.ascontiguousarray(np.atleast_2d(np.asarray(fields, dtype=np.float64).T).T)
+        n, nf = fields.shape
+        x = np.zeros((n, nf, 9)); st = np.zeros(n, np.int32)
+        cls.lib().orc_wls_fields(np.ascontiguousarray(xyz, dtype=np.float64),
+                                 np.ascontiguousarray(types, dtype=np.uint8), n, row, col, re, l0, reg, nf, fields,
+                                 x.reshape(-1), st)
+        return x, st
 
     @classmethod
     def ppe_assemble(cls, variant, xyz, types, row, col, re, l0, max_unknowns, diag_shift=0.0,
