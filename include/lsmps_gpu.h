@@ -357,6 +357,33 @@ typedef struct lsmps_series_stats {
     double neighbor_ms, wls_ms, assembly_ms, solve_ms, step_ms;
 } lsmps_series_stats;
 
+/* Rain validation outputs of each step, the reference's schema (python/rain_plate_cpu.py
+ * compute_window_metrics:182-213, compute_section_crossings:216-239, validated by
+ * python/validate_outputs.py): plate coordinate u = 1 - s / L (0 at the upper edge, 1 at the
+ * outflow edge, s along the plate, L its length), normal distance d above the plate surface.
+ * Window w: fluid particles with lo <= u < hi and 0 <= d <= wet_distance_factor l0, binned in
+ * coverage_cells cells along u; coverage = share of cells holding at least
+ * min_particles_per_cell; film thickness per occupied cell = max d + l0, and its mean, 90th
+ * percentile (linear interpolation) and maximum. Section: particles whose u went from below to
+ * at least section_u this step with 0 <= d <= max normal distance l0. Defaults: the reference's
+ * config/rain_plate_validation.json. */
+#define LSMPS_RAIN_MAX_WINDOWS 8
+#define LSMPS_RAIN_MAX_SECTIONS 8
+#define LSMPS_RAIN_MAX_CELLS 64
+typedef struct lsmps_rain_validation {
+    int32_t nwindows, nsections, coverage_cells, min_particles_per_cell;
+    double wet_distance_factor;
+    double window_lo[LSMPS_RAIN_MAX_WINDOWS], window_hi[LSMPS_RAIN_MAX_WINDOWS];
+    double section_u[LSMPS_RAIN_MAX_SECTIONS], section_max_normal[LSMPS_RAIN_MAX_SECTIONS];
+} lsmps_rain_validation;
+
+typedef struct lsmps_rain_outputs {
+    uint64_t window_particles[LSMPS_RAIN_MAX_WINDOWS];
+    double window_coverage[LSMPS_RAIN_MAX_WINDOWS];
+    double film_mean[LSMPS_RAIN_MAX_WINDOWS], film_p90[LSMPS_RAIN_MAX_WINDOWS], film_max[LSMPS_RAIN_MAX_WINDOWS];
+    uint64_t section_crossings[LSMPS_RAIN_MAX_SECTIONS];
+} lsmps_rain_outputs;
+
 /* xyz / type: the initial particles (host, as lsmps_upload_particles; Wall marks the plate).
  * The series borrows ctx (and its network for LSMPS_SOLVER_LEARNED) until destroyed. */
 int lsmps_series_create(lsmps_ctx* ctx, const lsmps_series_params* params, const double* xyz, const uint8_t* type,
@@ -367,6 +394,10 @@ int lsmps_series_step(lsmps_series* series, lsmps_series_stats* out);
 int lsmps_series_particles(lsmps_series* series, double* xyz, uint8_t* material, double* pressure, size_t cap,
                            size_t* n);
 void lsmps_series_destroy(lsmps_series* series);
+/* Replace the validation windows and sections (takes effect at the next step). */
+int lsmps_series_set_validation(lsmps_series* series, const lsmps_rain_validation* cfg);
+/* The validation outputs of the last step. */
+int lsmps_series_rain_outputs(lsmps_series* series, lsmps_rain_outputs* out);
 
 /* ---- learned preconditioner (message-passing network over the PPE graph) ----------- */
 /* No reference counterpart. Nodes are the PPE unknowns, edges the

@@ -364,6 +364,14 @@ int lsmps_series_particles(lsmps_series* series, double* xyz, uint8_t* material,
     return guarded(series_context(series), [&] { series_particles(series, xyz, material, pressure, cap, n); });
 }
 
+int lsmps_series_set_validation(lsmps_series* series, const lsmps_rain_validation* cfg) {
+    return guarded(series_context(series), [&] { series_set_validation(series, cfg); });
+}
+
+int lsmps_series_rain_outputs(lsmps_series* series, lsmps_rain_outputs* out) {
+    return guarded(series_context(series), [&] { series_rain_outputs(series, out); });
+}
+
 void lsmps_series_destroy(lsmps_series* series) {
     if (!series) return;
     cudaSetDevice(series_context(series)->device);

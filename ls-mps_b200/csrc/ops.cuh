@@ -13,6 +13,8 @@ void series_create(lsmps_ctx* ctx, const lsmps_series_params* p, const double* x
 void series_step(lsmps_series* s, lsmps_series_stats* out);
 void series_particles(lsmps_series* s, double* xyz, uint8_t* material, double* pressure, size_t cap, size_t* n);
 void series_destroy(lsmps_series* s);
+void series_set_validation(lsmps_series* s, const lsmps_rain_validation* v);
+void series_rain_outputs(lsmps_series* s, lsmps_rain_outputs* out);
 lsmps_ctx* series_context(lsmps_series* s);
 void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_neighbor_stats* out);
 void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);

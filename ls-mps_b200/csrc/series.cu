@@ -12,6 +12,7 @@
 // The reference's step series is the 2-D penalty-force baseline python/rain_plate_cpu.py
 // (inject:67-87, remove_outflow:146-154) and the keys steps / injected_per_step /
 // cnl_rebuild_interval of config/rain_injection.cfg, which its C++ benchmark does not parse.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -31,14 +32,26 @@ struct Frame {
     double nx, nz;      // plate normal (-sin a, 0, cos a)
     double vd, vf;      // droplet fall and film slide per step (length units)
     double film_top;    // normal coordinate where a droplet joins the film
+    double plate_len;   // L: u = 1 - s / L
 };
 
+// sections of the validation outputs, as the advance kernel counts them
+struct Sections {
+    int n;
+    double u[LSMPS_RAIN_MAX_SECTIONS], maxd[LSMPS_RAIN_MAX_SECTIONS];
+};
+
+__device__ __forceinline__ double plate_u(const Frame& F, double x, double z) {
+    return 1.0 - (x * F.t1x + z * F.t1z) / F.plate_len;
+}
+
 __global__ void k_advance(size_t n, double* __restrict__ pos, uint8_t* __restrict__ mat, uint8_t* __restrict__ del,
-                          Frame F) {
+                          Frame F, Sections SC, unsigned long long* __restrict__ crossings) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint8_t m = mat[i];
         if (m == MAT_WALL) continue;
         double x = pos[3 * i], z = pos[3 * i + 2];
+        const double u0 = plate_u(F, x, z);
         if (m == MAT_DROP) {
             z -= F.vd;
             if (x * F.nx + z * F.nz <= F.film_top) {
@@ -52,6 +65,35 @@ __global__ void k_advance(size_t n, double* __restrict__ pos, uint8_t* __restric
         pos[3 * i] = x;
         pos[3 * i + 2] = z;
         if (x * F.t1x + z * F.t1z < 0.0) del[i] = 1;  // past the outflow edge
+        const double u1 = plate_u(F, x, z), d = x * F.nx + z * F.nz;
+        for (int c = 0; c < SC.n; ++c)
+            if (u0 < SC.u[c] && u1 >= SC.u[c] && d >= 0.0 && d <= SC.maxd[c]) atomicAdd(&crossings[c], 1ull);
+    }
+}
+
+// windows of the validation outputs: per window and cell along u, the fluid particle count
+// and the largest thickness d + l0 (non-negative doubles order as their bits)
+struct Windows {
+    int n, cells;
+    double wet, l0;
+    double lo[LSMPS_RAIN_MAX_WINDOWS], hi[LSMPS_RAIN_MAX_WINDOWS];
+};
+
+__global__ void k_rain_windows(size_t n, const double* __restrict__ pos, const uint8_t* __restrict__ mat, Frame F,
+                               Windows W, unsigned long long* __restrict__ count,
+                               unsigned long long* __restrict__ thick) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (mat[i] == MAT_WALL) continue;
+        const double x = pos[3 * i], z = pos[3 * i + 2];
+        const double u = plate_u(F, x, z), d = x * F.nx + z * F.nz;
+        if (d < 0.0 || d > W.wet) continue;
+        for (int w = 0; w < W.n; ++w) {
+            if (u < W.lo[w] || u >= W.hi[w]) continue;
+            const int c = min(W.cells - 1, (int)((u - W.lo[w]) / (W.hi[w] - W.lo[w]) * W.cells));
+            const size_t slot = (size_t)w * LSMPS_RAIN_MAX_CELLS + c;
+            atomicAdd(&count[slot], 1ull);
+            atomicMax(&thick[slot], (unsigned long long)__double_as_longlong(d + W.l0));
+        }
     }
 }
 
@@ -130,9 +172,12 @@ struct lsmps_series {
     std::mt19937 rng;
     std::vector<double> tmpl;  // droplet lattice offsets (x, y, z) in l0
     cudaEvent_t ev[6] = {};
+    lsmps_rain_validation vcfg{};
+    lsmps_rain_outputs vout{};
+    DevBuf vbuf;  // crossings [8], window counts [8 x 64], window thickness bits [8 x 64]
     ~lsmps_series() {
         DevBuf* bufs[] = {&pos, &mat, &type, &pres, &del, &qpos, &qmat, &qdel, &keep, &dest,
-                          &opos, &omat, &otype, &opres, &counts};
+                          &opos, &omat, &otype, &opres, &counts, &vbuf};
         for (auto* b : bufs) b->release();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -179,6 +224,19 @@ void series_create(lsmps_ctx* ctx, const lsmps_series_params* pp, const double* 
     }
     S->plate_len = smax;
     S->plate_wid = ymax;
+    S->F.plate_len = std::max(smax, p.l0);
+    // the reference's config/rain_plate_validation.json
+    lsmps_rain_validation& v = S->vcfg;
+    v.nwindows = 3;
+    v.nsections = 2;
+    v.coverage_cells = 32;
+    v.min_particles_per_cell = 1;
+    v.wet_distance_factor = 3.0;
+    const double wl[3] = {0.1, 0.4, 0.75}, wh[3] = {0.35, 0.7, 0.95};
+    for (int w = 0; w < 3; ++w) { v.window_lo[w] = wl[w]; v.window_hi[w] = wh[w]; }
+    v.section_u[0] = 0.55; v.section_u[1] = 0.9;
+    v.section_max_normal[0] = v.section_max_normal[1] = 5.0;
+    S->vbuf.ensure<unsigned long long>(LSMPS_RAIN_MAX_SECTIONS + 2 * LSMPS_RAIN_MAX_WINDOWS * LSMPS_RAIN_MAX_CELLS);
     const int R = (int)std::ceil(p.droplet_radius);
     for (int k = -R; k <= R; ++k)
         for (int j = -R; j <= R; ++j)
@@ -288,6 +346,60 @@ void merge(lsmps_series& S) {
 
 }  // namespace
 
+// Window and section outputs from the step's device histograms (host side: at most 8 x 64 cells).
+static void rain_outputs_from(lsmps_series& S, const std::vector<unsigned long long>& hv) {
+    const lsmps_rain_validation& vc = S.vcfg;
+    lsmps_rain_outputs o{};
+    for (int c = 0; c < vc.nsections; ++c) o.section_crossings[c] = hv[c];
+    const unsigned long long* cnt = hv.data() + LSMPS_RAIN_MAX_SECTIONS;
+    const unsigned long long* thk = cnt + LSMPS_RAIN_MAX_WINDOWS * LSMPS_RAIN_MAX_CELLS;
+    for (int w = 0; w < vc.nwindows; ++w) {
+        std::vector<double> t;
+        int covered = 0;
+        uint64_t np = 0;
+        for (int c = 0; c < vc.coverage_cells; ++c) {
+            const size_t slot = (size_t)w * LSMPS_RAIN_MAX_CELLS + c;
+            np += cnt[slot];
+            if (cnt[slot] >= (unsigned long long)vc.min_particles_per_cell) ++covered;
+            if (cnt[slot]) {
+                double d;
+                std::memcpy(&d, &thk[slot], sizeof(d));
+                t.push_back(d);
+            }
+        }
+        o.window_particles[w] = np;
+        o.window_coverage[w] = vc.coverage_cells ? (double)covered / vc.coverage_cells : 0.0;
+        if (!t.empty()) {
+            std::sort(t.begin(), t.end());
+            double sum = 0;
+            for (double v : t) sum += v;
+            o.film_mean[w] = sum / t.size();
+            const double q = 0.9 * (t.size() - 1);  // linear interpolation between order statistics
+            const size_t lo = (size_t)std::floor(q);
+            const size_t hi = std::min(lo + 1, t.size() - 1);
+            o.film_p90[w] = t[lo] + (t[hi] - t[lo]) * (q - lo);
+            o.film_max[w] = t.back();
+        }
+    }
+    S.vout = o;
+}
+
+void series_set_validation(lsmps_series* S, const lsmps_rain_validation* v) {
+    LSMPS_REQUIRE(S && v, LSMPS_ERR_ARG, "null series or validation config");
+    LSMPS_REQUIRE(v->nwindows >= 0 && v->nwindows <= LSMPS_RAIN_MAX_WINDOWS && v->nsections >= 0 &&
+                      v->nsections <= LSMPS_RAIN_MAX_SECTIONS && v->coverage_cells >= 1 &&
+                      v->coverage_cells <= LSMPS_RAIN_MAX_CELLS && v->min_particles_per_cell >= 0,
+                  LSMPS_ERR_ARG, "validation config: at most 8 windows, 8 sections, 1..64 cells");
+    for (int w = 0; w < v->nwindows; ++w)
+        LSMPS_REQUIRE(v->window_hi[w] > v->window_lo[w], LSMPS_ERR_ARG, "validation window with hi <= lo");
+    S->vcfg = *v;
+}
+
+void series_rain_outputs(lsmps_series* S, lsmps_rain_outputs* out) {
+    LSMPS_REQUIRE(S && out, LSMPS_ERR_ARG, "null series or output");
+    *out = S->vout;
+}
+
 void series_step(lsmps_series* Sp, lsmps_series_stats* out) {
     LSMPS_REQUIRE(Sp, LSMPS_ERR_ARG, "null series");
     lsmps_series& S = *Sp;
@@ -298,15 +410,25 @@ void series_step(lsmps_series* Sp, lsmps_series_stats* out) {
     S.step += 1;
     st.step = S.step;
     LSMPS_CUDA(cudaEventRecord(S.ev[0], s));
+    // validation accumulators of this step
+    const lsmps_rain_validation& vc = S.vcfg;
+    Sections SC{};
+    SC.n = vc.nsections;
+    for (int c = 0; c < vc.nsections; ++c) {
+        SC.u[c] = vc.section_u[c];
+        SC.maxd[c] = vc.section_max_normal[c] * p.l0;
+    }
+    auto* vb = S.vbuf.get<unsigned long long>();
+    LSMPS_CUDA(cudaMemsetAsync(vb, 0, S.vbuf.bytes, s));
     // 1. kinematics of the particle set and of the droplets in flight; 2. injection
     if (S.n) {
         k_advance<<<grid_for(S.n), 256, 0, s>>>(S.n, S.pos.get<double>(), S.mat.get<uint8_t>(), S.del.get<uint8_t>(),
-                                                S.F);
+                                                S.F, SC, vb);
         LSMPS_CHECK_LAUNCH();
     }
     if (S.nq) {
         k_advance<<<grid_for(S.nq), 256, 0, s>>>(S.nq, S.qpos.get<double>(), S.qmat.get<uint8_t>(),
-                                                 S.qdel.get<uint8_t>(), S.F);
+                                                 S.qdel.get<uint8_t>(), S.F, SC, vb);
         LSMPS_CHECK_LAUNCH();
     }
     inject(S);
@@ -379,9 +501,29 @@ void series_step(lsmps_series* Sp, lsmps_series_stats* out) {
         k_count<<<grid_for(S.nq), 256, 0, s>>>(S.nq, S.qmat.get<uint8_t>(), S.qdel.get<uint8_t>(), cnt + 2);
         LSMPS_CHECK_LAUNCH();
     }
+    // validation windows over the fluid of the set and in flight (the domain's fluid)
+    Windows W{};
+    W.n = vc.nwindows;
+    W.cells = vc.coverage_cells;
+    W.wet = vc.wet_distance_factor * p.l0;
+    W.l0 = p.l0;
+    for (int w = 0; w < vc.nwindows; ++w) {
+        W.lo[w] = vc.window_lo[w];
+        W.hi[w] = vc.window_hi[w];
+    }
+    unsigned long long* wcount = vb + LSMPS_RAIN_MAX_SECTIONS;
+    unsigned long long* wthick = wcount + LSMPS_RAIN_MAX_WINDOWS * LSMPS_RAIN_MAX_CELLS;
+    if (S.n) k_rain_windows<<<grid_for(S.n), 256, 0, s>>>(S.n, S.pos.get<double>(), S.mat.get<uint8_t>(), S.F, W,
+                                                         wcount, wthick);
+    if (S.nq) k_rain_windows<<<grid_for(S.nq), 256, 0, s>>>(S.nq, S.qpos.get<double>(), S.qmat.get<uint8_t>(), S.F, W,
+                                                           wcount, wthick);
+    LSMPS_CHECK_LAUNCH();
     unsigned long long hc[4];
+    std::vector<unsigned long long> hv(LSMPS_RAIN_MAX_SECTIONS + 2 * LSMPS_RAIN_MAX_WINDOWS * LSMPS_RAIN_MAX_CELLS);
     LSMPS_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaMemcpyAsync(hv.data(), vb, hv.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     LSMPS_CUDA(cudaStreamSynchronize(s));
+    rain_outputs_from(S, hv);
     float ms[4];  // neighbor lists, WLS, assembly, whole step
     LSMPS_CUDA(cudaEventElapsedTime(&ms[0], S.ev[1], S.ev[2]));
     LSMPS_CUDA(cudaEventElapsedTime(&ms[1], S.ev[2], S.ev[3]));

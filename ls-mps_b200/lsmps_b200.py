@@ -96,6 +96,27 @@ class SeriesStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+RAIN_MAX = 8
+
+
+class RainValidation(C.Structure):
+    _fields_ = [("nwindows", C.c_int32), ("nsections", C.c_int32), ("coverage_cells", C.c_int32),
+                ("min_particles_per_cell", C.c_int32), ("wet_distance_factor", C.c_double),
+                ("window_lo", C.c_double * RAIN_MAX), ("window_hi", C.c_double * RAIN_MAX),
+                ("section_u", C.c_double * RAIN_MAX), ("section_max_normal", C.c_double * RAIN_MAX)]
+
+
+class RainOutputs(C.Structure):
+    _fields_ = [("window_particles", C.c_uint64 * RAIN_MAX), ("window_coverage", C.c_double * RAIN_MAX),
+                ("film_mean", C.c_double * RAIN_MAX), ("film_p90", C.c_double * RAIN_MAX),
+                ("film_max", C.c_double * RAIN_MAX), ("section_crossings", C.c_uint64 * RAIN_MAX)]
+
+
+# the reference's config/rain_plate_validation.json (windows and sections in plate coordinate u)
+RAIN_WINDOWS = [("impact_zone", 0.1, 0.35), ("film_zone", 0.4, 0.7), ("outlet_zone", 0.75, 0.95)]
+RAIN_SECTIONS = [("mid_section", 0.55, 5.0), ("outlet_section", 0.9, 5.0)]
+
+
 SERIES_DEFAULTS = dict(steps=200, injected_per_step=2000, cnl_rebuild_interval=10, solver="learned", l0=1.0, re=2.1,
                        skin=1.0, droplet_speed=0.05, film_speed=0.02, theta_deg=20.0, film_thickness=4.0,
                        droplet_radius=3.0, inject_hmin=10.0, inject_hmax=40.0, tol=3e-11, max_iter=20000,
@@ -165,6 +186,8 @@ SIGNATURES = {
     "lsmps_series_step": (C.c_int, [_vp, C.POINTER(SeriesStats)]),
     "lsmps_series_particles": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "lsmps_series_destroy": (None, [_vp]),
+    "lsmps_series_set_validation": (C.c_int, [_vp, C.POINTER(RainValidation)]),
+    "lsmps_series_rain_outputs": (C.c_int, [_vp, C.POINTER(RainOutputs)]),
     "lsmps_set_initial_pressure_device": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_download_pressure_particles": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
     "lsmps_download_pressure_particles_device": (C.c_int, [_vp, _vp, C.c_size_t, C.c_double]),
@@ -531,6 +554,16 @@ class Series:
         st = SeriesStats()
         self.ctx._check(self.ctx.L.lsmps_series_step(self.h, C.byref(st)))
         return st
+
+    def rain_outputs(self):
+        """Validation outputs of the last step: {window: (particles, coverage, film mean, p90, max)},
+        {section: crossings} (the default windows and sections are RAIN_WINDOWS, RAIN_SECTIONS)."""
+        o = RainOutputs()
+        self.ctx._check(self.ctx.L.lsmps_series_rain_outputs(self.h, C.byref(o)))
+        win = {name: (o.window_particles[w], o.window_coverage[w], o.film_mean[w], o.film_p90[w], o.film_max[w])
+               for w, (name, _, _) in enumerate(RAIN_WINDOWS)}
+        sec = {name: o.section_crossings[c] for c, (name, _, _) in enumerate(RAIN_SECTIONS)}
+        return win, sec
 
     def particles(self):
         """(xyz, material, pressure) of the current particle set (material: 0 wall, 1 film, 2 droplet)."""

@@ -10,7 +10,11 @@ particles and injection seed, so every step has the same particles for every sol
 step: neighbor lists (candidate rebuild every --interval steps, refresh in between), WLS,
 WLS-Laplacian PPE with the manufactured p* = sin(0.3x) cos(0.2y) + 0.1z, solve warm-started
 from the previous pressure; mass balance (device fluid count against initial + injected -
-deleted) and PPE relative L2 per step. Writes series_<solver>.csv per solver and summary.json.
+deleted) and PPE relative L2 per step. Writes series_<solver>.csv per solver and summary.json,
+and (from the first solver's run; the particles are the same for all) the reference's rain
+validation outputs in validation/: metrics.csv, sampling_windows.csv, flow_sections.csv and
+mass_conservation.csv with the columns python/validate_outputs.py requires. Lengths are in l0
+units scaled by --l0-m (meters per l0) and one step lasts --dt-s seconds.
 A .cfg (keys particles, seed, re_ratio, steps, injected_per_step, cnl_rebuild_interval) sets
 the defaults of the matching options; the plate and droplets are in units of l0 = 1.
 """
@@ -36,7 +40,49 @@ def read_cfg(path):
     return out
 
 
-def run(ctx, xyz, t, solver, a):
+def validation_rows(rows, rain, a):
+    """The reference's four validation tables (python/rain_plate_cpu.py:326-372) from the
+    series statistics and the per-step rain outputs."""
+    vol = a.l0_m ** 3
+    r0 = rows[0]
+    fluid0 = r0["fluid_particles"] - r0["injected_total"] + r0["deleted_total"] - r0["mass_balance"]
+    metrics, windows, sections, mass = [], [], [], []
+    cumulative = {}
+    for r, (win, sec) in zip(rows, rain):
+        time = r["step"] * a.dt_s
+        injected = fluid0 + r["injected_total"]  # the initial fluid counts as injected at t = 0
+        metrics.append({"step": r["step"], "time": time, "particles": r["fluid_particles"],
+                        "injected_total": injected, "outflow_total": r["deleted_total"], "invalid_removed_total": 0,
+                        "mass_error": injected - r["deleted_total"] - r["fluid_particles"],
+                        "pairs": r["pairs"], "unknowns": r["unknowns"], "in_flight": r["in_flight"],
+                        "flagged": r["flagged"]})
+        for name, (np_, cov, fmean, fp90, fmax) in win.items():
+            windows.append({"time": time, "window": name, "particle_count": np_, "fluid_volume_m3": np_ * vol,
+                            "coverage_ratio": cov, "film_mean_m": fmean * a.l0_m, "film_p90_m": fp90 * a.l0_m,
+                            "film_max_m": fmax * a.l0_m})
+        for name, n in sec.items():
+            cumulative[name] = cumulative.get(name, 0.0) + n * vol
+            sections.append({"time": time, "section": name, "crossing_particle_count": n,
+                             "instantaneous_flow_rate_m3s": n * vol / a.dt_s, "crossing_volume_m3": n * vol,
+                             "cumulative_volume_m3": cumulative[name]})
+        inj_v, rem_v, out_v = injected * vol, r["fluid_particles"] * vol, r["deleted_total"] * vol
+        bal = inj_v - rem_v - out_v
+        denom = max(inj_v, vol)
+        mass.append({"time": time, "injected_volume_m3": inj_v, "remaining_volume_m3": rem_v, "outlet_volume_m3": out_v,
+                     "invalid_removed_volume_m3": 0.0, "balance_error_m3": bal, "relative_mass_error": abs(bal) / denom,
+                     "invalid_removed_ratio": 0.0})
+    return {"metrics.csv": metrics, "sampling_windows.csv": windows, "flow_sections.csv": sections,
+            "mass_conservation.csv": mass}
+
+
+def write_csv(path, rows):
+    with open(path, "w", newline="") as f:
+        w = csv.DictWriter(f, fieldnames=list(rows[0].keys()))
+        w.writeheader()
+        w.writerows(rows)
+
+
+def run(ctx, xyz, t, solver, a, rain=None):
     rows = []
     kw = dict(steps=a.steps, injected_per_step=a.injected, cnl_rebuild_interval=a.interval, solver=solver,
               re=a.re, skin=a.skin, tol=a.tol, seed=a.seed)
@@ -45,6 +91,8 @@ def run(ctx, xyz, t, solver, a):
             st = s.step().as_dict()
             st["solver"] = solver
             rows.append(st)
+            if rain is not None:
+                rain.append(s.rain_outputs())
             if a.verbose:
                 print(f"{solver} step {st['step']}: n {st['particles']} U {st['unknowns']} it {st['iterations']} "
                       f"L2 {st['relative_l2_error']:.2e} solve {st['solve_ms']:.1f} ms step {st['step_ms']:.1f} ms "
@@ -97,6 +145,8 @@ def main():
     ap.add_argument("--weights", default=lib.DEFAULT_WEIGHTS)
     ap.add_argument("--out", default="results/series")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--l0-m", type=float, default=0.004, help="meters per l0 in the validation outputs")
+    ap.add_argument("--dt-s", type=float, default=1e-3, help="seconds per step in the validation outputs")
     a = ap.parse_args()
     cfg = read_cfg(a.cfg) if a.cfg else {}
     defaults = {"particles": ("particles", int, 3_000_000), "steps": ("steps", int, 200),
@@ -110,14 +160,17 @@ def main():
     summary = {"config": {k: getattr(a, k) for k in ("particles", "steps", "injected", "interval", "seed", "re",
                                                      "skin", "tol", "solvers")}, "solvers": {}}
     with lib.Context(0) as ctx:
-        for solver in a.solvers.split(","):
+        for k, solver in enumerate(a.solvers.split(",")):
             if solver == "learned":
                 ctx.mpnn_load(a.weights)
-            rows = run(ctx, xyz, t, solver, a)
-            with open(os.path.join(a.out, f"series_{solver}.csv"), "w", newline="") as f:
-                w = csv.DictWriter(f, fieldnames=list(rows[0].keys()))
-                w.writeheader()
-                w.writerows(rows)
+            rain = [] if k == 0 else None
+            rows = run(ctx, xyz, t, solver, a, rain)
+            write_csv(os.path.join(a.out, f"series_{solver}.csv"), rows)
+            if rain is not None:
+                vdir = os.path.join(a.out, "validation")
+                os.makedirs(vdir, exist_ok=True)
+                for name, tab in validation_rows(rows, rain, a).items():
+                    write_csv(os.path.join(vdir, name), tab)
             summary["solvers"][solver] = summarize(rows)
             print(solver, json.dumps(summary["solvers"][solver]), flush=True)
     names = list(summary["solvers"])

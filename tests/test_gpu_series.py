@@ -9,7 +9,15 @@
   balance 0); candidate rebuilds at step 1 and every interval steps; every PPE reaches
   relative L2 <= 1e-8 against p*; the warm start needs fewer iterations than the cold first
   solve; the learned and plain FP64 series see the same particles.
+* Rain validation outputs: the reference's four tables (python/validate_outputs.py columns
+  and checks restated: particle identity, coverage in [0, 1], p90 <= max, cumulative flow
+  non-decreasing, mass error within the config's 1 %), and the window statistics of the last
+  step equal a numpy recomputation from the particle positions.
 """
+import math
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -90,8 +98,12 @@ def series_runs(built, plate):
         ctx.mpnn_load(lib.DEFAULT_WEIGHTS)
         for solver in ("learned", "fp64"):
             with lib.Series(ctx, xyz, t, solver=solver, **SMALL) as s:
-                rows = [s.step() for _ in range(SMALL["steps"])]
+                rows, rain = [], []
+                for _ in range(SMALL["steps"]):
+                    rows.append(s.step())
+                    rain.append(s.rain_outputs())
                 out[solver] = (rows, s.particles())
+                out[solver + "_rain"] = rain
     return out
 
 
@@ -124,3 +136,64 @@ def test_series_same_particles_for_both_solvers(series_runs):
     assert [r.particles for r in ra] == [r.particles for r in rb]
     assert [r.unknowns for r in ra] == [r.unknowns for r in rb]
     assert np.array_equal(xa, xb) and np.array_equal(ma, mb)
+
+
+REQUIRED = {
+    "metrics.csv": {"step", "time", "particles", "injected_total", "outflow_total", "invalid_removed_total",
+                    "mass_error"},
+    "sampling_windows.csv": {"time", "window", "particle_count", "fluid_volume_m3", "coverage_ratio", "film_mean_m",
+                             "film_p90_m", "film_max_m"},
+    "flow_sections.csv": {"time", "section", "crossing_particle_count", "instantaneous_flow_rate_m3s",
+                          "crossing_volume_m3", "cumulative_volume_m3"},
+    "mass_conservation.csv": {"time", "injected_volume_m3", "remaining_volume_m3", "outlet_volume_m3",
+                              "invalid_removed_volume_m3", "balance_error_m3", "relative_mass_error",
+                              "invalid_removed_ratio"},
+}
+
+
+def test_rain_validation_outputs(series_runs):
+    sys.path.insert(0, os.path.dirname(lib.__file__))
+    import run_series
+
+    rows, (xyz, mat, _) = series_runs["fp64"]
+    rain = series_runs["fp64_rain"]
+
+    class A:
+        l0_m, dt_s = 0.004, 1e-3
+
+    tabs = run_series.validation_rows([r.as_dict() for r in rows], rain, A)
+    for name, cols in REQUIRED.items():
+        tab = tabs[name]
+        assert tab and cols <= set(tab[0])
+        assert all(math.isfinite(float(v)) for r in tab for k, v in r.items() if k not in ("window", "section"))
+    m = tabs["metrics.csv"]
+    assert all(b["time"] > a["time"] for a, b in zip(m, m[1:]))
+    for r in m:
+        assert r["injected_total"] - r["outflow_total"] - r["invalid_removed_total"] - r["particles"] == r["mass_error"]
+        assert r["mass_error"] == 0
+    for r in tabs["sampling_windows.csv"]:
+        assert 0 <= r["coverage_ratio"] <= 1 and r["film_p90_m"] <= r["film_max_m"] + 1e-15
+    by = {}
+    for r in tabs["flow_sections.csv"]:
+        by.setdefault(r["section"], []).append(r["cumulative_volume_m3"])
+    assert all(all(b >= a for a, b in zip(v, v[1:])) for v in by.values())
+    assert max(r["relative_mass_error"] for r in tabs["mass_conservation.csv"]) <= 0.01
+    # the last step's windows from the positions (numpy), the same definitions
+    a = math.radians(20.0)
+    t1 = np.array([math.cos(a), 0, math.sin(a)])
+    nrm = np.array([-math.sin(a), 0, math.cos(a)])
+    plate_len = max((xyz[mat == 0] @ t1).max(), 1.0)
+    fluid = mat != 0
+    u = 1 - (xyz[fluid] @ t1) / plate_len
+    d = xyz[fluid] @ nrm
+    win, _ = rain[-1]
+    for name, lo, hi in lib.RAIN_WINDOWS:
+        sel = (u >= lo) & (u < hi) & (d >= 0) & (d <= 3.0)
+        cell = np.minimum(31, ((u[sel] - lo) / (hi - lo) * 32).astype(int))
+        cnt = np.bincount(cell, minlength=32)
+        thick = np.array([d[sel][cell == c].max() + 1.0 for c in range(32) if cnt[c]])
+        np_, cov, fmean, fp90, fmax = win[name]
+        assert np_ == sel.sum() and cov == (cnt >= 1).sum() / 32
+        if len(thick):
+            assert abs(fmean - thick.mean()) <= 1e-12 and abs(fp90 - np.quantile(thick, 0.9)) <= 1e-12
+            assert abs(fmax - thick.max()) <= 1e-12  # d = x n_x + z n_z: FMA on the GPU
