@@ -165,7 +165,7 @@ typedef struct lsmps_wls_stats {
 int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
 
 /* ---- PPE assembly ----------------------------------------------------------------- */
-enum { LSMPS_PPE_REFERENCE = 0, LSMPS_PPE_SHIFTED = 1, LSMPS_PPE_WLS = 2 };
+enum { LSMPS_PPE_REFERENCE = 0, LSMPS_PPE_SHIFTED = 1, LSMPS_PPE_WLS = 2, LSMPS_PPE_LOADED = 3 /* lsmps_ppe_load_csr */ };
 
 typedef struct lsmps_ppe_opts {
     int32_t variant;         /* LSMPS_PPE_* */
@@ -188,6 +188,16 @@ typedef struct lsmps_ppe_stats {
 
 /* assemble_ppe (src/lsmps.cpp:30-64) and its variants; keeps A, b = A p*, p* on the device. */
 int lsmps_ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);
+
+/* A caller's sparse system in place of an assembled PPE, for the solvers and kernel benches
+ * (e.g. the synthetic CSR that the reference's python/workload_calibration.py:253-301 writes):
+ * host CSR with n rows, row_ptr (n + 1, 64-bit), col (row_ptr[n] entries, any order,
+ * duplicates allowed; entries on the diagonal are summed into it), val (NULL: -1 for every
+ * off-diagonal entry and a diagonal of (off-diagonal count) (1 + 1e-3), at least 1), b (NULL:
+ * b = A 1, and the error statistics measure against p* = 1). Rows are the unknowns in the given
+ * numbering. The learned solver and the per-particle calls refuse a loaded system. */
+int lsmps_ppe_load_csr(lsmps_ctx* ctx, const int64_t* row_ptr, const int32_t* col, const double* val,
+                       const double* b, size_t n, lsmps_ppe_stats* out);
 
 /* ---- PPE solve -------------------------------------------------------------------- */
 enum {

@@ -92,6 +92,8 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf ref_rank, u_of_sorted, sorted_of_u, ref_of_u, u_of_ref;
     lsmps_gpu::DevBuf A_row, A_col, A_val, A_valf, A_b, A_xexact, A_dinv, A_dinvf, A_cnt;
     lsmps_ppe_stats ppe_assembly{};
+    bool ppe_loaded = false;        // the system came from lsmps_ppe_load_csr (no particles behind it)
+    lsmps_gpu::DevBuf ld_ident;     // identity map standing in for the particle permutation
     // SELL-32 copies of A for the fast solvers (built on first use after an assembly)
     bool have_sell = false, have_sell_s = false, have_sell_f = false;
     long long sell_nslices = 0, sell_entries = 0;

@@ -1111,7 +1111,8 @@ void mpnn_load(lsmps_ctx* ctx, const char* path) {
 size_t mpnn_param_count() { return NPARAM; }
 
 void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
-    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "manufactured fields need an assembled system");
+    LSMPS_REQUIRE(ctx->have_ppe && !ctx->ppe_loaded, LSMPS_ERR_STATE,
+                  "manufactured fields need an assembled particle system");
     LSMPS_REQUIRE(params && nmodes >= 0 && nmodes <= 64, LSMPS_ERR_ARG, "manufactured field parameters");
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;

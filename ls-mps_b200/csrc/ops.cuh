@@ -36,6 +36,8 @@ void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho,
 
 // ppe.cu
 void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);
+void ppe_load_csr(lsmps_ctx* ctx, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                  size_t n, lsmps_ppe_stats* out);
 void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, double* b, double* xe,
                   int32_t* unknown_particle);
 

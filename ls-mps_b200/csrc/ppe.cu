@@ -1,3 +1,6 @@
+#include <algorithm>
+#include <vector>
+#include <climits>
 // Pressure-Poisson (PPE) CSR assembly on sm_100a.
 //
 // Unknowns are the Interior / NearWall particles ranked in caller order and capped at
@@ -333,6 +336,89 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     ctx->U = U;
     ctx->nnz = nnz;
     ctx->ppe_variant = o->variant;
+    ctx->ppe_loaded = false;
+    ctx->have_ppe = true;
+    ctx->have_solution = false;
+    ctx->assembly_gen += 1;
+    ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = false;
+    ctx->ppe_assembly = ps;
+    if (out) *out = ps;
+}
+
+// A caller's system in place of an assembled one (rows = unknowns, identity numbering). The
+// diagonal goes last in every row, as the assembly stores it; entries j == i are summed into it.
+// Without values: -1 for every off-diagonal entry and a diagonal of (off-diagonal count)
+// (1 + 1e-3) (at least 1), a diagonally dominant operator; without b: b = A 1 and p* = 1.
+void ppe_load_csr(lsmps_ctx* ctx, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                  size_t n, lsmps_ppe_stats* out) {
+    LSMPS_REQUIRE(row_ptr && (n == 0 || col || row_ptr[n] == 0), LSMPS_ERR_ARG, "null CSR arrays");
+    LSMPS_REQUIRE(n < (size_t)INT_MAX && row_ptr[0] == 0, LSMPS_ERR_ARG, "row_ptr[0] must be 0 and n < 2^31");
+    const int64_t nnz_in = row_ptr[n];
+    std::vector<int> arow(n + 1), acol;
+    std::vector<double> aval, adinv(n), ab(n), axe(n);
+    acol.reserve((size_t)nnz_in + n);
+    aval.reserve((size_t)nnz_in + n);
+    arow[0] = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const int64_t e0 = row_ptr[i], e1 = row_ptr[i + 1];
+        LSMPS_REQUIRE(e1 >= e0 && e1 <= nnz_in, LSMPS_ERR_ARG, "row_ptr must be non-decreasing up to row_ptr[n]");
+        double diag = 0;
+        int off = 0;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int32_t j = col[e];
+            LSMPS_REQUIRE(j >= 0 && (size_t)j < n, LSMPS_ERR_ARG, "column index out of range");
+            if ((size_t)j == i) {
+                if (val) diag += val[e];
+                continue;
+            }
+            acol.push_back(j);
+            aval.push_back(val ? val[e] : -1.0);
+            ++off;
+        }
+        if (!val) diag = std::max(1.0, off * (1.0 + 1e-3));
+        LSMPS_REQUIRE(std::isfinite(diag) && diag != 0.0, LSMPS_ERR_ARG,
+                      "row " + std::to_string(i) + " has a zero or non-finite diagonal");
+        acol.push_back((int)i);
+        aval.push_back(diag);
+        adinv[i] = 1.0 / diag;
+        LSMPS_REQUIRE(acol.size() < (size_t)INT_MAX, LSMPS_ERR_OVERFLOW, "more than 2^31 entries");
+        arow[i + 1] = (int)acol.size();
+    }
+    for (size_t i = 0; i < n; ++i) {
+        if (b) {
+            ab[i] = b[i];
+            axe[i] = 0.0;
+        } else {
+            double s = 0;
+            for (int e = arow[i]; e < arow[i + 1]; ++e) s += aval[e];
+            ab[i] = s;
+            axe[i] = 1.0;
+        }
+    }
+    std::vector<int> ident(n);
+    for (size_t i = 0; i < n; ++i) ident[i] = (int)i;
+    cudaStream_t s = ctx->stream;
+    const size_t nnz = acol.size();
+    auto up = [&](DevBuf& d, const void* h, size_t bytes) {
+        void* p = d.ensure<char>(bytes + 16);
+        if (bytes) LSMPS_CUDA(cudaMemcpyAsync(p, h, bytes, cudaMemcpyHostToDevice, s));
+    };
+    up(ctx->A_row, arow.data(), (n + 1) * sizeof(int));
+    up(ctx->A_col, acol.data(), nnz * sizeof(int));
+    up(ctx->A_val, aval.data(), nnz * sizeof(double));
+    up(ctx->A_b, ab.data(), n * sizeof(double));
+    up(ctx->A_xexact, axe.data(), n * sizeof(double));
+    up(ctx->A_dinv, adinv.data(), n * sizeof(double));
+    for (DevBuf* d : {&ctx->ref_of_u, &ctx->u_of_ref, &ctx->sorted_of_u, &ctx->ld_ident})
+        up(*d, ident.data(), n * sizeof(int));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    lsmps_ppe_stats ps{};
+    ps.unknowns = n;
+    ps.nnz = nnz;
+    ctx->U = (long long)n;
+    ctx->nnz = (long long)nnz;
+    ctx->ppe_variant = LSMPS_PPE_LOADED;
+    ctx->ppe_loaded = true;
     ctx->have_ppe = true;
     ctx->have_solution = false;
     ctx->assembly_gen += 1;
@@ -365,7 +451,8 @@ void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, doubl
                                                       ctx->A_row.get<int>(), ctx->A_col.get<int>(),
                                                       ctx->A_val.get<double>(), ctx->A_b.get<double>(),
                                                       ctx->A_xexact.get<double>(), ctx->sorted_of_u.get<int>(),
-                                                      ctx->perm.get<int>(), U, orow, ocol, oval, ob, oxe, opart);
+                                                      ctx->ppe_loaded ? ctx->ld_ident.get<int>() : ctx->perm.get<int>(),
+                                                      U, orow, ocol, oval, ob, oxe, opart);
         LSMPS_CHECK_LAUNCH();
     }
     if (row) LSMPS_CUDA(cudaMemcpyAsync(row, orow, (U + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -1548,7 +1548,8 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
 }
 
 void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool device) {
-    LSMPS_REQUIRE(ctx->have_ppe, LSMPS_ERR_STATE, "initial guess needs an assembled system");
+    LSMPS_REQUIRE(ctx->have_ppe && !ctx->ppe_loaded, LSMPS_ERR_STATE,
+                  "per-particle initial guesses need an assembled particle system");
     LSMPS_REQUIRE(n == ctx->n && (n == 0 || pp), LSMPS_ERR_ARG, "initial guess must hold one value per particle");
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;
@@ -1569,6 +1570,7 @@ void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool 
 
 void ppe_pressure_particles(lsmps_ctx* ctx, double* pp, size_t n, double fill, bool device) {
     LSMPS_REQUIRE(ctx->have_solution, LSMPS_ERR_STATE, "no solution: lsmps_ppe_solve first");
+    LSMPS_REQUIRE(!ctx->ppe_loaded, LSMPS_ERR_STATE, "per-particle pressure needs an assembled particle system");
     LSMPS_REQUIRE(n == ctx->n && (n == 0 || pp), LSMPS_ERR_ARG, "output must hold one value per particle");
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;
@@ -1593,6 +1595,8 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
     LSMPS_REQUIRE(o && o->solver >= 0 && o->solver <= 5, LSMPS_ERR_ARG, "unknown solver");
     LSMPS_REQUIRE(o->solver != LSMPS_SOLVER_LEARNED || mpnn_ready(ctx), LSMPS_ERR_STATE,
                   "learned solver needs lsmps_mpnn_init / lsmps_mpnn_load first");
+    LSMPS_REQUIRE(o->solver != LSMPS_SOLVER_LEARNED || !ctx->ppe_loaded, LSMPS_ERR_STATE,
+                  "the learned solver needs an assembled particle system (its features are per particle)");
     lsmps_ppe_stats ps = ctx->ppe_assembly;
     ps.iterations = 0;
     ps.converged = 0;

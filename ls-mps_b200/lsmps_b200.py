@@ -180,6 +180,7 @@ SIGNATURES = {
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
     "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_wls_fields": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "lsmps_ppe_load_csr": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, C.POINTER(PpeStats)]),
     "lsmps_projection_step": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.POINTER(SolverOpts), _vp, _vp,
                                         C.POINTER(ProjectionStats)]),
     "lsmps_series_create": (C.c_int, [_vp, C.POINTER(SeriesParams), _vp, _vp, C.c_size_t, C.POINTER(_vp)]),
@@ -411,6 +412,18 @@ class Context:
         p = np.zeros(unknowns)
         self._check(self.L.lsmps_download_pressure(self.h, _p(p), unknowns))
         return p
+
+    def ppe_load_csr(self, row_ptr, col, val=None, b=None):
+        """Install a caller's CSR system (lsmps_ppe_load_csr); returns its PpeStats."""
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = None if val is None else np.ascontiguousarray(val, dtype=np.float64)
+        b = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+        st = PpeStats()
+        self._check(self.L.lsmps_ppe_load_csr(self.h, _p(row_ptr), _p(col), _p(val), _p(b), len(row_ptr) - 1,
+                                              C.byref(st)))
+        self._last_ppe = st
+        return st
 
     def wls_fields(self, fields):
         """WLS solutions (n x k x 9) of k per-particle fields (torch CUDA tensor or array, n x k;
