@@ -7,21 +7,25 @@ Workload (one "step" = the whole per-step path on one particle set):
   l0 = 1, re = 2.1 l0, max_neighbors 128; neighbor build + 14-direction classification,
   batched WLS over every particle, WLS-Laplacian PPE over all Interior / NearWall
   particles with p* = sin(0.3x) cos(0.2y) + 0.1z and b = A p*, solved to relative residual
-  1e-10 (PPE relative L2 against p* <= 1e-8 is checked).
-  Synthetic data, seeded; matrices are larger than L2 (126 MB) so no flush is needed.
+  3e-11 (PPE relative L2 against p* <= 1e-8, checked). Steps cycle through --sets seeded
+  particle sets held on the device (a device-to-device copy into the library per step):
+  BiCGStab's stopping iteration on one system moves by +-15 % with summation order, so the
+  step time is a mean over systems. Synthetic data, seeded; matrices are larger than L2
+  (126 MB) so no flush is needed.
 
 `value` = particles x GPUs / (device step time, CUDA events on the library's stream, max
-over ranks) with the headline solver (mixed precision: FP32 Jacobi-BiCGStab inner solves,
-FP64 residual refinement). `e2e` = the same through the C ABI with host buffers: upload
-from pinned memory, the step, and the download of the pressure inside the timed region.
-The plain FP64 GPU BiCGStab (the reference iteration) is timed on the same system beside
-it. `--impl reference` times the reference's own CPU implementation of the path.
+over ranks) with the headline solver (learned + mixed precision). `e2e` = the same through
+the C ABI with host buffers: upload from pinned memory, the step, and the download of the
+pressure inside the timed region. The plain FP64 GPU BiCGStab (the reference iteration),
+Jacobi FP64 and MIXED are timed on the same systems beside it (means and per set).
+`--impl reference` times the reference's own CPU implementation of the path.
 
-Multi-GPU: replicas only (one independent particle set per rank), `scaling: weak`.
+Multi-GPU: replicas only (independent particle sets per rank), `scaling: weak`.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -52,6 +56,7 @@ def parse_args():
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--case", default="mixed")
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--sets", type=int, default=4, help="seeded particle sets the steps cycle through")
     ap.add_argument("--solver", default="learned", choices=["learned", "mixed", "jacobi", "fp64"])
     ap.add_argument("--weights", default=os.path.join(ROOT, "ls-mps_b200", "weights", "mpnn_rain200k.bin"),
                     help="network weights for the learned solver (trained by ls-mps_b200/train_mpnn.py)")
@@ -209,86 +214,123 @@ def run_mine(args, dist):
 
     dev = dist.local_rank
     torch.cuda.set_device(dev)
-    xyz, types, _ = lib.generate(None, case=args.case, particles=args.particles, l0=L0,
-                                 seed=args.seed + dist.rank)
-    n = len(types)
+    # K seeded particle sets of the workload, resident on the device; step i works on set i mod K
+    # (one system's BiCGStab iteration count moves by +-15 % with summation order, so the step
+    # time is a mean over systems)
+    K = max(1, args.sets)
+    sets = [lib.generate(None, case=args.case, particles=args.particles, l0=L0, seed=args.seed + dist.rank * K + k)
+            for k in range(K)]
+    n = len(sets[0][1])
+    dsets = [(torch.from_numpy(np.ascontiguousarray(x)).to(f"cuda:{dev}"),
+              torch.from_numpy(np.ascontiguousarray(t)).to(f"cuda:{dev}")) for x, t, _ in sets]
     ctx = lib.Context(dev)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     if args.solver == "learned":
         ctx.mpnn_load(args.weights)
-    ctx.upload(xyz, types)
+    L = lib.load()
+
+    def put(k):  # device-to-device copy of set k into the context (the inputs stay resident)
+        x, t = dsets[k]
+        torch.cuda.synchronize()
+        ctx._check(L.lsmps_upload_particles_device(ctx.h, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()),
+                                                   len(t)))
+        ctx.n = len(t)
+
     timings = []
-    for _ in range(args.warmup):
+    for i in range(max(args.warmup, K)):
+        put(i % K)
         nst, pst, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings)
     timings.clear()
 
     # ---- device-timed steps (inputs resident) ----
     clocks = ClockSampler(dev)
-    launches0 = lib.load().lsmps_launch_count()
+    launches0 = L.lsmps_launch_count()
     dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(args.steps):
+    l2s = []
+    for i in range(args.steps):
+        put(i % K)
         nst, pst, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings)
+        l2s.append(s.relative_l2_error)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
     dist.barrier()
     clk = clocks.stop()
-    launches = lib.load().lsmps_launch_count() - launches0
+    launches = L.lsmps_launch_count() - launches0
     ms_step = ev0.elapsed_time(ev1) / args.steps
     ms_step_max = dist.reduce(ms_step, "max")
     launches_total = int(dist.reduce(float(launches), "sum"))
-    rel_l2 = s.relative_l2_error
+    rel_l2 = max(l2s)
 
     # ---- end to end through the C ABI with host buffers ----
-    pin_xyz = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    pin_typ = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
-    pin_xyz[:] = xyz
-    pin_typ[:] = types
-    U = int(pst.unknowns)
-    pin_p = torch.empty(U, dtype=torch.float64, pin_memory=True).numpy()
+    pins = []
+    for x, t, _ in sets:
+        px = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        pt = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
+        px[:] = x
+        pt[:] = t
+        pins.append((px, pt))
+    U = max(int(pst.unknowns), 1)
+    pin_p = torch.empty(4 * U, dtype=torch.float64, pin_memory=True).numpy()
+    d2h = []
     dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ctx.upload(pin_xyz, pin_typ)
-        step(ctx, args.solver, args.tol, args.max_iter, [])
-        ctx.pressure_into(pin_p)
+    for i in range(args.steps):
+        px, pt = pins[i % K]
+        ctx.upload(px, pt)
+        _, pst_e, _, _ = step(ctx, args.solver, args.tol, args.max_iter, [])
+        u = int(pst_e.unknowns)
+        ctx.pressure_into(pin_p[:u])
+        d2h.append(8 * u)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     e2e_ms_max = dist.reduce(e2e_ms, "max")
 
     result = {
         "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": dist.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step_max,
+        "steps": args.steps, "warmup": max(args.warmup, K), "ms_per_step": ms_step_max,
         "value": n * dist.world / (ms_step_max * 1e-3),
         "scaling": "weak", "vs_baseline": None,
         "dtype": {"learned": "f64 vectors + f32 matrix; bf16 network", "mixed": "f64 vectors + f32 matrix"}.get(
             args.solver, "f64"),
         "data": "synthetic (seeded generator; no dataset)",
         "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}",
-                   "particles": n, "case": args.case, "l0": L0, "re": RE_RATIO * L0, "max_neighbors": MAXN,
-                   "solver": args.solver, "ppe_unknowns": U, "ppe_nnz": int(pst.nnz), "pairs": int(nst.pairs),
+                   "particles": n, "case": args.case, "particle_sets": K, "seeds": [args.seed + dist.rank * K + k
+                                                                                    for k in range(K)],
+                   "l0": L0, "re": RE_RATIO * L0, "max_neighbors": MAXN, "solver": args.solver,
+                   "ppe_unknowns": int(pst.unknowns), "ppe_nnz": int(pst.nnz), "pairs": int(nst.pairs),
                    "parallelism": f"replicas x{dist.world}", "l2_flush": "inputs larger than L2 (matrix > 126 MB)"},
         "e2e": {"value": n * dist.world / (e2e_ms_max * 1e-3), "unit": UNIT,
-                "h2d_bytes_per_step": int(pin_xyz.nbytes + pin_typ.nbytes), "d2h_bytes_per_step": int(pin_p.nbytes),
-                "ms_per_step": e2e_ms_max},
+                "h2d_bytes_per_step": int(pins[0][0].nbytes + pins[0][1].nbytes),
+                "d2h_bytes_per_step": int(sum(d2h) / len(d2h)), "ms_per_step": e2e_ms_max},
         "gpu_launches": launches_total,
         "clocks": clk,
-        "phases_ms": {k: statistics.median(t[k] for t in timings) for k in timings[0]},
+        "phases_ms": {k: statistics.mean(t[k] for t in timings) for k in timings[0]},
         "ppe": {"relative_l2_error": rel_l2, "relative_residual": s.relative_residual,
-                "iterations": s.iterations, "outer_iterations": s.outer_iterations, "converged": bool(s.converged),
-                "solve_ms": statistics.median(t["solve_ms"] for t in timings)},
+                "iterations": statistics.mean(t["iterations"] for t in timings),
+                "outer_iterations": s.outer_iterations, "converged": bool(s.converged),
+                "solve_ms": statistics.mean(t["solve_ms"] for t in timings)},
     }
 
-    # ---- the plain FP64 GPU BiCGStab (and the stages between) on the same system ----
+    # ---- the plain FP64 GPU BiCGStab (and the stages between) on the same systems ----
     if not args.no_compare:
-        cmp = {}
-        for name in ("fp64", "jacobi", "mixed") + (("learned",) if args.solver == "learned" else ()):
-            r = ctx.ppe_solve(name, args.max_iter, args.tol)
-            cmp[name] = {"solve_ms": r.solve_ms, "iterations": r.iterations, "converged": bool(r.converged),
-                         "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual}
+        names = ("fp64", "jacobi", "mixed") + (("learned",) if args.solver == "learned" else ())
+        per = {nm: [] for nm in names}
+        for k in reversed(range(K)):  # ends on set 0, whose system the CPU baseline reads
+            put(k)
+            step(ctx, args.solver, args.tol, args.max_iter, [])
+            for nm in names:
+                r = ctx.ppe_solve(nm, args.max_iter, args.tol)
+                per[nm].append({"solve_ms": r.solve_ms, "iterations": r.iterations, "converged": bool(r.converged),
+                                "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual})
+        cmp = {nm: {"solve_ms": statistics.mean(x["solve_ms"] for x in v),
+                    "iterations": statistics.mean(x["iterations"] for x in v),
+                    "converged": all(x["converged"] for x in v),
+                    "relative_l2_error": max(x["relative_l2_error"] for x in v),
+                    "per_set": list(reversed(v))} for nm, v in per.items()}
         result["ppe_compare"] = cmp
         result["speedup_vs_plain_fp64"] = cmp["fp64"]["solve_ms"] / result["ppe"]["solve_ms"]
         result["l2_target"] = {"bound": 1e-8, "met": bool(rel_l2 <= 1e-8 and all(
@@ -313,8 +355,8 @@ def run_mine(args, dist):
     # ---- CPU baseline: the reference's own code on a bounded sample (rank 0, N = 1) ----
     if dist.world == 1 and dist.rank == 0 and not args.no_cpu_baseline:
         try:
-            result["cpu_baseline"] = cpu_baseline(ctx, xyz, types, cmp["fp64"]["iterations"] if not args.no_compare
-                                                  else s.iterations, args.cpu_sample_s)
+            plain_it = cmp["fp64"]["per_set"][0]["iterations"] if not args.no_compare else s.iterations
+            result["cpu_baseline"] = cpu_baseline(ctx, sets[0][0], sets[0][1], plain_it, args.cpu_sample_s)
         except Exception as e:  # the reference build may be absent on a machine without its sources
             result["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     ctx.close()

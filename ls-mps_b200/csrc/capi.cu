@@ -148,7 +148,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->nbr_stats, &ctx->wls_status, &ctx->wls_z, &ctx->wls_wsum, &ctx->wls_x,
                                  &ctx->wf_in, &ctx->wf_x, &ctx->wf_status, &ctx->wf_z, &ctx->wf_wsum, &ctx->wf_stats,
                                  &ctx->pj_grad, &ctx->pj_gradp, &ctx->pj_div, &ctx->pj_mask, &ctx->pj_stats,
-                                 &ctx->pj_hop, &ctx->ld_ident,
+                                 &ctx->pj_hop, &ctx->ld_ident, &ctx->S_dcol, &ctx->S_rbase,
                                  &ctx->wls_stats, &ctx->wls_sample, &ctx->ref_rank, &ctx->u_of_sorted,
                                  &ctx->sorted_of_u, &ctx->ref_of_u, &ctx->u_of_ref, &ctx->A_row, &ctx->A_col,
                                  &ctx->A_val, &ctx->A_valf, &ctx->A_b, &ctx->A_xexact, &ctx->A_dinv,

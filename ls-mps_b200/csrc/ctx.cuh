@@ -98,6 +98,9 @@ struct lsmps_ctx {
     bool have_sell = false, have_sell_s = false, have_sell_f = false;
     long long sell_nslices = 0, sell_entries = 0;
     lsmps_gpu::DevBuf S_ptr, S_len, S_col, S_val, S_vals, S_valf;
+    // 16-bit column steps of the SELL copies (used when every row ascends in steps < 65536)
+    bool have_steps = false, sell_steps_enabled = true;
+    lsmps_gpu::DevBuf S_dcol, S_rbase;
 
     // ---- solver state ----
     bool have_solution = false;

@@ -239,9 +239,63 @@ __device__ __forceinline__ void ld4(const int* p, int v[4]) {
     int4 q = __ldcs(reinterpret_cast<const int4*>(p));
     v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 }
+// four 16-bit column steps (8 bytes) -> four columns continuing from c
+__device__ __forceinline__ void ld4_steps(const unsigned short* p, int& c, int out[4]) {
+    uint2 q = __ldcs(reinterpret_cast<const uint2*>(p));
+    c += (int)(q.x & 0xffffu);
+    out[0] = c;
+    c += (int)(q.x >> 16);
+    out[1] = c;
+    c += (int)(q.y & 0xffffu);
+    out[2] = c;
+    c += (int)(q.y >> 16);
+    out[3] = c;
+}
 
+// The row product with 16-bit column steps (2 bytes per entry instead of 4).
 template <class TM, class T>
+__device__ __forceinline__ double sell_row16(const Sell<TM>& A, long long s, int lane, const T* __restrict__ x) {
+    const long long base = (long long)A.sptr[s] + 4 * lane;
+    const TM* __restrict__ val = A.val + base;
+    const unsigned short* __restrict__ dc = A.dcol + base;
+    int cur = A.rbase[(s << 5) + lane];
+    const int chunks = A.slen[s] >> 2;
+    double a0 = 0, a1 = 0;
+    int c = 0;
+    for (; c + 2 <= chunks; c += 2) {
+        TM v0[4], v1[4];
+        int c0[4], c1[4];
+        ld4(val + 128 * c, v0);
+        ld4(val + 128 * (c + 1), v1);
+        ld4_steps(dc + 128 * c, cur, c0);
+        ld4_steps(dc + 128 * (c + 1), cur, c1);
+        T x0[4], x1[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            x0[j] = x[c0[j]];
+            x1[j] = x[c1[j]];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a0 += (double)v0[j] * (double)x0[j];
+            a1 += (double)v1[j] * (double)x1[j];
+        }
+    }
+    if (c < chunks) {
+        TM v0[4];
+        int c0[4];
+        ld4(val + 128 * c, v0);
+        ld4_steps(dc + 128 * c, cur, c0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a0 += (double)v0[j] * (double)x[c0[j]];
+    }
+    return a0 + a1;
+}
+
+// C16: the view's columns are 16-bit steps (a compile-time choice: one code path per kernel)
+template <bool C16, class TM, class T>
 __device__ __forceinline__ double sell_row(const Sell<TM>& A, long long s, int lane, const T* __restrict__ x) {
+    if constexpr (C16) return sell_row16(A, s, lane, x);
     const long long base = (long long)A.sptr[s] + 4 * lane;
     const TM* __restrict__ val = A.val + base;
     const int* __restrict__ col = A.col + base;
@@ -330,13 +384,13 @@ __global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__
 }
 
 // v = A p; den = (r0, v); alpha = rho / den
-template <class T, class TM = T>
+template <class T, class TM = T, bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_bcg_v(Sell<TM> A, const T* __restrict__ p, T* __restrict__ v,
                                               const T* __restrict__ r0, BcgScalars* S, Partials P) {
     if (S->done) return;
     double acc = 0;
     SELL_LOOP(A) {
-        double y = sell_row(A, s, lane, p);
+        double y = sell_row<C16>(A, s, lane, p);
         long long i = (s << 5) + lane;
         if (i < A.n) {
             T yi = (T)y;
@@ -388,13 +442,13 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
 }
 
 // t = A s; omega = (t, s) / (t, t)
-template <class T, class TM = T>
+template <class T, class TM = T, bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_bcg_t(Sell<TM> A, const T* __restrict__ sv, T* __restrict__ t,
                                               BcgScalars* S, Partials P) {
     if (S->done || S->s_conv) return;
     double ats = 0, att = 0;
     SELL_LOOP(A) {
-        double y = sell_row(A, s, lane, sv);
+        double y = sell_row<C16>(A, s, lane, sv);
         long long i = (s << 5) + lane;
         if (i < A.n) {
             T ti = (T)y;
@@ -483,7 +537,7 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
 }
 
 // Initialisation: r = b - A x (or r = b when x = 0), r0 = r, p = v = 0, |b|, rho = (r0, r).
-template <class T, class TM = T>
+template <class T, class TM = T, bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restrict__ b, const T* __restrict__ x,
                                                  int use_x, T* __restrict__ r, T* __restrict__ r0,
                                                  T* __restrict__ p, T* __restrict__ v, BcgScalars* S,
@@ -492,7 +546,7 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restr
     if (gate && *gate != want) return;  // device-driven loop: runs only when the control chose it
     double abb = 0, arr = 0;
     SELL_LOOP(A) {
-        double ax = use_x ? sell_row(A, s, lane, x) : 0.0;
+        double ax = use_x ? sell_row<C16>(A, s, lane, x) : 0.0;
         long long i = (s << 5) + lane;
         if (i < A.n) {
             T bi = b[i];
@@ -533,12 +587,13 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_init(Sell<TM> A, const T* __restr
 }
 
 // r = b - A x (FP64), |r|^2 and |b|^2 into out2 (fixed-order partials).
+template <bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_residual64(Sell<double> A, const double* __restrict__ b,
                                                    const double* __restrict__ x, double* __restrict__ r,
                                                    double* out2, Partials P, unsigned int* counter) {
     double arr = 0, abb = 0;
     SELL_LOOP(A) {
-        double ax = sell_row(A, s, lane, x);
+        double ax = sell_row<C16>(A, s, lane, x);
         long long i = (s << 5) + lane;
         if (i < A.n) {
             double ri = b[i] - ax;
@@ -591,18 +646,50 @@ __global__ void k_sell_fill(long long n, long long nslices, const int* __restric
         e0 = row[i];
         len = row[i + 1] - e0;
     }
-    const int pad_col = i < n ? (int)i : 0;
+    // the CSR row's last entry is its diagonal; it goes where it belongs in column order (the
+    // off-diagonals come ascending from the assembly), padding repeats the last column
+    int pos = 0;
+    if (len > 0)
+        while (pos < len - 1 && acol[e0 + pos] < (int)i) ++pos;
+    int last = i < n ? (int)i : 0;
     long long base = (long long)sptr[s] + 4 * lane;
     for (int k = 0; k < slen[s]; ++k) {
         long long e = base + 128LL * (k >> 2) + (k & 3);
         if (k < len) {
-            col[e] = acol[e0 + k];
-            val[e] = aval[e0 + k];
+            const int src = k < pos ? e0 + k : (k == pos ? e0 + len - 1 : e0 + k - 1);
+            last = acol[src];
+            col[e] = last;
+            val[e] = aval[src];
         } else {
-            col[e] = pad_col;
+            col[e] = last;
             val[e] = 0.0;
         }
     }
+}
+
+// 16-bit column steps of the SELL layout: per slot row, rbase = its first column and dcol[k] =
+// col[k] - col[k - 1] (0 for the first entry); a row that does not ascend or steps by more
+// than 65535 sets *bad (the 32-bit columns are used then).
+__global__ void k_sell_steps(long long nslices, const int* __restrict__ sptr, const int* __restrict__ slen,
+                             const int* __restrict__ col, unsigned short* __restrict__ dcol, int* __restrict__ rbase,
+                             int* bad) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nslices * 32) return;
+    long long s = i >> 5;
+    int lane = (int)(i & 31);
+    long long base = (long long)sptr[s] + 4 * lane;
+    int prev = col[base];
+    rbase[i] = prev;
+    bool ok = true;
+    for (int k = 0; k < slen[s]; ++k) {
+        long long e = base + 128LL * (k >> 2) + (k & 3);
+        const int c = col[e];
+        const int d = c - prev;
+        ok = ok && d >= 0 && d <= 65535;
+        dcol[e] = (unsigned short)(d >= 0 && d <= 65535 ? d : 0);
+        prev = c;
+    }
+    if (!ok) atomicOr(bad, 1);
 }
 
 // Column scaling A D^-1 (Jacobi right preconditioning folded into the matrix).
@@ -713,6 +800,7 @@ __global__ void k_start_rhs(long long n, const double* __restrict__ r64, const d
 // Residual replacement of the mixed solver (FP64 vectors, FP32 matrix in the iteration):
 // r = b - (A D^-1) y with the FP64 matrix; rho' = (r0, r) and the next beta follow, so the
 // iteration continues with its search direction (van der Vorst & Ye). |r| goes to S->rn.
+template <bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_replace_residual(Sell<double> A, const double* __restrict__ b,
                                                             const double* __restrict__ y, double* __restrict__ r,
                                                             const double* __restrict__ r0, BcgScalars* S,
@@ -720,7 +808,7 @@ __global__ void __launch_bounds__(RB, 6) k_replace_residual(Sell<double> A, cons
     if (gate && *gate != want) return;  // device-driven loop: runs only when the control chose it
     double arr = 0, ar0r = 0;
     SELL_LOOP(A) {
-        double ay = sell_row(A, s, lane, y);
+        double ay = sell_row<C16>(A, s, lane, y);
         long long i = (s << 5) + lane;
         if (i < A.n) {
             double ri = b[i] - ay;
@@ -972,20 +1060,35 @@ template <class T, class TM = T>
 void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V) {
     note_launches(5);
     k_bcg_p<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.p, V.v, E.S);
-    k_bcg_v<T, TM><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
+    if (A.dcol) k_bcg_v<T, TM, true><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
+    else k_bcg_v<T, TM, false><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
     k_bcg_s<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.v, V.s, E.S, E.P);
-    k_bcg_t<T, TM><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
+    if (A.dcol) k_bcg_t<T, TM, true><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
+    else k_bcg_t<T, TM, false><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
     k_bcg_x<T><<<RGRID, RB, 0, E.s>>>(A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P);
 }
 
 template <class T, class TM = T>
 void init(Engine& E, const Sell<TM>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
-    k_bcg_init<T, TM><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol, bnorm_override);
+    if (A.dcol)
+        k_bcg_init<T, TM, true><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol,
+                                                       bnorm_override);
+    else
+        k_bcg_init<T, TM, false><<<RGRID, RB, 0, E.s>>>(A, b, V.x, use_x, V.r, V.r0, V.p, V.v, E.S, E.P, tol,
+                                                        bnorm_override);
     LSMPS_CHECK_LAUNCH();
 }
 
+// the mixed solver's FP64 residual replacement (gated by the device-driven loop's control)
+void launch_replace(cudaStream_t s, const Sell<double>& As, const double* b, const Vecs<double>& V, Engine& E,
+                    const int* gate, int want) {
+    if (As.dcol) k_replace_residual<true><<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P, gate, want);
+    else k_replace_residual<false><<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P, gate, want);
+}
+
 void residual64(Engine& E, const Sell<double>& A, const double* b, const double* x, double* r, double* out2) {
-    k_residual64<<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, &E.S->counter[5]);
+    if (A.dcol) k_residual64<true><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, &E.S->counter[5]);
+    else k_residual64<false><<<RGRID, RB, 0, E.s>>>(A, b, x, r, out2, E.P, &E.S->counter[5]);
     LSMPS_CHECK_LAUNCH();
 }
 
@@ -1166,12 +1269,31 @@ static void sell_structure(lsmps_ctx* ctx) {
                                                              ctx->A_val.get<double>(), sptr, slen, col, val);
         LSMPS_CHECK_LAUNCH();
     }
+    // 16-bit column steps when every row ascends with steps below 65536
+    ctx->have_steps = false;
+    if (ns) {
+        unsigned short* dcol = ctx->S_dcol.ensure<unsigned short>((size_t)total + 8);
+        int* rbase = ctx->S_rbase.ensure<int>(ns * 32 + 1);
+        int* bad = ctx->scratch.get<int>() + 46;
+        LSMPS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+        k_sell_steps<<<blocks_for(ns * 32, 256), 256, 0, s>>>(ns, sptr, slen, col, dcol, rbase, bad);
+        LSMPS_CHECK_LAUNCH();
+        int hbad = 1;
+        LSMPS_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        LSMPS_CUDA(cudaStreamSynchronize(s));
+        ctx->have_steps = hbad == 0 && ctx->sell_steps_enabled;
+    }
     ctx->have_sell = true;
 }
 
 template <class T>
 static Sell<T> sell_view(lsmps_ctx* ctx, const T* val) {
-    return Sell<T>{ctx->U, ctx->sell_nslices, ctx->S_ptr.get<int>(), ctx->S_len.get<int>(), ctx->S_col.get<int>(), val};
+    Sell<T> A{ctx->U, ctx->sell_nslices, ctx->S_ptr.get<int>(), ctx->S_len.get<int>(), ctx->S_col.get<int>(), val};
+    if (ctx->have_steps) {
+        A.dcol = ctx->S_dcol.get<unsigned short>();
+        A.rbase = ctx->S_rbase.get<int>();
+    }
+    return A;
 }
 
 static Sell<double> sell_a64(lsmps_ctx* ctx) {
@@ -1469,10 +1591,14 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         cudaGraphExec_t wexec = build_while_graph(s, C, [&] {
             for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
             k_mix_after_chunk<<<1, 1, 0, s>>>(E.S, C);
-            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P, &C->act, 1);
+            launch_replace(s, As, b, V, E, &C->act, 1);
             k_mix_after_replace<<<1, 1, 0, s>>>(E.S, C);
-            k_bcg_init<double, double><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P, o->tol,
-                                                            -1.0, &C->act, 2);
+            if (As.dcol)
+                k_bcg_init<double, double, true><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P,
+                                                                      o->tol, -1.0, &C->act, 2);
+            else
+                k_bcg_init<double, double, false><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P,
+                                                                       o->tol, -1.0, &C->act, 2);
             k_mix_after_restart<<<1, 1, 0, s>>>(E.S, C);
         });
         note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
@@ -1507,14 +1633,14 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         const int why = h.done;  // 0: drop by delta; else the iteration stopped
         if (why == 3 || total >= o->max_iter) {
             // iteration cap: report the true residual of the last iterate
-            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P);
+            launch_replace(s, As, b, V, E, nullptr, 0);
             LSMPS_CHECK_LAUNCH();
             read(h);
             converged = h.done == 1;
             break;
         }
         if (why == 0) {
-            k_replace_residual<<<RGRID, RB, 0, s>>>(As, b, V.x, V.r, V.r0, E.S, E.P);
+            launch_replace(s, As, b, V, E, nullptr, 0);
             LSMPS_CHECK_LAUNCH();
             ++replacements;
             read(h);
@@ -1667,8 +1793,10 @@ void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, doubl
     if (f32) Af = sell_scaled32(ctx);
     else Ad = sell_a64(ctx);
     auto launch = [&] {
-        if (f32) k_bcg_v<double, float><<<RGRID, RB, 0, s>>>(Af, x, y, r0, E.S, E.P);
-        else k_bcg_v<double, double><<<RGRID, RB, 0, s>>>(Ad, x, y, r0, E.S, E.P);
+        if (f32 && Af.dcol) k_bcg_v<double, float, true><<<RGRID, RB, 0, s>>>(Af, x, y, r0, E.S, E.P);
+        else if (f32) k_bcg_v<double, float, false><<<RGRID, RB, 0, s>>>(Af, x, y, r0, E.S, E.P);
+        else if (Ad.dcol) k_bcg_v<double, double, true><<<RGRID, RB, 0, s>>>(Ad, x, y, r0, E.S, E.P);
+        else k_bcg_v<double, double, false><<<RGRID, RB, 0, s>>>(Ad, x, y, r0, E.S, E.P);
         LSMPS_CHECK_LAUNCH();
     };
     launch();
@@ -1679,7 +1807,8 @@ void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, doubl
     // algorithmic bytes: values + columns of the nonzeros (not the padding), the x gathers
     // counted once, y written, r0 read (FP64 vectors), slice pointers and lengths
     const double nnz = (double)ctx->nnz;
-    *bytes = (f32 ? 8.0 : 12.0) * nnz + 24.25 * U;
+    // values + columns (2 bytes as steps, plus a 4-byte first column per row) per entry
+    *bytes = ((f32 ? 4.0 : 8.0) + (ctx->have_steps ? 2.0 : 4.0)) * nnz + (ctx->have_steps ? 28.25 : 24.25) * U;
     // the bench overwrote solver vectors: a warm start from them is no longer valid
     ctx->have_solution = false;
 }

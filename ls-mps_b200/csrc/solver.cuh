@@ -26,7 +26,9 @@ struct BcgScalars {
 // A SELL-32x4 matrix view in the solver's numbering: rows in slices of 32, slice s holding
 // slen[s] (a multiple of 4) entries per row from sptr[s], in chunks of four consecutive
 // entries per row (entry k of row 32 s + l at sptr[s] + 128 (k / 4) + 4 l + k % 4),
-// zero-padded to its longest row.
+// zero-padded to its longest row. Every row's columns ascend (the diagonal in place). With
+// dcol set, the columns are stored as 16-bit steps: column k = rbase[row] + dcol[0] + ... +
+// dcol[k] (dcol of the first entry and of padding entries is 0), and col is not read.
 template <class T>
 struct Sell {
     long long n;
@@ -35,6 +37,8 @@ struct Sell {
     const int* slen;
     const int* col;
     const T* val;
+    const unsigned short* dcol = nullptr;
+    const int* rbase = nullptr;
 };
 
 }  // namespace lsmps_gpu
