@@ -72,8 +72,10 @@ enum {
     LSMPS_KB_NBR_COUNT = 2,
     LSMPS_KB_NBR_FILL = 3,
     LSMPS_KB_WLS = 4,
-    LSMPS_KB_MPNN_LAYER = 5 /* one message-passing layer (aggregation + 64x128 tensor-core GEMM) of the
+    LSMPS_KB_MPNN_LAYER = 5, /* one message-passing layer (aggregation + 64x128 tensor-core GEMM) of the
                                loaded network over the assembled PPE graph: 256 U + 8 Z */
+    LSMPS_KB_MG_VCYCLE = 6   /* one multigrid V-cycle (all its kernels) on the assembled system's
+                               hierarchy: 144 U + 464 (rows of the coarse levels) */
 };
 int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
@@ -212,6 +214,19 @@ enum {
     LSMPS_SOLVER_MIXED_F32 = 5  /* FP32 vectors and matrix, FP64 solution and residual refinement */
 };
 
+/* Right preconditioner of MIXED and LEARNED (lsmps_solver_opts.precond; the other solvers take
+ * only JACOBI). MULTIGRID: a cell-aggregation multigrid V-cycle in FP32. Level 1 has one
+ * aggregate per neighbor-grid cell; each coarser level groups 2x2x2 blocks of the level below.
+ * Coarse operators are the Galerkin products, stored as 27-slot stencils. One Jacobi sweep
+ * smooths each level; the coarsest level of at most 256 rows gets 10 sweeps. It is rebuilt
+ * after each assembly (its setup time is in solve_ms). No reference counterpart: the
+ * reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for loaded CSR systems,
+ * which have no cells. */
+enum {
+    LSMPS_PRECOND_JACOBI = 0,
+    LSMPS_PRECOND_MULTIGRID = 1
+};
+
 typedef struct lsmps_solver_opts {
     int32_t solver;          /* LSMPS_SOLVER_* */
     int32_t max_iter;        /* total BiCGStab iterations (inner ones for MIXED / LEARNED) */
@@ -228,10 +243,18 @@ typedef struct lsmps_solver_opts {
     int32_t inner_max_iter;  /* reserved */
     int32_t stall_window;    /* LEARNED: iterations without progress before fallback (20) */
     int32_t check_every;     /* iterations between host convergence checks (default 8) */
-    int32_t reserved;
+    int32_t precond;         /* LSMPS_PRECOND_* (MIXED / LEARNED; default JACOBI) */
 } lsmps_solver_opts;
 
 int lsmps_ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out);
+
+/* The multigrid hierarchy of the assembled system, built by the last multigrid solve (or by
+ * lsmps_mg_apply): the number of coarse levels, the rows of levels 0 (the unknowns) .. levels
+ * (up to `cap` entries) and its setup time. lsmps_mg_apply: out = D M z for one host vector
+ * of U values in the reference's unknown numbering (D the diagonal of A, M the V-cycle), the
+ * operator the solvers apply in their iteration on y = D x. No reference counterpart. */
+int lsmps_mg_info(lsmps_ctx* ctx, int32_t* levels, int64_t* rows, int32_t cap, double* setup_ms);
+int lsmps_mg_apply(lsmps_ctx* ctx, const double* z, double* out, size_t u);
 
 /* ---- downloads (host buffers, caller's particle / unknown order) ------------------- */
 int lsmps_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);

@@ -159,6 +159,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf};
     for (auto* b : bufs) b->release();
     mpnn_destroy(ctx);
+    mg_destroy(ctx);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -193,6 +194,8 @@ int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_laun
             wls_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
         else if (kernel == LSMPS_KB_MPNN_LAYER)
             mpnn_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
+        else if (kernel == LSMPS_KB_MG_VCYCLE)
+            mg_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
         else
             throw Error{LSMPS_ERR_ARG, "unknown kernel id"};
     });
@@ -302,6 +305,18 @@ int lsmps_ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_sta
         LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null solver options");
         ppe_solve(ctx, opts, out);
     });
+}
+
+int lsmps_mg_info(lsmps_ctx* ctx, int32_t* levels, int64_t* rows, int32_t cap, double* setup_ms) {
+    return guarded(ctx, [&] {
+        int lv = 0;
+        mg_info(ctx, &lv, rows, cap, setup_ms);
+        if (levels) *levels = lv;
+    });
+}
+
+int lsmps_mg_apply(lsmps_ctx* ctx, const double* z, double* out, size_t u) {
+    return guarded(ctx, [&] { mg_apply_host(ctx, z, out, u); });
 }
 
 int lsmps_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n) {

@@ -25,6 +25,7 @@
 
 namespace lsmps_gpu {
 struct MpnnState;
+struct MgState;
 
 // Autotuner table of one context: per "kernel n~2^k" key, the candidate launch shapes,
 // their measured ms per launch and the chosen one.
@@ -43,7 +44,7 @@ struct lsmps_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
-    cudaEvent_t ev[16] = {};
+    cudaEvent_t ev[18] = {};
     double timings[8] = {};
 
     lsmps_gpu::DevBuf dflags;      // int device error flags
@@ -110,6 +111,8 @@ struct lsmps_ctx {
 
     // ---- learned preconditioner (weights, training store, workspace) ----
     lsmps_gpu::MpnnState* mpnn = nullptr;
+    // cell-aggregation multigrid hierarchy of the assembled system (multigrid.cu)
+    lsmps_gpu::MgState* mg = nullptr;
     long long assembly_gen = 0;  // bumped by every PPE assembly
 
     lsmps_gpu::Tuner tuner;  // launch shapes chosen by the autotuner

@@ -66,11 +66,22 @@ void mpnn_load(lsmps_ctx* ctx, const char* path);
 void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
 void ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
 
+// multigrid.cu: the cell-aggregation V-cycle preconditioner (out = D M z, gated by the
+// solver scalars; need_s also skips once the |s| test has passed)
+struct BcgScalars;
+void mg_setup(lsmps_ctx* ctx);
+void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S, int need_s);
+int mg_launches_per_apply(lsmps_ctx* ctx);
+void mg_destroy(lsmps_ctx* ctx);
+void mg_info(lsmps_ctx* ctx, int* levels, int64_t* rows, int cap, double* setup_ms);
+void mg_apply_host(lsmps_ctx* ctx, const double* z, double* out, size_t n);
+
 // Profiling hooks behind lsmps_kernel_bench (mean ms per launch, algorithmic bytes).
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
 void wls_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
 void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
 void mpnn_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
+void mg_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
 
 // Timing helpers: record event `slot` on the context stream.
 // Launch-shape autotuner. For a kernel whose candidate launch shapes all compute the same

@@ -23,6 +23,7 @@
 #include <climits>
 #include <cstring>
 #include <tuple>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -373,6 +374,7 @@ __device__ __forceinline__ void vec_loop(long long n, F4&& f4, F1&& f1) {
 template <class T>
 __global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__ r, T* __restrict__ p,
                                               const T* __restrict__ v, const BcgScalars* S) {
+    pdl_begin();
     if (S->done) return;
     const T beta = (T)S->beta, omega = (T)S->omega;
     vec_loop(n, [&](long long i) {
@@ -387,6 +389,7 @@ __global__ void __launch_bounds__(RB) k_bcg_p(long long n, const T* __restrict__
 template <class T, class TM = T, bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_bcg_v(Sell<TM> A, const T* __restrict__ p, T* __restrict__ v,
                                               const T* __restrict__ r0, BcgScalars* S, Partials P) {
+    pdl_begin();
     if (S->done) return;
     double acc = 0;
     SELL_LOOP(A) {
@@ -414,6 +417,7 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_v(Sell<TM> A, const T* __restrict
 template <class T>
 __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__ r, const T* __restrict__ v,
                                               T* __restrict__ s, BcgScalars* S, Partials P) {
+    pdl_begin();
     if (S->done) return;
     const T alpha = (T)S->alpha;
     double acc = 0;
@@ -441,10 +445,12 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
     }
 }
 
-// t = A s; omega = (t, s) / (t, t)
+// t = A sv; omega = (t, s) / (t, t), with sv = s, or the preconditioned M s when a
+// preconditioner is applied (s then only enters the dot)
 template <class T, class TM = T, bool C16 = false>
 __global__ void __launch_bounds__(RB, 6) k_bcg_t(Sell<TM> A, const T* __restrict__ sv, T* __restrict__ t,
-                                              BcgScalars* S, Partials P) {
+                                              BcgScalars* S, Partials P, const T* __restrict__ sd) {
+    pdl_begin();
     if (S->done || S->s_conv) return;
     double ats = 0, att = 0;
     SELL_LOOP(A) {
@@ -453,7 +459,7 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_t(Sell<TM> A, const T* __restrict
         if (i < A.n) {
             T ti = (T)y;
             t[i] = ti;
-            ats += (double)ti * (double)sv[i];
+            ats += (double)ti * (double)sd[i];
             att += (double)ti * (double)ti;
         }
     }
@@ -471,17 +477,22 @@ __global__ void __launch_bounds__(RB, 6) k_bcg_t(Sell<TM> A, const T* __restrict
 }
 
 // x += alpha p + omega s; r = s - omega t; |r|, rho' = (r0, r); beta
-// (or, when the |s| test passed: x += alpha p and finish)
-template <class T>
+// (or, when the |s| test passed: x += alpha p and finish). PRE: the x update takes the
+// preconditioned directions ph = M p and sh = M s instead of p and s.
+template <class T, bool PRE = false>
 __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T* __restrict__ r,
                                               const T* __restrict__ p, const T* __restrict__ s,
                                               const T* __restrict__ t, const T* __restrict__ r0,
-                                              BcgScalars* S, Partials P) {
+                                              BcgScalars* S, Partials P, const T* __restrict__ ph = nullptr,
+                                              const T* __restrict__ sh = nullptr) {
+    pdl_begin();
     if (S->done) return;
     const T alpha = (T)S->alpha, omega = (T)S->omega;
+    const T* __restrict__ xp = PRE ? ph : p;
+    const T* __restrict__ xs = PRE ? sh : s;
     if (S->s_conv) {
         for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
-            x[i] += alpha * p[i];
+            x[i] += alpha * xp[i];
             r[i] = s[i];
         }
         __syncthreads();
@@ -494,10 +505,11 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
     }
     double arr = 0, ar0r = 0;
     vec_loop(n, [&](long long i) {
-        V4<T> xx = ld_v4(x + i), pp = ld_v4(p + i), ss = ld_v4(s + i), tt = ld_v4(t + i), q0 = ld_v4(r0 + i), rr;
+        V4<T> xx = ld_v4(x + i), pp = ld_v4(xp + i), ss = ld_v4(s + i), tt = ld_v4(t + i), q0 = ld_v4(r0 + i), rr;
+        V4<T> xsv = PRE ? ld_v4(xs + i) : ss;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            xx.a[j] += alpha * pp.a[j] + omega * ss.a[j];
+            xx.a[j] += alpha * pp.a[j] + omega * xsv.a[j];
             rr.a[j] = ss.a[j] - omega * tt.a[j];
             arr += (double)rr.a[j] * (double)rr.a[j];
             ar0r += (double)q0.a[j] * (double)rr.a[j];
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(RB) k_bcg_x(long long n, T* __restrict__ x, T*
         st_v4(r + i, rr);
     }, [&](long long i) {
         T si = s[i];
-        x[i] += alpha * p[i] + omega * si;
+        x[i] += alpha * xp[i] + omega * (PRE ? xs[i] : si);
         T ri = si - omega * t[i];
         r[i] = ri;
         arr += (double)ri * (double)ri;
@@ -999,6 +1011,7 @@ struct Engine {
 template <class T>
 struct Vecs {
     T *x, *r, *r0, *p, *v, *s, *t;
+    T *ph = nullptr, *sh = nullptr;  // preconditioned directions M p, M s (multigrid)
 };
 
 Engine make_engine(lsmps_ctx* ctx) {
@@ -1056,17 +1069,40 @@ cudaGraphExec_t build_while_graph(cudaStream_t s, LoopCtl* C, F&& body) {
     return exec;
 }
 
+// One BiCGStab iteration; with `mg` (FP64 vectors only) the multigrid V-cycle is the right
+// preconditioner: ph = D M p before v = A ph, sh = D M s before t = A sh.
 template <class T, class TM = T>
-void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V) {
+void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V, bool mg = false) {
     note_launches(5);
-    k_bcg_p<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.p, V.v, E.S);
-    if (A.dcol) k_bcg_v<T, TM, true><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
-    else k_bcg_v<T, TM, false><<<RGRID, RB, 0, E.s>>>(A, V.p, V.v, V.r0, E.S, E.P);
-    k_bcg_s<T><<<RGRID, RB, 0, E.s>>>(A.n, V.r, V.v, V.s, E.S, E.P);
-    if (A.dcol) k_bcg_t<T, TM, true><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
-    else k_bcg_t<T, TM, false><<<RGRID, RB, 0, E.s>>>(A, V.s, V.t, E.S, E.P);
-    k_bcg_x<T><<<RGRID, RB, 0, E.s>>>(A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P);
+    launch_pdl(k_bcg_p<T>, RGRID, RB, 0, E.s, A.n, V.r, V.p, V.v, E.S);
+    const T* pv = V.p;
+    const T* sv = V.s;
+    if constexpr (std::is_same<T, double>::value) {
+        if (mg) {
+            mg_apply(E.ctx, V.p, V.ph, E.S, 0);
+            pv = V.ph;
+        }
+    }
+    if (A.dcol) launch_pdl(k_bcg_v<T, TM, true>, RGRID, RB, 0, E.s, A, pv, V.v, V.r0, E.S, E.P);
+    else launch_pdl(k_bcg_v<T, TM, false>, RGRID, RB, 0, E.s, A, pv, V.v, V.r0, E.S, E.P);
+    launch_pdl(k_bcg_s<T>, RGRID, RB, 0, E.s, A.n, V.r, V.v, V.s, E.S, E.P);
+    if constexpr (std::is_same<T, double>::value) {
+        if (mg) {
+            mg_apply(E.ctx, V.s, V.sh, E.S, 1);
+            sv = V.sh;
+        }
+    }
+    if (A.dcol) launch_pdl(k_bcg_t<T, TM, true>, RGRID, RB, 0, E.s, A, sv, V.t, E.S, E.P, V.s);
+    else launch_pdl(k_bcg_t<T, TM, false>, RGRID, RB, 0, E.s, A, sv, V.t, E.S, E.P, V.s);
+    if (mg)
+        launch_pdl(k_bcg_x<T, true>, RGRID, RB, 0, E.s, A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P, V.ph, V.sh);
+    else
+        launch_pdl(k_bcg_x<T, false>, RGRID, RB, 0, E.s, A.n, V.x, V.r, V.p, V.s, V.t, V.r0, E.S, E.P,
+                   (const T*)nullptr, (const T*)nullptr);
 }
+
+// kernel launches of one iteration
+int launches_per_iteration(lsmps_ctx* ctx, bool mg) { return 5 + (mg ? 2 * mg_launches_per_apply(ctx) : 0); }
 
 template <class T, class TM = T>
 void init(Engine& E, const Sell<TM>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
@@ -1301,6 +1337,8 @@ static Sell<double> sell_a64(lsmps_ctx* ctx) {
     return sell_view<double>(ctx, ctx->S_val.get<double>());
 }
 
+Sell<double> sell_a64_view(lsmps_ctx* ctx) { return sell_a64(ctx); }
+
 static Sell<double> sell_scaled64(lsmps_ctx* ctx) {
     sell_structure(ctx);
     if (!ctx->have_sell_s) {
@@ -1503,6 +1541,13 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     const int chunk = std::max(1, o->check_every > 0 ? o->check_every : 8);
     const int stall = o->stall_window > 0 ? o->stall_window : 20;
     ev_record(ctx, 10);
+    const bool mg = o->precond == LSMPS_PRECOND_MULTIGRID;
+    if (mg) {
+        mg_setup(ctx);
+        V.ph = ctx->vph.ensure<double>(U + 1);
+        V.sh = ctx->vsh.ensure<double>(U + 1);
+    }
+    const uint64_t kpi = (uint64_t)launches_per_iteration(ctx, mg);
     Sell<double> As = sell_scaled64(ctx);
     Sell<float> Af = sell_scaled32(ctx);
     set_scalar_caps(E, o->max_iter, use_nn ? stall : 0);
@@ -1545,8 +1590,8 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     if (o->use_graph == 2) {
         cudaGraph_t graph;
         LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
-        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mg);
+        note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         LSMPS_CUDA(e);
         LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -1589,7 +1634,7 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         c0.use_nn = use_nn ? 1 : 0;
         LSMPS_CUDA(cudaMemcpyAsync(C, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
         cudaGraphExec_t wexec = build_while_graph(s, C, [&] {
-            for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V);
+            for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mg);
             k_mix_after_chunk<<<1, 1, 0, s>>>(E.S, C);
             launch_replace(s, As, b, V, E, &C->act, 1);
             k_mix_after_replace<<<1, 1, 0, s>>>(E.S, C);
@@ -1601,14 +1646,14 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
                                                                        o->tol, -1.0, &C->act, 2);
             k_mix_after_restart<<<1, 1, 0, s>>>(E.S, C);
         });
-        note_launches(0 - (uint64_t)(5 * chunk));  // captured, not launched
+        note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
         cudaError_t e = cudaGraphLaunch(wexec, s);
         LoopCtl hc{};
         if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, C, sizeof(hc), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         cudaGraphExecDestroy(wexec);
         LSMPS_CUDA(e);
-        note_launches((uint64_t)hc.trips * (5 * (uint64_t)chunk + 6));
+        note_launches((uint64_t)hc.trips * (kpi * (uint64_t)chunk + 6));
         total = hc.total;
         replacements = hc.replacements;
         restarts = hc.restarts;
@@ -1620,9 +1665,9 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         if (!h.done) {
             if (exec) {
                 LSMPS_CUDA(cudaGraphLaunch(exec, s));
-                note_launches(5 * (uint64_t)chunk);
+                note_launches(kpi * (uint64_t)chunk);
             } else {
-                for (int k = 0; k < chunk; ++k) iteration<double, float>(E, Af, V);
+                for (int k = 0; k < chunk; ++k) iteration<double, float>(E, Af, V, mg);
                 LSMPS_CHECK_LAUNCH();
             }
             read(h);
@@ -1723,6 +1768,12 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
                   "learned solver needs lsmps_mpnn_init / lsmps_mpnn_load first");
     LSMPS_REQUIRE(o->solver != LSMPS_SOLVER_LEARNED || !ctx->ppe_loaded, LSMPS_ERR_STATE,
                   "the learned solver needs an assembled particle system (its features are per particle)");
+    LSMPS_REQUIRE(o->precond == LSMPS_PRECOND_JACOBI ||
+                      (o->precond == LSMPS_PRECOND_MULTIGRID &&
+                       (o->solver == LSMPS_SOLVER_MIXED || o->solver == LSMPS_SOLVER_LEARNED)),
+                  LSMPS_ERR_ARG, "the multigrid preconditioner is for the MIXED and LEARNED solvers");
+    LSMPS_REQUIRE(o->precond != LSMPS_PRECOND_MULTIGRID || !ctx->ppe_loaded, LSMPS_ERR_STATE,
+                  "the multigrid preconditioner aggregates particle cells: a loaded CSR system has none");
     lsmps_ppe_stats ps = ctx->ppe_assembly;
     ps.iterations = 0;
     ps.converged = 0;

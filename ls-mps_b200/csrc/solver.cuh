@@ -41,4 +41,7 @@ struct Sell {
     const int* rbase = nullptr;
 };
 
+// The assembled system's SELL copy with FP64 values of A (built on first use).
+Sell<double> sell_a64_view(lsmps_ctx* ctx);
+
 }  // namespace lsmps_gpu

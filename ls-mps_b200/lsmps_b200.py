@@ -23,7 +23,8 @@ INTERIOR, FREE_SURFACE, SPLASH, NEAR_WALL, WALL = range(5)
 NBR_CLASSIFY = 1
 PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
 SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED, SOLVER_MIXED_F32 = range(6)
-KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER = range(6)
+KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER, KB_MG_VCYCLE = range(7)
+PRECONDS = {"jacobi": 0, "multigrid": 1}
 SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4, "mixed_f32": 5}
 VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}
 
@@ -137,7 +138,7 @@ class SolverOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("max_iter", C.c_int32), ("tol", C.c_double),
                 ("warm_start", C.c_int32), ("use_graph", C.c_int32), ("inner_tol", C.c_double),
                 ("inner_max_iter", C.c_int32), ("stall_window", C.c_int32), ("check_every", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("precond", C.c_int32)]
 
 
 class MpnnTrainOpts(C.Structure):
@@ -181,6 +182,8 @@ SIGNATURES = {
     "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
     "lsmps_wls_fields": (C.c_int, [_vp, _vp, C.c_int, _vp]),
     "lsmps_ppe_load_csr": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, C.POINTER(PpeStats)]),
+    "lsmps_mg_info": (C.c_int, [_vp, C.POINTER(C.c_int32), _vp, C.c_int32, C.POINTER(C.c_double)]),
+    "lsmps_mg_apply": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
     "lsmps_projection_step": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.POINTER(SolverOpts), _vp, _vp,
                                         C.POINTER(ProjectionStats)]),
     "lsmps_series_create": (C.c_int, [_vp, C.POINTER(SeriesParams), _vp, _vp, C.c_size_t, C.POINTER(_vp)]),
@@ -375,14 +378,28 @@ class Context:
         return st
 
     def ppe_solve(self, solver, max_iter, tol, warm_start=False, use_graph=True, inner_tol=0.0,
-                  inner_max_iter=0, stall_window=0, check_every=0):
+                  inner_max_iter=0, stall_window=0, check_every=0, precond="jacobi"):
         o = SolverOpts(solver=SOLVERS.get(solver, solver), max_iter=int(max_iter), tol=tol,
                        warm_start=1 if warm_start else 0, use_graph=int(use_graph),
                        inner_tol=inner_tol, inner_max_iter=inner_max_iter, stall_window=stall_window,
-                       check_every=check_every)
+                       check_every=check_every, precond=PRECONDS.get(precond, precond))
         st = PpeStats()
         self._check(self.L.lsmps_ppe_solve(self.h, C.byref(o), C.byref(st)))
         return st
+
+    def mg_info(self):
+        """Multigrid hierarchy of the assembled system: rows per level (0 = unknowns) and setup ms."""
+        lv = C.c_int32(0); ms = C.c_double(0)
+        rows = np.zeros(64, np.int64)
+        self._check(self.L.lsmps_mg_info(self.h, C.byref(lv), _p(rows), 64, C.byref(ms)))
+        return rows[: lv.value + 1].copy(), ms.value
+
+    def mg_apply(self, z):
+        """D M z: the multigrid V-cycle as the solvers apply it (reference unknown numbering)."""
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        out = np.zeros_like(z)
+        self._check(self.L.lsmps_mg_apply(self.h, _p(z), _p(out), len(z)))
+        return out
 
     def types(self):
         t = np.zeros(self.n, np.uint8)

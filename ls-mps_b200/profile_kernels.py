@@ -6,7 +6,7 @@ Builds the workload of bench.py (case `mixed`, l0 = 1, re = 2.1, max_neighbors 1
 WLS-Laplacian PPE) with the library, then launches the chosen kernel `reps` times through
 lsmps_kernel_bench and prints its mean time and achieved bandwidth. Under ncu, select the
 kernel with -k (spmv32/spmv64: k_bcg_v, nbr_count: k_seg_pass<0>, nbr_fill: k_seg_pass<1>,
-wls: k_wls_all, mpnn_layer: k_layer_fwd). mpnn_layer loads --weights. --autotune prints the
+wls: k_wls_all, mpnn_layer: k_layer_fwd, mg_vcycle: regex k_mg_). mpnn_layer loads --weights. --autotune prints the
 launch shapes the autotuner timed and chose.
 """
 import argparse
@@ -17,7 +17,8 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import lsmps_b200 as lib  # noqa: E402
 
 KERNELS = {"spmv32": lib.KB_SPMV32, "spmv64": lib.KB_SPMV64, "nbr_count": lib.KB_NBR_COUNT,
-           "nbr_fill": lib.KB_NBR_FILL, "wls": lib.KB_WLS, "mpnn_layer": lib.KB_MPNN_LAYER}
+           "nbr_fill": lib.KB_NBR_FILL, "wls": lib.KB_WLS, "mpnn_layer": lib.KB_MPNN_LAYER,
+           "mg_vcycle": lib.KB_MG_VCYCLE}
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "mpnn_rain200k.bin")
 
 
@@ -29,6 +30,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--solve", choices=["fp64", "jacobi", "mixed", "learned"], default=None,
                     help="also run one PPE solve to relative residual 1e-10")
+    ap.add_argument("--precond", choices=["jacobi", "multigrid"], default="jacobi")
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--autotune", type=int, default=1, help="0 off (default shapes), 1 on")
     a = ap.parse_args()
@@ -46,7 +48,7 @@ def main():
             ms, nb = ctx.kernel_bench(KERNELS[k], a.reps)
             print(f"{k}: {ms * 1e3:.1f} us per launch, {nb / 1e6:.1f} MB algorithmic, {nb / ms / 1e6:.0f} GB/s")
         if a.solve:
-            s = ctx.ppe_solve(a.solve, 20000, 1e-10)
+            s = ctx.ppe_solve(a.solve, 20000, 1e-10, precond=a.precond)
             print(f"solve {a.solve}: {s.solve_ms:.2f} ms, {s.iterations} iterations, {s.outer_iterations} sweeps, "
                   f"relative L2 {s.relative_l2_error:.2e}")
         for key, shape, ms, best in ctx.autotune_report():
