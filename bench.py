@@ -14,10 +14,12 @@ Workload (one "step" = the whole per-step path on one particle set):
   (126 MB) so no flush is needed.
 
 `value` = particles x GPUs / (device step time, CUDA events on the library's stream, max
-over ranks) with the headline solver (learned + mixed precision). `e2e` = the same through
-the C ABI with host buffers: upload from pinned memory, the step, and the download of the
-pressure inside the timed region. The plain FP64 GPU BiCGStab (the reference iteration),
-Jacobi FP64 and MIXED are timed on the same systems beside it (means and per set).
+over ranks) with the headline solver (--solver, default `multigrid`: mixed-precision
+BiCGStab with the cell-aggregation multigrid V-cycle as preconditioner). `e2e` = the same
+through the C ABI with host buffers: upload from pinned memory, the step, and the download of
+the pressure inside the timed region. The plain FP64 GPU BiCGStab (the reference iteration),
+Jacobi FP64, MIXED, LEARNED and both with the multigrid preconditioner are timed on the same
+systems beside it (means and per set).
 `--impl reference` times the reference's own CPU implementation of the path.
 
 Multi-GPU: replicas only (independent particle sets per rank), `scaling: weak`.
@@ -45,19 +47,27 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 METRIC = "PPE solve ms & particle-steps/s at 1M, learned+mixed vs plain FP64 @ L2<=1e-8"
 UNIT = "particle-steps/s"
 L0, RE_RATIO, MAXN = 1.0, 2.1, 128
+# bench solver name -> (library solver, preconditioner)
+SOLVER_SPECS = {"fp64": ("fp64", "jacobi"), "jacobi": ("jacobi", "jacobi"), "mixed": ("mixed", "jacobi"),
+                "learned": ("learned", "jacobi"), "multigrid": ("mixed", "multigrid"),
+                "learned_multigrid": ("learned", "multigrid")}
+DTYPES = {"fp64": "f64", "jacobi": "f64", "mixed": "f64 vectors + f32 matrix",
+          "learned": "f64 vectors + f32 matrix; bf16 network",
+          "multigrid": "f64 vectors + f32 matrix; f32 V-cycle, f16 fine A*P",
+          "learned_multigrid": "f64 vectors + f32 matrix; f32 V-cycle, f16 fine A*P; bf16 network"}
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--case", default="mixed")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--sets", type=int, default=4, help="seeded particle sets the steps cycle through")
-    ap.add_argument("--solver", default="learned", choices=["learned", "mixed", "jacobi", "fp64"])
+    ap.add_argument("--solver", default="multigrid", choices=sorted(SOLVER_SPECS))
     ap.add_argument("--weights", default=os.path.join(ROOT, "ls-mps_b200", "weights", "mpnn_rain200k.bin"),
                     help="network weights for the learned solver (trained by ls-mps_b200/train_mpnn.py)")
     ap.add_argument("--tol", type=float, default=3e-11,
@@ -200,7 +210,8 @@ def step(ctx, solver, tol, max_iter, timings):
     nst = ctx.build_neighbors(re, MAXN, L0)
     ctx.wls(re, L0, mode=1)
     pst = ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
-    s = ctx.ppe_solve(solver, max_iter, tol)
+    sv, pc = SOLVER_SPECS[solver]
+    s = ctx.ppe_solve(sv, max_iter, tol, precond=pc)
     t = ctx.timings()
     timings.append({"neighbor_ms": t[1], "wls_ms": t[3], "assembly_ms": t[4], "solve_ms": s.solve_ms,
                     "iterations": s.iterations, "outer": s.outer_iterations})
@@ -225,7 +236,8 @@ def run_mine(args, dist):
               torch.from_numpy(np.ascontiguousarray(t)).to(f"cuda:{dev}")) for x, t, _ in sets]
     ctx = lib.Context(dev)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
-    if args.solver == "learned":
+    compare = () if args.no_compare else tuple(SOLVER_SPECS)
+    if "learned" in args.solver or any("learned" in c for c in compare):
         ctx.mpnn_load(args.weights)
     L = lib.load()
 
@@ -294,8 +306,7 @@ def run_mine(args, dist):
         "steps": args.steps, "warmup": max(args.warmup, K), "ms_per_step": ms_step_max,
         "value": n * dist.world / (ms_step_max * 1e-3),
         "scaling": "weak", "vs_baseline": None,
-        "dtype": {"learned": "f64 vectors + f32 matrix; bf16 network", "mixed": "f64 vectors + f32 matrix"}.get(
-            args.solver, "f64"),
+        "dtype": DTYPES[args.solver],
         "data": "synthetic (seeded generator; no dataset)",
         "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}",
                    "particles": n, "case": args.case, "particle_sets": K, "seeds": [args.seed + dist.rank * K + k
@@ -317,13 +328,21 @@ def run_mine(args, dist):
 
     # ---- the plain FP64 GPU BiCGStab (and the stages between) on the same systems ----
     if not args.no_compare:
-        names = ("fp64", "jacobi", "mixed") + (("learned",) if args.solver == "learned" else ())
+        names = compare
         per = {nm: [] for nm in names}
+        re = RE_RATIO * L0
+        for nm in names:  # first solves: launch-shape autotuning, graph and buffer set-up
+            sv, pc = SOLVER_SPECS[nm]
+            ctx.ppe_solve(sv, args.max_iter, args.tol, precond=pc)
         for k in reversed(range(K)):  # ends on set 0, whose system the CPU baseline reads
             put(k)
             step(ctx, args.solver, args.tol, args.max_iter, [])
             for nm in names:
-                r = ctx.ppe_solve(nm, args.max_iter, args.tol)
+                # a fresh assembly before each solve, so each solver pays its own set-up (SELL
+                # copies, multigrid hierarchy, network graph) as in a step
+                ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
+                sv, pc = SOLVER_SPECS[nm]
+                r = ctx.ppe_solve(sv, args.max_iter, args.tol, precond=pc)
                 per[nm].append({"solve_ms": r.solve_ms, "iterations": r.iterations, "converged": bool(r.converged),
                                 "relative_l2_error": r.relative_l2_error, "relative_residual": r.relative_residual})
         cmp = {nm: {"solve_ms": statistics.mean(x["solve_ms"] for x in v),
@@ -341,11 +360,12 @@ def run_mine(args, dist):
     kern = {}
     for name, kid in (("spmv32", lib.KB_SPMV32), ("spmv64", lib.KB_SPMV64), ("nbr_count", lib.KB_NBR_COUNT),
                       ("nbr_fill", lib.KB_NBR_FILL), ("wls", lib.KB_WLS)) + (
-                          (("mpnn_layer", lib.KB_MPNN_LAYER),) if args.solver == "learned" else ()):
+                          (("mpnn_layer", lib.KB_MPNN_LAYER),) if "learned" in args.solver else ()) + (
+                          (("mg_vcycle", lib.KB_MG_VCYCLE),) if "multigrid" in args.solver else ()):
         ms, nbytes = ctx.kernel_bench(kid, 20)
         gbs = nbytes / (ms * 1e-3) / 1e9
         kern[name] = {"ms": ms, "alg_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
-    dom = "spmv32" if args.solver in ("mixed", "learned") else "spmv64"
+    dom = "spmv64" if args.solver in ("fp64", "jacobi") else "spmv32"
     # the mixed solver's SpMV: FP32 values of A D^-1, FP64 vectors
     traffic = committed_traffic().get(dom)
     result["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"], "peak": peak,

@@ -371,6 +371,8 @@ typedef struct lsmps_series_params {
     int32_t wls_precision;        /* 0 FP64, 1 FP32 + FP64 refinement */
     int32_t warm_start;           /* 1: start each solve from the previous pressure */
     uint32_t seed;                /* injection positions */
+    int32_t precond;              /* LSMPS_PRECOND_* for the MIXED and LEARNED solvers */
+    int32_t reserved;
 } lsmps_series_params;
 
 typedef struct lsmps_series_stats {

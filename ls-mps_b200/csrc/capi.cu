@@ -362,7 +362,7 @@ int lsmps_download_pressure_particles_device(lsmps_ctx* ctx, double* d_p, size_t
     return guarded(ctx, [&] { ppe_pressure_particles(ctx, d_p, n, fill, true); });
 }
 
-static_assert(sizeof(lsmps_series_params) == 128, "lsmps_series_params layout");
+static_assert(sizeof(lsmps_series_params) == 136, "lsmps_series_params layout");
 static_assert(sizeof(lsmps_series_stats) == 184, "lsmps_series_stats layout");
 
 int lsmps_series_create(lsmps_ctx* ctx, const lsmps_series_params* params, const double* xyz, const uint8_t* type,

@@ -194,6 +194,10 @@ void series_create(lsmps_ctx* ctx, const lsmps_series_params* pp, const double* 
                   LSMPS_ERR_ARG, "series parameters: l0, re > 0, skin >= 0, interval >= 1, injection >= 0");
     LSMPS_REQUIRE(p.solver >= LSMPS_SOLVER_FP64 && p.solver <= LSMPS_SOLVER_MIXED_F32, LSMPS_ERR_ARG,
                   "series solver must be one of the GPU solvers");
+    LSMPS_REQUIRE(p.precond == LSMPS_PRECOND_JACOBI ||
+                      (p.precond == LSMPS_PRECOND_MULTIGRID &&
+                       (p.solver == LSMPS_SOLVER_MIXED || p.solver == LSMPS_SOLVER_LEARNED)),
+                  LSMPS_ERR_ARG, "the multigrid preconditioner is for the MIXED and LEARNED solvers");
     LSMPS_REQUIRE(p.droplet_radius >= 0 && p.inject_hmax >= p.inject_hmin, LSMPS_ERR_ARG, "injection band");
     LSMPS_REQUIRE(p.max_candidates >= p.max_neighbors && p.max_neighbors >= 0, LSMPS_ERR_ARG,
                   "max_candidates must be at least max_neighbors");
@@ -482,6 +486,7 @@ void series_step(lsmps_series* Sp, lsmps_series_stats* out) {
     if (warm) ppe_set_initial_particles(ctx, S.pres.get<double>(), S.n, true);
     lsmps_solver_opts so{};
     so.solver = p.solver;
+    so.precond = p.precond;
     so.max_iter = p.max_iter;
     so.tol = p.tol;
     so.warm_start = warm ? 1 : 0;

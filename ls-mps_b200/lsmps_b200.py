@@ -79,7 +79,7 @@ class SeriesParams(C.Structure):
                 ("film_thickness", C.c_double), ("droplet_radius", C.c_double), ("inject_hmin", C.c_double),
                 ("inject_hmax", C.c_double), ("tol", C.c_double), ("max_iter", C.c_int32),
                 ("max_neighbors", C.c_int32), ("max_candidates", C.c_int32), ("wls_precision", C.c_int32),
-                ("warm_start", C.c_int32), ("seed", C.c_uint32)]
+                ("warm_start", C.c_int32), ("seed", C.c_uint32), ("precond", C.c_int32), ("reserved", C.c_int32)]
 
 
 class SeriesStats(C.Structure):
@@ -121,7 +121,8 @@ RAIN_SECTIONS = [("mid_section", 0.55, 5.0), ("outlet_section", 0.9, 5.0)]
 SERIES_DEFAULTS = dict(steps=200, injected_per_step=2000, cnl_rebuild_interval=10, solver="learned", l0=1.0, re=2.1,
                        skin=1.0, droplet_speed=0.05, film_speed=0.02, theta_deg=20.0, film_thickness=4.0,
                        droplet_radius=3.0, inject_hmin=10.0, inject_hmax=40.0, tol=3e-11, max_iter=20000,
-                       max_neighbors=128, max_candidates=512, wls_precision=0, warm_start=1, seed=23)
+                       max_neighbors=128, max_candidates=512, wls_precision=0, warm_start=1, seed=23,
+                       precond="jacobi")
 
 
 class PpeStats(C.Structure):
@@ -559,7 +560,8 @@ def struct_dict(s):
 
 class Series:
     """A rain-on-plate step series on a context (lsmps_series_*). Keyword arguments override
-    SERIES_DEFAULTS; `solver` is a name of SOLVERS. wls_precision defaults to FP64 for every
+    SERIES_DEFAULTS; `solver` is a name of SOLVERS, `precond` one of PRECONDS. wls_precision
+    defaults to FP64 for every
     solver: on B200 the FP32 factorisation with FP64 refinement measured 2x slower than the
     FP64 solve (5.5 vs 2.8 ms per step at 3M particles); None picks mixed for the mixed and
     learned solvers."""
@@ -571,6 +573,7 @@ class Series:
         if p["wls_precision"] is None:
             p["wls_precision"] = 1 if solver in (SOLVERS["mixed"], SOLVERS["learned"], SOLVERS["mixed_f32"]) else 0
         p["solver"] = solver
+        p["precond"] = PRECONDS.get(p["precond"], p["precond"])
         self.params = SeriesParams(**p)
         self.ctx = ctx
         self.h = None

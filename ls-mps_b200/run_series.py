@@ -4,8 +4,8 @@
     python ls-mps_b200/run_series.py --cfg config/industrial_3m_template.cfg --steps 200
 
 Initial particles: the rain_plate generator (20 deg plate, 3 wall layers, 4-layer film with
-70 % of the fluid, droplets of radius 3 l0 at 10-40 l0). Each solver (default: the learned
-preconditioner with mixed precision, then plain FP64) runs the same series from the same
+70 % of the fluid, droplets of radius 3 l0 at 10-40 l0). Each solver (default: mixed precision
+with the multigrid preconditioner, the learned solver, then plain FP64) runs the same series from the same
 particles and injection seed, so every step has the same particles for every solver. Per
 step: neighbor lists (candidate rebuild every --interval steps, refresh in between), WLS,
 WLS-Laplacian PPE with the manufactured p* = sin(0.3x) cos(0.2y) + 0.1z, solve warm-started
@@ -84,8 +84,9 @@ def write_csv(path, rows):
 
 def run(ctx, xyz, t, solver, a, rain=None):
     rows = []
-    kw = dict(steps=a.steps, injected_per_step=a.injected, cnl_rebuild_interval=a.interval, solver=solver,
-              re=a.re, skin=a.skin, tol=a.tol, seed=a.seed)
+    name, _, pc = solver.partition("+")  # e.g. mixed+multigrid: the MIXED solver, multigrid preconditioner
+    kw = dict(steps=a.steps, injected_per_step=a.injected, cnl_rebuild_interval=a.interval, solver=name,
+              precond=pc or "jacobi", re=a.re, skin=a.skin, tol=a.tol, seed=a.seed)
     with lib.Series(ctx, xyz, t, **kw) as s:
         for _ in range(a.steps):
             st = s.step().as_dict()
@@ -141,7 +142,8 @@ def main():
     ap.add_argument("--re", type=float, default=None, help="support radius in l0 (re_ratio)")
     ap.add_argument("--skin", type=float, default=1.0)
     ap.add_argument("--tol", type=float, default=3e-11)
-    ap.add_argument("--solvers", default="learned,fp64")
+    ap.add_argument("--solvers", default="mixed+multigrid,learned,fp64",
+                    help="comma list of solver names, optionally +multigrid (the preconditioner)")
     ap.add_argument("--weights", default=lib.DEFAULT_WEIGHTS)
     ap.add_argument("--out", default="results/series")
     ap.add_argument("--verbose", action="store_true")
@@ -161,7 +163,7 @@ def main():
                                                      "skin", "tol", "solvers")}, "solvers": {}}
     with lib.Context(0) as ctx:
         for k, solver in enumerate(a.solvers.split(",")):
-            if solver == "learned":
+            if solver.startswith("learned"):
                 ctx.mpnn_load(a.weights)
             rain = [] if k == 0 else None
             rows = run(ctx, xyz, t, solver, a, rain)

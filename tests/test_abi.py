@@ -36,7 +36,7 @@ def test_abi_version_and_struct_sizes(built):
     assert C.sizeof(lib.NeighborStats) == 8 + 8 + 8 + 16 + 40 + 8 + 8
     assert C.sizeof(lib.PpeStats) == 5 * 8 + 8 + 6 * 8 + 8 + 8
     assert C.sizeof(lib.SolverOpts) == 4 + 4 + 8 + 4 + 4 + 8 + 4 + 4 + 4 + 4
-    assert C.sizeof(lib.SeriesParams) == 4 * 4 + 11 * 8 + 6 * 4
+    assert C.sizeof(lib.SeriesParams) == 4 * 4 + 11 * 8 + 8 * 4
     assert C.sizeof(lib.SeriesStats) == 4 * 4 + 10 * 8 + 4 * 4 + 9 * 8
 
 

@@ -8,7 +8,7 @@
 * Series: the device fluid count matches initial + injected - deleted at every step (mass
   balance 0); candidate rebuilds at step 1 and every interval steps; every PPE reaches
   relative L2 <= 1e-8 against p*; the warm start needs fewer iterations than the cold first
-  solve; the learned and plain FP64 series see the same particles.
+  solve; the learned, plain FP64 and multigrid-preconditioned series see the same particles.
 * Rain validation outputs: the reference's four tables (python/validate_outputs.py columns
   and checks restated: particle identity, coverage in [0, 1], p90 <= max, cumulative flow
   non-decreasing, mass error within the config's 1 %), and the window statistics of the last
@@ -96,14 +96,15 @@ def series_runs(built, plate):
     out = {}
     with lib.Context(0) as ctx:
         ctx.mpnn_load(lib.DEFAULT_WEIGHTS)
-        for solver in ("learned", "fp64"):
-            with lib.Series(ctx, xyz, t, solver=solver, **SMALL) as s:
+        for key, solver, pc in (("learned", "learned", "jacobi"), ("fp64", "fp64", "jacobi"),
+                                ("multigrid", "mixed", "multigrid")):
+            with lib.Series(ctx, xyz, t, solver=solver, precond=pc, **SMALL) as s:
                 rows, rain = [], []
                 for _ in range(SMALL["steps"]):
                     rows.append(s.step())
                     rain.append(s.rain_outputs())
-                out[solver] = (rows, s.particles())
-                out[solver + "_rain"] = rain
+                out[key] = (rows, s.particles())
+                out[key + "_rain"] = rain
     return out
 
 
@@ -122,7 +123,7 @@ def test_series_mass_balance_and_cadence(series_runs):
 
 
 def test_series_accuracy_and_warm_start(series_runs):
-    for solver in ("learned", "fp64"):
+    for solver in ("learned", "fp64", "multigrid"):
         rows, _ = series_runs[solver]
         for r in rows:
             assert r.converged, (solver, r.step)
@@ -136,6 +137,11 @@ def test_series_same_particles_for_both_solvers(series_runs):
     assert [r.particles for r in ra] == [r.particles for r in rb]
     assert [r.unknowns for r in ra] == [r.unknowns for r in rb]
     assert np.array_equal(xa, xb) and np.array_equal(ma, mb)
+    rm, (xm, mm, _) = series_runs["multigrid"]
+    assert [r.unknowns for r in rm] == [r.unknowns for r in rb]
+    assert np.array_equal(xm, xb) and np.array_equal(mm, mb)
+    # the preconditioner cuts the iterations of every step
+    assert sum(r.iterations for r in rm) * 3 < sum(r.iterations for r in rb)
 
 
 REQUIRED = {
