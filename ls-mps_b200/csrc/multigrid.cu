@@ -147,60 +147,53 @@ __global__ void k_mg_nbr(long long n, const int3* __restrict__ coord, int gx, in
 
 // AP[i][t]: row i's entries summed per neighbor aggregate, in FP32 slice-major (for level 1)
 // and as AP / a_ii in FP16 row-major, MG_APH_STRIDE halves per row (for the V-cycle). One warp
-// per SELL slice of the FP64 matrix, one lane per row, four entries per load (coalesced). In
-// a SELL row the columns ascend, and with cell-sorted numbering so do the entries' cells, so
-// the slots arrive in nondecreasing order: each lane sums a run and writes it when the slot
-// changes, writing 0 to the slots it skips. An entry out of that order is added to its stored
-// slot. Each row's sums are in entry order, so AP is deterministic.
+// per SELL slice of the FP64 matrix, one lane per row, four entries per load (coalesced). Each
+// lane adds its entries, in entry order, into its own column of a shared-memory table of 27
+// slots; the table is then written out with coalesced stores. AP is deterministic.
 constexpr int MG_APH_STRIDE = 28;  // 27 slots + 1 zero pad: 56 B rows, read as seven 8-byte loads
-__global__ void k_mg_fine_ap(Sell<double> A, const unsigned* __restrict__ upack, Pack pk,
-                             const double* __restrict__ dinv, float* __restrict__ ap, __half* __restrict__ aph) {
-    const long long sl = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+constexpr int AP_WARPS = 4;
+__global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<double> A, const unsigned* __restrict__ upack,
+                                                              Pack pk, const double* __restrict__ dinv,
+                                                              float* __restrict__ ap, __half* __restrict__ aph) {
+    __shared__ float acc[AP_WARPS][MG_APH_STRIDE][33];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long sl = blockIdx.x * (long long)AP_WARPS + w;
     if (sl >= A.nslices) return;  // whole warp
-    const int lane = threadIdx.x & 31;
     const long long i = (sl << 5) + lane;
-    if (i >= A.n) return;
-    const int3 ci = unpack(upack[i], pk);
-    const double di = dinv[i];
-    __half* hrow = aph + i * MG_APH_STRIDE;
+    const bool live = i < A.n;
+#pragma unroll
+    for (int t = 0; t < MG_APH_STRIDE; ++t) acc[w][t][lane] = 0.0f;
+    const int3 ci = unpack(live ? upack[i] : 0u, pk);
     const long long base = (long long)A.sptr[sl] + 4 * lane;
     const int chunks = A.slen[sl] >> 2;
-    int cur = 0;  // next slot to write
-    int open = -1;
-    float acc = 0.0f;
-    auto put = [&](int t, float a) {
-        ap[slot_index(i, t)] = a;
-        hrow[t] = __float2half_rn((float)((double)a * di));
-    };
     for (int c = 0; c < chunks; ++c) {
-        const double2 v01 = *reinterpret_cast<const double2*>(A.val + base + 128 * c);
-        const double2 v23 = *reinterpret_cast<const double2*>(A.val + base + 128 * c + 2);
-        const int4 cc = *reinterpret_cast<const int4*>(A.col + base + 128 * c);
+        const double2 v01 = __ldcs(reinterpret_cast<const double2*>(A.val + base + 128 * c));
+        const double2 v23 = __ldcs(reinterpret_cast<const double2*>(A.val + base + 128 * c + 2));
+        const int4 cc = __ldcs(reinterpret_cast<const int4*>(A.col + base + 128 * c));
         const double v[4] = {v01.x, v01.y, v23.x, v23.y};
         const int col[4] = {cc.x, cc.y, cc.z, cc.w};
         unsigned pj[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) pj[k] = upack[col[k]];
+        for (int k = 0; k < 4; ++k) pj[k] = live ? upack[col[k]] : 0u;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int t = slot_of(ci, unpack(pj[k], pk));
-            if (t == open) {
-                acc += (float)v[k];
-            } else if (t > open) {
-                if (open >= 0) put(open, acc);
-                for (; cur < t; ++cur)
-                    if (cur != open) put(cur, 0.0f);
-                cur = t + 1;
-                open = t;
-                acc = (float)v[k];
-            } else {  // out of order: this lane wrote slot t already
-                put(t, ap[slot_index(i, t)] + (float)v[k]);
-            }
-        }
+        for (int k = 0; k < 4; ++k) acc[w][slot_of(ci, unpack(pj[k], pk))][lane] += (float)v[k];
     }
-    if (open >= 0) put(open, acc);
-    for (; cur < MG_SLOTS; ++cur) put(cur, 0.0f);
-    hrow[MG_SLOTS] = __float2half_rn(0.0f);
+    __syncwarp();
+    if (!live) return;
+#pragma unroll
+    for (int t = 0; t < MG_SLOTS; ++t) ap[slot_index(i, t)] = acc[w][t][lane];
+    const double di = dinv[i];
+    uint2* hr = reinterpret_cast<uint2*>(aph + i * MG_APH_STRIDE);
+#pragma unroll
+    for (int k = 0; k < MG_APH_STRIDE / 4; ++k) {
+        __half2 h0 = __floats2half2_rn((float)(acc[w][4 * k][lane] * di), (float)(acc[w][4 * k + 1][lane] * di));
+        __half2 h1 = __floats2half2_rn((float)(acc[w][4 * k + 2][lane] * di),
+                                       4 * k + 3 < MG_SLOTS ? (float)(acc[w][4 * k + 3][lane] * di) : 0.0f);
+        uint2 q;
+        q.x = *reinterpret_cast<unsigned*>(&h0);
+        q.y = *reinterpret_cast<unsigned*>(&h1);
+        hr[k] = q;
+    }
 }
 
 __device__ __forceinline__ float safe_inv(double d) {
@@ -481,27 +474,33 @@ __global__ void __launch_bounds__(UP0_THREADS) k_mg_up0(long long U, const int* 
     __shared__ float E[UP0_THREADS * MG_SLOTS];
     const long long i0 = blockIdx.x * (long long)UP0_THREADS;
     const long long i = i0 + threadIdx.x;
+    const bool live = i < U;
+    // the row's own data first, so its loads overlap the neighbor gathers below
+    uint2 h[MG_APH_STRIDE / 4];
+    const uint2* hr = reinterpret_cast<const uint2*>(aph + (live ? i : i0) * MG_APH_STRIDE);
+#pragma unroll
+    for (int k = 0; k < MG_APH_STRIDE / 4; ++k) h[k] = __ldcs(hr + k);
+    const double zi = live ? z[i] : 0.0, di = live ? dinv[i] : 1.0;
+    const int I = agg0[live ? i : i0];
     const int I0 = agg0[i0];
     const int na = agg0[min(i0 + UP0_THREADS - 1, U - 1)] - I0 + 1;  // <= UP0_THREADS
     for (int q = threadIdx.x; q < na * MG_SLOTS; q += UP0_THREADS) {
         const int a = q / MG_SLOTS;
         E[q] = e1[max(nbr1[slot_index(I0 + a, q - a * MG_SLOTS)], 0)];  // empty slots: AP is 0 there
     }
+    const float eI = e1[I];
     __syncthreads();
-    if (i >= U) return;
-    const int I = agg0[i];
+    if (!live) return;
     const float* Er = E + (I - I0) * MG_SLOTS;
-    const uint2* hr = reinterpret_cast<const uint2*>(aph + i * MG_APH_STRIDE);
     float s = 0.0f;
 #pragma unroll
     for (int k = 0; k < MG_APH_STRIDE / 4; ++k) {
-        const uint2 q = __ldcs(hr + k);
-        const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
-        const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
+        const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&h[k].x));
+        const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&h[k].y));
         s += f0.x * Er[4 * k] + f0.y * Er[4 * k + 1] + f1.x * Er[4 * k + 2];
         if (4 * k + 3 < MG_SLOTS) s += f1.y * Er[4 * k + 3];
     }
-    out[i] = (double)MG_OMEGA * z[i] + (double)MG_ALPHA * ((double)e1[I] - (double)MG_OMEGA * (double)s) / dinv[i];
+    out[i] = (double)MG_OMEGA * zi + (double)MG_ALPHA * ((double)eI - (double)MG_OMEGA * (double)s) / di;
 }
 
 inline unsigned grid_for(long long n, int threads) {
@@ -576,8 +575,8 @@ void mg_setup(lsmps_ctx* ctx) {
     LSMPS_CHECK_LAUNCH();
     float* ap = M.ap.ensure<float>(padded(U) * MG_SLOTS);
     const Sell<double> A64 = sell_a64_view(ctx);
-    k_mg_fine_ap<<<grid_for(32 * A64.nslices, 256), 256, 0, s>>>(A64, upack, pk, ctx->A_dinv.get<double>(), ap,
-                                                               M.aph.ensure<__half>(U * MG_APH_STRIDE + 8));
+    k_mg_fine_ap<<<grid_for(A64.nslices, AP_WARPS), AP_WARPS * 32, 0, s>>>(
+        A64, upack, pk, ctx->A_dinv.get<double>(), ap, M.aph.ensure<__half>(U * MG_APH_STRIDE + 8));
     LSMPS_CHECK_LAUNCH();
     k_mg_level1<<<grid_for(32 * n1, 256), 256, 0, s>>>(n1, ustart, ap, L1.val.ensure<float>(padded(n1) * MG_SLOTS),
                                                        L1.dinv.ensure<float>(n1));
@@ -634,24 +633,30 @@ void mg_setup(lsmps_ctx* ctx) {
     M.gen = ctx->assembly_gen;
 }
 
-// restrict0, the down steps (two kernels for level 1), the coarsest, the up steps and the
-// fine kernel
-int mg_launches_per_apply(lsmps_ctx* ctx) {
+// restrict0 (unless the caller restricted), the down steps (two kernels for level 1), the
+// coarsest, the up steps and the fine kernel
+int mg_launches_per_apply(lsmps_ctx* ctx, bool restricted) {
     if (!ctx->mg) return 0;
     const int Lc = ctx->mg->levels;
-    return 1 + (Lc > 1 ? 2 + (Lc - 2) : 0) + 1 + (Lc - 1) + 1;
+    return (restricted ? 0 : 1) + (Lc > 1 ? 2 + (Lc - 2) : 0) + 1 + (Lc - 1) + 1;
+}
+
+MgFine mg_fine(lsmps_ctx* ctx) {
+    MgState& M = *ctx->mg;
+    return MgFine{M.L[1].n, M.ustart.get<int>(), M.L[1].r.get<float>()};
 }
 
 // out = D M z on the context stream (z, out: U doubles); gated by the solver scalars S
 // (need_s: also skip once the |s| test has passed).
-void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S, int need_s) {
+void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S, int need_s, bool restricted) {
     MgState& M = *ctx->mg;
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;
     const int Lc = M.levels;
     MgLevel* L = M.L;
-    launch_pdl(k_mg_restrict0, grid_for(L[1].n, 256), 256, 0, s, L[1].n, M.ustart.get<int>(), z, L[1].r.get<float>(),
-               S, need_s);
+    if (!restricted)
+        launch_pdl(k_mg_restrict0, grid_for(L[1].n, 256), 256, 0, s, L[1].n, M.ustart.get<int>(), z,
+                   L[1].r.get<float>(), S, need_s);
     for (int l = 1; l < Lc; ++l) {
         if (l == 1) {
             launch_pdl(k_mg_res, grid_for(4 * L[1].n, 256), 256, 0, s, L[1].n, L[1].val.get<float>(),
@@ -673,7 +678,7 @@ void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S,
                    L[l].x.get<float>(), L[l + 1].e.get<float>(), L[l].e.get<float>(), S, need_s);
     launch_pdl(k_mg_up0, grid_for(U, UP0_THREADS), UP0_THREADS, 0, s, U, M.agg0.get<int>(), M.aph.get<__half>(), L[1].nbr.get<int>(),
                L[1].e.get<float>(), z, ctx->A_dinv.get<double>(), out, S, need_s);
-    note_launches((uint64_t)mg_launches_per_apply(ctx));
+    note_launches((uint64_t)mg_launches_per_apply(ctx, restricted));
 }
 
 // One V-cycle (ungated) `reps` times between events; algorithmic bytes: the fine level reads

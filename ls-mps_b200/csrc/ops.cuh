@@ -67,11 +67,13 @@ void ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
 void ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
 
 // multigrid.cu: the cell-aggregation V-cycle preconditioner (out = D M z, gated by the
-// solver scalars; need_s also skips once the |s| test has passed)
+// solver scalars; need_s also skips once the |s| test has passed; restricted: the caller
+// has already written the level-1 right-hand side P^T z)
 struct BcgScalars;
 void mg_setup(lsmps_ctx* ctx);
-void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S, int need_s);
-int mg_launches_per_apply(lsmps_ctx* ctx);
+void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S, int need_s,
+              bool restricted = false);
+int mg_launches_per_apply(lsmps_ctx* ctx, bool restricted = false);
 void mg_destroy(lsmps_ctx* ctx);
 void mg_info(lsmps_ctx* ctx, int* levels, int64_t* rows, int cap, double* setup_ms);
 void mg_apply_host(lsmps_ctx* ctx, const double* z, double* out, size_t n);

@@ -445,6 +445,53 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
     }
 }
 
+// With the multigrid: p = r + beta (p - omega v) and its restriction r1 = P^T p in one pass,
+// one thread per level-1 aggregate over its contiguous rows.
+__global__ void __launch_bounds__(RB) k_bcg_p_agg(MgFine G, const double* __restrict__ r, double* __restrict__ p,
+                                                  const double* __restrict__ v, const BcgScalars* S) {
+    pdl_begin();
+    if (S->done) return;
+    const double beta = S->beta, omega = S->omega;
+    for (long long I = blockIdx.x * (long long)RB + threadIdx.x; I < G.n1; I += (long long)gridDim.x * RB) {
+        double a = 0;
+        for (int i = G.ustart[I], e = G.ustart[I + 1]; i < e; ++i) {
+            const double pi = r[i] + beta * (p[i] - omega * v[i]);
+            p[i] = pi;
+            a += pi;
+        }
+        G.r1[I] = (float)a;
+    }
+}
+
+// With the multigrid: s = r - alpha v, |s|, and r1 = P^T s in one pass (as k_bcg_p_agg).
+__global__ void __launch_bounds__(RB) k_bcg_s_agg(MgFine G, const double* __restrict__ r,
+                                                  const double* __restrict__ v, double* __restrict__ s,
+                                                  BcgScalars* S, Partials P) {
+    pdl_begin();
+    if (S->done) return;
+    const double alpha = S->alpha;
+    double acc = 0;
+    for (long long I = blockIdx.x * (long long)RB + threadIdx.x; I < G.n1; I += (long long)gridDim.x * RB) {
+        double a = 0;
+        for (int i = G.ustart[I], e = G.ustart[I + 1]; i < e; ++i) {
+            const double si = r[i] - alpha * v[i];
+            s[i] = si;
+            acc += si * si;
+            a += si;
+        }
+        G.r1[I] = (float)a;
+    }
+    if (block_partials(acc, 0.0, P, &S->counter[1])) {
+        double ss, unused;
+        final_sum(P, &ss, &unused);
+        if (threadIdx.x == 0) {
+            S->counter[1] = 0;
+            S->sn = sqrt(ss);
+            if (S->sn <= S->thresh) { S->s_conv = 1; S->iters = S->it + 1; }
+        }
+    }
+}
+
 // t = A sv; omega = (t, s) / (t, t), with sv = s, or the preconditioned M s when a
 // preconditioner is applied (s then only enters the dot)
 template <class T, class TM = T, bool C16 = false>
@@ -1074,24 +1121,26 @@ cudaGraphExec_t build_while_graph(cudaStream_t s, LoopCtl* C, F&& body) {
 template <class T, class TM = T>
 void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V, bool mg = false) {
     note_launches(5);
-    launch_pdl(k_bcg_p<T>, RGRID, RB, 0, E.s, A.n, V.r, V.p, V.v, E.S);
     const T* pv = V.p;
     const T* sv = V.s;
     if constexpr (std::is_same<T, double>::value) {
-        if (mg) {
-            mg_apply(E.ctx, V.p, V.ph, E.S, 0);
+        if (mg) {  // p and its level-1 restriction in one pass, then the rest of the V-cycle
+            launch_pdl(k_bcg_p_agg, RGRID, RB, 0, E.s, mg_fine(E.ctx), V.r, V.p, V.v, E.S);
+            mg_apply(E.ctx, V.p, V.ph, E.S, 0, true);
             pv = V.ph;
         }
     }
+    if (!mg) launch_pdl(k_bcg_p<T>, RGRID, RB, 0, E.s, A.n, V.r, V.p, V.v, E.S);
     if (A.dcol) launch_pdl(k_bcg_v<T, TM, true>, RGRID, RB, 0, E.s, A, pv, V.v, V.r0, E.S, E.P);
     else launch_pdl(k_bcg_v<T, TM, false>, RGRID, RB, 0, E.s, A, pv, V.v, V.r0, E.S, E.P);
-    launch_pdl(k_bcg_s<T>, RGRID, RB, 0, E.s, A.n, V.r, V.v, V.s, E.S, E.P);
     if constexpr (std::is_same<T, double>::value) {
         if (mg) {
-            mg_apply(E.ctx, V.s, V.sh, E.S, 1);
+            launch_pdl(k_bcg_s_agg, RGRID, RB, 0, E.s, mg_fine(E.ctx), V.r, V.v, V.s, E.S, E.P);
+            mg_apply(E.ctx, V.s, V.sh, E.S, 1, true);
             sv = V.sh;
         }
     }
+    if (!mg) launch_pdl(k_bcg_s<T>, RGRID, RB, 0, E.s, A.n, V.r, V.v, V.s, E.S, E.P);
     if (A.dcol) launch_pdl(k_bcg_t<T, TM, true>, RGRID, RB, 0, E.s, A, sv, V.t, E.S, E.P, V.s);
     else launch_pdl(k_bcg_t<T, TM, false>, RGRID, RB, 0, E.s, A, sv, V.t, E.S, E.P, V.s);
     if (mg)
@@ -1102,7 +1151,7 @@ void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V, bool mg = false) 
 }
 
 // kernel launches of one iteration
-int launches_per_iteration(lsmps_ctx* ctx, bool mg) { return 5 + (mg ? 2 * mg_launches_per_apply(ctx) : 0); }
+int launches_per_iteration(lsmps_ctx* ctx, bool mg) { return 5 + (mg ? 2 * mg_launches_per_apply(ctx, true) : 0); }
 
 template <class T, class TM = T>
 void init(Engine& E, const Sell<TM>& A, const T* b, const Vecs<T>& V, bool use_x, double tol, double bnorm_override) {
