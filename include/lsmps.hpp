@@ -58,6 +58,7 @@ struct Config {
     std::string wls_precision{"fp64"};  // fp64 | mixed (fp32 Cholesky + fp64 refinement)
     int device{0};                 // CUDA device ordinal
     std::string mpnn_weights{};    // learned preconditioner weights file (solver=learned)
+    std::string precond{"jacobi"};  // jacobi | multigrid (the mixed and learned solvers)
 };
 
 // (reference include/lsmps.hpp:20)

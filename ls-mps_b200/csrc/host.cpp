@@ -58,6 +58,7 @@ bool apply_key(Config& c, const std::string& k, const std::string& v) {
     else if (k == "wls_precision") c.wls_precision = v;
     else if (k == "device") c.device = std::stoi(v);
     else if (k == "mpnn_weights") c.mpnn_weights = v;
+    else if (k == "precond") c.precond = v;
     else return false;
     return true;
 }
@@ -250,6 +251,12 @@ int solver_id(const std::string& s) {
     throw std::runtime_error("unknown solver: " + s);
 }
 
+int precond_id(const std::string& s) {
+    if (s == "jacobi") return LSMPS_PRECOND_JACOBI;
+    if (s == "multigrid") return LSMPS_PRECOND_MULTIGRID;
+    throw std::runtime_error("unknown precond: " + s);
+}
+
 int variant_id(const std::string& s) {
     if (s == "reference") return LSMPS_PPE_REFERENCE;
     if (s == "shifted") return LSMPS_PPE_SHIFTED;
@@ -347,6 +354,7 @@ Metrics run_benchmark(const Config& c, std::vector<Particle>& ps) {
     ctx.check(lsmps_ppe_assemble(ctx.p, &po, &pst), "PPE assembly");
     lsmps_solver_opts so{};
     so.solver = solver_id(c.solver);
+    so.precond = precond_id(c.precond);
     so.max_iter = c.ppe_max_iter;
     so.tol = c.ppe_tol;
     so.use_graph = 1;

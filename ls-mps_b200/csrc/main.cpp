@@ -23,7 +23,8 @@ int main(int argc, char** argv) {
         lsmps::write_csv(base + ".csv", cfg, m);
         {
             std::ofstream o(base + ".gpu.json");
-            o << std::setprecision(10) << "{\"solver\": \"" << cfg.solver << "\", \"ppe_variant\": \"" << cfg.ppe_variant
+            o << std::setprecision(10) << "{\"solver\": \"" << cfg.solver << "\", \"precond\": \"" << cfg.precond
+              << "\", \"ppe_variant\": \"" << cfg.ppe_variant
               << "\", \"wls_mode\": \"" << cfg.wls_mode << "\", \"upload_ms\": " << m.upload_ms
               << ", \"neighbor_ms\": " << m.neighbor_ms << ", \"wls_ms\": " << m.wls_ms
               << ", \"assembly_ms\": " << m.ppe.assembly_ms << ", \"solve_ms\": " << m.ppe.solve_ms
