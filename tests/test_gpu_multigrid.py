@@ -53,6 +53,30 @@ def test_vcycle_matches_restatement(ctx, case):
     assert np.array_equal(ctx.mg_apply(z), out)  # deterministic
 
 
+def test_single_level_hierarchy(ctx):
+    """A system with at most 256 cells: level 1 is the coarsest (one block solves it)."""
+    import scipy.sparse as sp
+    from _util import jittered_lattice
+
+    xyz = jittered_lattice(12, 0.1, seed=4)
+    ctx.upload(xyz, np.zeros(len(xyz), np.uint8))
+    ctx.build_neighbors(RE, 128, L0)
+    ctx.wls(RE, L0, mode=1)
+    st = ctx.ppe_assemble("wls", 10**9, RE, L0, diag_shift=0.0)
+    row, col, val, b, xe, part = ctx.ppe(st.unknowns, st.nnz)
+    A = sp.csr_matrix((val, col, row), shape=(st.unknowns, st.unknowns))
+    H = mgo.Hierarchy(A, mgo.cells_of(xyz, xyz[part], RE))
+    assert H.levels == 1
+    z = np.random.default_rng(2).standard_normal(st.unknowns)
+    out = ctx.mg_apply(z)
+    rows, _ = ctx.mg_info()
+    assert list(rows) == H.sizes
+    ref = H.apply(z)
+    assert np.linalg.norm(out - ref) <= 1e-4 * np.linalg.norm(ref)
+    s = ctx.ppe_solve("mixed", 5000, 3e-11, precond="multigrid")
+    assert s.converged and s.relative_l2_error <= 1e-8
+
+
 def test_multigrid_solves_to_target(ctx):
     _setup(ctx, "mixed", 200_000, 7)
     jac = ctx.ppe_solve("mixed", 20000, 3e-11)
