@@ -61,8 +61,10 @@ uint64_t lsmps_launch_count(void);
 /* Profiling hook: launches one kernel of the path `reps` times on the context stream on
  * the current data and returns its mean duration (CUDA events around the launches) and
  * its algorithmic bytes per launch (the traffic a perfect kernel would move):
- *   LSMPS_KB_SPMV64  SELL SpMV + fused dot, FP64 values (plain FP64 solver)   12 nnz + 24.25 U
- *   LSMPS_KB_SPMV32  SELL SpMV + fused dot, FP32 values, FP64 vectors (MIXED)  8 nnz + 24.25 U
+ *   LSMPS_KB_SPMV64  SELL SpMV + fused dot, FP64 values (plain FP64 solver)   10 nnz + 28.25 U
+ *   LSMPS_KB_SPMV32  SELL SpMV + fused dot, FP32 values, FP64 vectors (MIXED)  6 nnz + 28.25 U
+ *                    (16-bit column steps and a 32-bit first column per row; with 32-bit
+ *                    columns, when a row does not ascend in small steps: 12 / 8 nnz + 24.25 U)
  *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL neighbor passes   24 N + 4 N (+ 4 P + 1 N fill)
  *   LSMPS_KB_WLS     all-particle WLS            24 N + 4 P + 80 N (z, sum w, status)
  * No reference counterpart (the reference has no GPU path). */
@@ -75,7 +77,7 @@ enum {
     LSMPS_KB_MPNN_LAYER = 5, /* one message-passing layer (aggregation + 64x128 tensor-core GEMM) of the
                                loaded network over the assembled PPE graph: 256 U + 8 Z */
     LSMPS_KB_MG_VCYCLE = 6   /* one multigrid V-cycle (all its kernels) on the assembled system's
-                               hierarchy: 144 U + 464 (rows of the coarse levels) */
+                               hierarchy: 92 U + 464 (rows of the coarse levels) */
 };
 int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
