@@ -380,6 +380,8 @@ class Context:
 
     def ppe_solve(self, solver, max_iter, tol, warm_start=False, use_graph=True, inner_tol=0.0,
                   inner_max_iter=0, stall_window=0, check_every=0, precond="jacobi"):
+        """lsmps_ppe_solve. solver: a name of SOLVERS; precond: "jacobi" or "multigrid" (the MIXED
+        and LEARNED solvers); use_graph: 1 device-driven graph, 2 chunk graphs, 0 eager."""
         o = SolverOpts(solver=SOLVERS.get(solver, solver), max_iter=int(max_iter), tol=tol,
                        warm_start=1 if warm_start else 0, use_graph=int(use_graph),
                        inner_tol=inner_tol, inner_max_iter=inner_max_iter, stall_window=stall_window,
