@@ -223,7 +223,8 @@ enum {
  * smooths each level; the coarsest level of at most 256 rows gets 10 sweeps. It is rebuilt
  * after each assembly (its setup time is in solve_ms). No reference counterpart: the
  * reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for loaded CSR systems,
- * which have no cells. */
+ * which have no cells. Opt-in: cell aggregates ignore connection strength, so systems with
+ * weakly coupled particles or strong row contrasts can need more iterations than JACOBI. */
 enum {
     LSMPS_PRECOND_JACOBI = 0,
     LSMPS_PRECOND_MULTIGRID = 1
