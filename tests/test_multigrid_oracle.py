@@ -63,3 +63,36 @@ def test_vcycle_preconditions(system):
     _, info_j, it_j = _iterations(A, b, sp.diags(1.0 / d))
     assert info_j == 0
     assert it_mg * 4 <= it_j, (it_mg, it_j)
+
+
+def test_restatement_matches_dense_two_level_cycle(built):
+    """The restatement on a system small enough for one coarse level, against the V-cycle
+    written out with dense matrices: P from the cells, A1 = P^T A P, the coarsest level's
+    Jacobi sweeps, alpha P e1, one fine Jacobi sweep, times D (FP16 A P / a_ii included)."""
+    from _util import jittered_lattice
+
+    xyz = jittered_lattice(10, 0.1, seed=3)
+    t = np.zeros(len(xyz), np.uint8)
+    row, col, _ = Oracle.neighbors(xyz, RE, 128)
+    cls = Oracle.classify(xyz, t, row, col, L0)
+    _, wst, z, ws = Oracle.wls(xyz, cls, row, col, RE, L0)
+    prow, pcol, pval, b, xe, up, _ = Oracle.ppe_assemble(2, xyz, cls, row, col, RE, L0, len(t), 0.0, z, ws, wst)
+    A = sp.csr_matrix((pval, pcol, prow), shape=(len(b), len(b))).toarray()
+    cells = mgo.cells_of(xyz, xyz[up], RE)
+    H = mgo.Hierarchy(sp.csr_matrix(A), cells)
+    assert H.levels == 1 and len(b) > 100
+    _, agg = np.unique(cells[:, 0] + 1000 * cells[:, 1] + 10 ** 6 * cells[:, 2], return_inverse=True)
+    P = np.zeros((len(b), agg.max() + 1))
+    P[np.arange(len(b)), agg] = 1.0
+    A1 = P.T @ A @ P
+    d, d1 = np.diag(A), np.diag(A1)
+    aps = (A @ P) / d[:, None]
+    aps = np.where(aps != 0, aps.astype(np.float16).astype(np.float64), 0.0)
+    zv = np.random.default_rng(5).standard_normal(len(b))
+    r1 = P.T @ zv
+    e = mgo.OMEGA * r1 / d1
+    for _ in range(mgo.SWEEPS - 1):
+        e = e + mgo.OMEGA * (r1 - A1 @ e) / d1
+    want = mgo.OMEGA * zv + mgo.ALPHA * d * (P @ e - mgo.OMEGA * (aps @ e))
+    got = H.apply(zv)
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
