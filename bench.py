@@ -78,6 +78,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 comparison solves")
     ap.add_argument("--cpu-sample-s", type=float, default=8.0, help="CPU BiCGStab sample budget (s)")
+    ap.add_argument("--ref-iterations", type=int, default=20,
+                    help="reference arm: BiCGStab iterations timed per step (projected to the full count)")
     return ap.parse_args()
 
 
@@ -444,58 +446,103 @@ def cpu_baseline(ctx, xyz, types, plain_iterations, sample_s):
 # the reference arm: the reference's CPU implementation of the path
 # ---------------------------------------------------------------------------------------
 def run_reference(args, dist):
-    """Times the reference's own CPU implementation (oracle/_ref) of this step. Where the
-    reference lacks a piece (all-particle WLS, the WLS-Laplacian rows) the oracle's CPU
-    restatement stands in; BiCGStab runs the reference's iteration for a bounded sample and
-    is extrapolated to the iteration count that the same FP64 iteration (run once, in the
-    warm-up, multi-threaded) needs to reach the tolerance."""
-    import lsmps_b200 as lib
+    """Times the reference's own CPU implementation (oracle/_ref, single-threaded as the
+    reference is) of this step on the GPU arm's particle sets (same generator, same seeds;
+    the oracle's restatement of the generator builds them, so this arm never loads the
+    product library). Each step is a bounded sample of the full step, and `value` projects
+    it to the full step:
+      * timed in full: the reference's neighbors, classify and assemble_ppe on every particle;
+      * timed on a sample: its wls_test on its own strided 4,096-particle sample (scaled to
+        every particle), and `--ref-iterations` iterations of its BiCGStab on the set's
+        WLS-Laplacian system (scaled to the iteration count the same FP64 iteration needs to
+        reach the tolerance on that system, found once per set in the warm-up with the
+        oracle's multi-threaded FP64 BiCGStab).
+    Where the reference lacks a piece (the all-particle WLS behind the WLS-Laplacian rows)
+    the oracle's CPU restatement builds the system, outside the timed region."""
     from oracle import Oracle, Ref
 
-    xyz, types, _ = lib.generate(None, case=args.case, particles=args.particles, l0=L0, seed=args.seed)
-    n = len(types)
+    K = max(1, args.sets)
+    seeds = [args.seed + k for k in range(K)]
     nt = os.cpu_count() or 1
     re = RE_RATIO * L0
-    # warm-up: the oracle's WLS-Laplacian system and the iteration count to the tolerance
-    r = _ref_case(xyz, types)
-    row, col, _ = r.neighbors()
-    cls = r.classify()
-    _, wst, z, ws = Oracle.wls(xyz, cls, row, col, re, L0)
-    prow, pcol, pval, pb, pxe, _, _ = Oracle.ppe_assemble(2, xyz, cls, row, col, re, L0, n, 0.0, z, ws, wst)
-    _, info = Oracle.bicgstab(prow, pcol, pval, pb, args.max_iter, args.tol, nthreads=nt)
-    iters = info["iterations"]
-    samples = []
+    sets = []
+    t_setup = time.perf_counter()
+    for sd in seeds:  # inputs and the iteration count to the tolerance, per set
+        xyz, types = Oracle.generate(args.case, args.particles, L0, sd)
+        n = len(types)
+        r = _ref_case(xyz, types)
+        row, col, _ = r.neighbors()
+        cls = r.classify()
+        _, wst, z, ws = Oracle.wls(xyz, cls, row, col, re, L0)
+        prow, pcol, pval, pb, pxe, _, _ = Oracle.ppe_assemble(2, xyz, cls, row, col, re, L0, n, 0.0, z, ws, wst)
+        _, info = Oracle.bicgstab(prow, pcol, pval, pb, args.max_iter, args.tol, nthreads=nt)
+        sets.append((xyz, types, (prow, pcol, pval, pb, pxe), info["iterations"]))
+    setup_s = time.perf_counter() - t_setup
+    k_it = max(1, args.ref_iterations)
+    timed, projected, phases = [], [], []
     for k in range(args.warmup + args.steps):
+        xyz, types, (prow, pcol, pval, pb, pxe), iters = sets[k % K]
+        n = len(types)
+        w0 = time.perf_counter()
         r = _ref_case(xyz, types)
         t0 = time.perf_counter()
         r.neighbors()
-        r.classify()
         t1 = time.perf_counter()
-        w = r.wls_test()
+        r.classify()
         t2 = time.perf_counter()
-        r.assemble_ppe()
+        w = r.wls_test()
         t3 = time.perf_counter()
-        _, si = Ref.bicgstab_csr(prow, pcol, pval, pb, pxe, 20, 0.0)
-        # wls_test runs on a strided sample: its time is scaled to every particle
-        wls_ms = (t2 - t1) * 1e3 * n / max(1.0, w["sampled"] + w["failed"])
-        step_ms = (t1 - t0) * 1e3 + wls_ms + (t3 - t2) * 1e3 + si["solve_ms"] / max(1, si["iterations"]) * iters
+        r.assemble_ppe()
+        t4 = time.perf_counter()
+        _, si = Ref.bicgstab_csr(prow, pcol, pval, pb, pxe, k_it, 0.0)
+        t5 = time.perf_counter()
+        sampled = max(1.0, w["sampled"] + w["failed"])
+        ms_it = si["solve_ms"] / max(1, si["iterations"])
+        ph = {"neighbors": (t1 - t0) * 1e3, "classify": (t2 - t1) * 1e3, "wls_test_sample": (t3 - t2) * 1e3,
+              "wls_projected": (t3 - t2) * 1e3 * n / sampled, "assemble_ppe": (t4 - t3) * 1e3,
+              "bicgstab_sample": (t5 - t4) * 1e3, "bicgstab_projected": ms_it * iters,
+              "bicgstab_iterations_projected": iters, "wls_particles_sampled": sampled}
         if k >= args.warmup:
-            samples.append(step_ms)
-    ms = statistics.median(samples)
-    value = n / (ms * 1e-3)
+            timed.append((t5 - w0) * 1e3)
+            projected.append(ph["neighbors"] + ph["classify"] + ph["wls_projected"] + ph["assemble_ppe"]
+                             + ph["bicgstab_projected"])
+            phases.append(ph)
+    n = args.particles
+    ms_timed = statistics.mean(timed)
+    ms_proj = statistics.mean(projected)
+    value = n / (ms_proj * 1e-3)
+    mean_ph = {key: statistics.mean(p[key] for p in phases) for key in phases[0]}
+    sample = (f"per step, on set k mod {K}: the reference's neighbors, classify and assemble_ppe on all {n} "
+              f"particles (timed in full); its wls_test on {int(mean_ph['wls_particles_sampled'])} strided "
+              f"particles, projected to all {n}; {k_it} of its BiCGStab iterations on the set's WLS-Laplacian "
+              f"system, projected to the {mean_ph['bicgstab_iterations_projected']:.0f} iterations (mean over "
+              f"sets) the same FP64 iteration needs to reach tol {args.tol:g}; single-threaded")
     return {
         "impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": dist.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "value": value, "scaling": "weak",
+        "steps": args.steps, "warmup": args.warmup,
+        # wall time of one timed (sampled) step; `value` is the full step projected from it
+        "ms_per_step": ms_timed, "value": value, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; no dataset)",
         "config": {"workload": f"{args.case} {n} particles, WLS-Laplacian PPE, tol {args.tol:g}", "particles": n,
-                   "solver": "reference FP64 BiCGStab (CPU)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"per step: reference neighbors+classify+assemble_ppe on all {n} particles, "
-                                   f"wls_test on its 4096-particle sample scaled to all, and 20 reference BiCGStab "
-                                   f"iterations on the WLS-Laplacian matrix extrapolated to the {iters} iterations "
-                                   f"the same FP64 iteration needs ({nt} threads, once, in the warm-up)"},
+                   "case": args.case, "particle_sets": K, "seeds": seeds, "l0": L0, "re": re,
+                   "max_neighbors": MAXN, "solver": "reference FP64 BiCGStab (CPU)"},
+        "projection": {"timed_ms_per_step": ms_timed, "projected_ms_per_full_step": ms_proj,
+                       "factor": ms_proj / ms_timed, "phases_ms": mean_ph,
+                       "setup_s": setup_s, "note": "value = particles / projected full-step time"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample,
+                         "host_nproc": nt},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "product_library_loaded": _product_loaded(),
     }
+
+
+def _product_loaded():
+    """Whether this process mapped the product library (the reference arm must not)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return "liblsmps_b200" in f.read()
+    except OSError:
+        return None
 
 
 def main():

@@ -65,7 +65,9 @@ uint64_t lsmps_launch_count(void);
  *   LSMPS_KB_SPMV32  SELL SpMV + fused dot, FP32 values, FP64 vectors (MIXED)  6 nnz + 28.25 U
  *                    (16-bit column steps and a 32-bit first column per row; with 32-bit
  *                    columns, when a row does not ascend in small steps: 12 / 8 nnz + 24.25 U)
- *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL neighbor passes   24 N + 4 N (+ 4 P + 1 N fill)
+ *   LSMPS_KB_NBR_COUNT / LSMPS_KB_NBR_FILL two-pass neighbor build   24 N + 4 N (+ 4 P + 1 N fill)
+ *   LSMPS_KB_NBR_SCAN  single-pass neighbor scan into slot rows + classes   34 N + 4 P
+ *   LSMPS_KB_NBR_COMPACT  slot rows packed into the CSR                     4 (N + 1) + 8 P
  *   LSMPS_KB_WLS     all-particle WLS            24 N + 4 P + 80 N (z, sum w, status)
  * No reference counterpart (the reference has no GPU path). */
 enum {
@@ -76,8 +78,10 @@ enum {
     LSMPS_KB_WLS = 4,
     LSMPS_KB_MPNN_LAYER = 5, /* one message-passing layer (aggregation + 64x128 tensor-core GEMM) of the
                                loaded network over the assembled PPE graph: 256 U + 8 Z */
-    LSMPS_KB_MG_VCYCLE = 6   /* one multigrid V-cycle (all its kernels) on the assembled system's
+    LSMPS_KB_MG_VCYCLE = 6,  /* one multigrid V-cycle (all its kernels) on the assembled system's
                                hierarchy: 92 U + 464 (rows of the coarse levels) */
+    LSMPS_KB_NBR_SCAN = 7,
+    LSMPS_KB_NBR_COMPACT = 8
 };
 int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
@@ -111,7 +115,10 @@ typedef struct lsmps_neighbor_stats {
     int32_t reserved;
 } lsmps_neighbor_stats;
 
-#define LSMPS_NBR_CLASSIFY 1  /* fuse the 14-direction classification into the fill pass */
+#define LSMPS_NBR_CLASSIFY 1  /* fuse the 14-direction classification into the neighbor scan */
+#define LSMPS_NBR_TWO_PASS 2  /* count pass + fill pass instead of the single pass (same lists; the
+                                 single pass needs 4 x max_neighbors bytes per particle of scratch
+                                 and falls back to two passes above 4 GB of it) */
 
 /* Uniform-grid neighbor lists, bit-exact with the reference's neighbors()
  * (src/lsmps.cpp:16-18,26): cell = floor(r / re) per axis, 27 cells dz, dy, dx from -1
@@ -170,10 +177,15 @@ int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
 
 /* ---- PPE assembly ----------------------------------------------------------------- */
 enum { LSMPS_PPE_REFERENCE = 0, LSMPS_PPE_SHIFTED = 1, LSMPS_PPE_WLS = 2, LSMPS_PPE_LOADED = 3 /* lsmps_ppe_load_csr */ };
+/* WLS rows with Neumann walls: wall neighbors take the row particle's own pressure (zero normal
+ * gradient), so they add neither an entry nor a diagonal term; without it walls are Dirichlet
+ * neighbors like the free surface. No reference counterpart in 3-D (the reference's 2-D step
+ * mirrors the wall value: python/rain_plate_lsmps_cpu.py:90-100,179). */
+#define LSMPS_PPE_WALL_NEUMANN 1
 
 typedef struct lsmps_ppe_opts {
     int32_t variant;         /* LSMPS_PPE_* */
-    int32_t reserved;
+    int32_t flags;           /* LSMPS_PPE_WALL_NEUMANN (variant WLS only) */
     int64_t max_unknowns;    /* reference Config::ppe_max_unknowns */
     double re, l0;
     double diag_shift;       /* SHIFTED / WLS: diagonal times (1 + diag_shift) */
@@ -186,7 +198,8 @@ typedef struct lsmps_ppe_stats {
     double initial_residual, final_residual, relative_l2_error, max_error, assembly_ms, solve_ms;
     /* extensions */
     int32_t outer_iterations;   /* FP64 refinement sweeps (mixed / learned) */
-    int32_t fallback;           /* learned: 1 when the stall rule switched to Jacobi */
+    int32_t fallback;           /* 1 when the solve continued as Jacobi MIXED: LEARNED after a stall or a
+                                   discarded guess, MULTIGRID after a stall or a breakdown */
     double relative_residual;   /* |b - Ax| / |b| at exit (FP64) */
 } lsmps_ppe_stats;
 
@@ -224,7 +237,9 @@ enum {
  * after each assembly (its setup time is in solve_ms). No reference counterpart: the
  * reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for loaded CSR systems,
  * which have no cells. Opt-in: cell aggregates ignore connection strength, so systems with
- * weakly coupled particles or strong row contrasts can need more iterations than JACOBI. */
+ * weakly coupled particles or strong row contrasts can need more iterations than JACOBI. A
+ * multigrid run that stalls (stall_window) or breaks down continues as Jacobi MIXED from its
+ * iterate (from zero if that is no longer finite) and reports fallback = 1. */
 enum {
     LSMPS_PRECOND_JACOBI = 0,
     LSMPS_PRECOND_MULTIGRID = 1
@@ -244,7 +259,8 @@ typedef struct lsmps_solver_opts {
     double inner_tol;        /* MIXED / LEARNED: residual drop between FP64 residual replacements
                                 (default 0.01); MIXED_F32: the same (default 0.1) */
     int32_t inner_max_iter;  /* reserved */
-    int32_t stall_window;    /* LEARNED: iterations without progress before fallback (20) */
+    int32_t stall_window;    /* LEARNED / MULTIGRID: iterations without 1 % progress of |r| before the
+                                fallback to Jacobi MIXED (default 20) */
     int32_t check_every;     /* iterations between host convergence checks (default 8) */
     int32_t precond;         /* LSMPS_PRECOND_* (MIXED / LEARNED; default JACOBI) */
 } lsmps_solver_opts;
@@ -303,9 +319,10 @@ int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes);
  * device, or whose device memory is already in their own pool. The reduction scratch is
  * one static device array of 42,880 bytes per device (partial sums of at most 592 blocks
  * for at most 8 vectors); nvec outside 1..8 fails with LSMPS_ERR_ARG. Its ticket word must
- * start at zero: each call clears it on the stream before the launch. The first call on a
- * device resolves the array's address (cudaGetSymbolAddress, checked; it may load the
- * module), so make that first call before any stream capture begins. The scratch is shared
+ * start at zero: each call clears it on the stream before the launch. Every call resolves
+ * the array's address on the context's device (cudaGetSymbolAddress, checked; nothing is
+ * cached, so a device reset between calls is harmless). The first call on a device may load
+ * the module, so make that first call before any stream capture begins. The scratch is shared
  * by every context on the device: calls whose executions overlap in time (two contexts, two
  * streams, two threads) race on it and must be serialised by the caller. */
 int lsmps_ppe_residual_static(lsmps_ctx* ctx, const double* d_p, size_t ld, int nvec, double* d_out);
@@ -328,14 +345,23 @@ typedef struct lsmps_projection_stats {
     double relative_residual, solve_ms, total_ms;
     uint64_t core;           /* Interior unknowns at least 3 neighbor hops from any other particle */
     double div_core_before_rms, div_core_after_rms;  /* over the core */
+    /* the wall bands: unknowns 1 (band 1) or 2 (band 2) neighbor hops from a wall particle and
+       at least 3 hops from any free-surface or splash particle */
+    uint64_t wall_band1, wall_band2;
+    double div_wall1_before_rms, div_wall1_after_rms, div_wall2_before_rms, div_wall2_after_rms;
 } lsmps_projection_stats;
 
 /* One pressure projection (the reference's 2-D python/rain_plate_lsmps_cpu.py:202-260 in
  * 3-D): div u* from lsmps_wls_fields of the velocity, the assembled WLS-Laplacian PPE (variant
  * LSMPS_PPE_WLS; free-surface / splash Dirichlet p = 0) solved with opts for
  * lap p = rho / dt div u* (b = -rho / dt div u*, as A ~ -lap), and u = u* - dt / rho grad p
- * (walls keep u*). d_vel / d_vel_out: n x 3 device arrays, caller order; d_pressure: n values,
- * 0 off the unknowns. Overwrites the assembled b (and p* with 0). */
+ * (walls keep u*). With a PPE assembled with LSMPS_PPE_WALL_NEUMANN the walls are Neumann
+ * boundaries: in the divergence, the pressure gradient and the PPE rows, wall neighbors take
+ * the particle's own value (zero normal gradient), the mirrored wall value of the reference's
+ * virtual points (python/rain_plate_lsmps_cpu.py:90-100,179); the wall particles themselves
+ * serve as the mirrored points in the moment matrices. d_vel / d_vel_out: n x 3 device arrays,
+ * caller order; d_pressure: n values, 0 off the unknowns. Overwrites the assembled b (and p*
+ * with 0). */
 int lsmps_projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* opts,
                           double* d_vel_out, double* d_pressure, lsmps_projection_stats* out);
 
@@ -438,7 +464,7 @@ int lsmps_series_set_validation(lsmps_series* series, const lsmps_rain_validatio
 int lsmps_series_rain_outputs(lsmps_series* series, lsmps_rain_outputs* out);
 
 /* ---- learned preconditioner (message-passing network over the PPE graph) ----------- */
-/* No reference counterpart. Nodes are the PPE unknowns, edges the
+/* No reference counterpart (this library's learned preconditioner). Nodes are the PPE unknowns, edges the
  * off-diagonal entries with weight -a_ij / a_ii. Input features per node: residual
  * (unit-norm residual times sqrt(U)), diagonal a_ii / mean(a) - 1, NearWall flag,
  * row length / 32 - 1. Encoder 4 -> 64 (ReLU); three residual message-passing layers

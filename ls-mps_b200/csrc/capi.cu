@@ -37,6 +37,7 @@ void check_device_flags(lsmps_ctx* ctx, const char* where) {
     if (f & DFLAG_CELL_OVERFLOW) throw Error{LSMPS_ERR_GRID, w + ": a cell holds more than 8192 particles"};
     if (f & DFLAG_INDEX) throw Error{LSMPS_ERR_OVERFLOW, w + ": a count exceeds the int32 range"};
     if (f & DFLAG_TIMEOUT) throw Error{LSMPS_ERR_TIMEOUT, w + ": a bounded device wait expired"};
+    if (f & DFLAG_STENCIL) throw Error{LSMPS_ERR_GRID, w + ": a coupling spans more than one neighbor cell"};
     throw Error{LSMPS_ERR_CUDA, w + ": device error flag " + std::to_string(f)};
 }
 
@@ -188,7 +189,8 @@ int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_laun
         LSMPS_REQUIRE(ms_per_launch && bytes_per_launch && reps > 0, LSMPS_ERR_ARG, "kernel bench arguments");
         if (kernel == LSMPS_KB_SPMV64 || kernel == LSMPS_KB_SPMV32)
             solver_kernel_bench(ctx, kernel, reps, ms_per_launch, bytes_per_launch);
-        else if (kernel == LSMPS_KB_NBR_COUNT || kernel == LSMPS_KB_NBR_FILL)
+        else if (kernel == LSMPS_KB_NBR_COUNT || kernel == LSMPS_KB_NBR_FILL || kernel == LSMPS_KB_NBR_SCAN ||
+                 kernel == LSMPS_KB_NBR_COMPACT)
             nb_kernel_bench(ctx, kernel, reps, ms_per_launch, bytes_per_launch);
         else if (kernel == LSMPS_KB_WLS)
             wls_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);

@@ -80,6 +80,7 @@ enum DeviceFlag : int {
     DFLAG_TIMEOUT = 2,
     DFLAG_CELL_OVERFLOW = 4,
     DFLAG_INDEX = 8,
+    DFLAG_STENCIL = 16,  // a PPE coupling spans more than one neighbor-grid cell (multigrid setup)
 };
 
 // ---- small device helpers ------------------------------------------------------------

@@ -69,6 +69,8 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf cell_of, slot, cell_count, cell_start, perm, iperm;
     lsmps_gpu::DevBuf sx, sy, sz, stype, scell, cls;
     lsmps_gpu::DevBuf nbr_cnt, nbr_row, nbr_col, nbr_stats, seg_list;
+    lsmps_gpu::DevBuf nbr_slots;  // single-pass build: maxn slots per particle before compaction
+    bool nbr_single = false;      // the last build used the single pass
     // candidate lists of radius re + skin (sorted numbering) and the sorted positions they
     // were built at, for refreshes of an unchanged particle set
     bool have_candidates = false;
@@ -92,6 +94,8 @@ struct lsmps_ctx {
     long long U = 0, nnz = 0;
     lsmps_gpu::DevBuf ref_rank, u_of_sorted, sorted_of_u, ref_of_u, u_of_ref;
     lsmps_gpu::DevBuf A_row, A_col, A_val, A_valf, A_b, A_xexact, A_dinv, A_dinvf, A_cnt;
+    lsmps_gpu::DevBuf A_slot_col, A_slot_val;
+    bool ppe_wall_neumann = false;  // the assembled WLS rows treat walls as Neumann boundaries  // assembly: rows at their neighbor-row slots before packing
     lsmps_ppe_stats ppe_assembly{};
     bool ppe_loaded = false;        // the system came from lsmps_ppe_load_csr (no particles behind it)
     lsmps_gpu::DevBuf ld_ident;     // identity map standing in for the particle permutation

@@ -154,7 +154,8 @@ constexpr int MG_APH_STRIDE = 28;  // 27 slots + 1 zero pad: 56 B rows, read as 
 constexpr int AP_WARPS = 4;
 __global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<double> A, const unsigned* __restrict__ upack,
                                                               Pack pk, const double* __restrict__ dinv,
-                                                              float* __restrict__ ap, __half* __restrict__ aph) {
+                                                              float* __restrict__ ap, __half* __restrict__ aph,
+                                                              int* __restrict__ dflag) {
     __shared__ float acc[AP_WARPS][MG_APH_STRIDE][33];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long sl = blockIdx.x * (long long)AP_WARPS + w;
@@ -176,7 +177,13 @@ __global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<double> A, co
 #pragma unroll
         for (int k = 0; k < 4; ++k) pj[k] = live ? upack[col[k]] : 0u;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc[w][slot_of(ci, unpack(pj[k], pk))][lane] += (float)v[k];
+        for (int k = 0; k < 4; ++k) {
+            const int3 cj = unpack(pj[k], pk);
+            // a coupling beyond the adjacent cells has no slot: flag it (clamped slot, no write
+            // out of bounds; the setup then fails with LSMPS_ERR_GRID)
+            if (abs(cj.x - ci.x) > 1 || abs(cj.y - ci.y) > 1 || abs(cj.z - ci.z) > 1) atomicOr(dflag, DFLAG_STENCIL);
+            acc[w][slot_of(ci, cj)][lane] += (float)v[k];
+        }
     }
     __syncwarp();
     if (!live) return;
@@ -576,7 +583,7 @@ void mg_setup(lsmps_ctx* ctx) {
     float* ap = M.ap.ensure<float>(padded(U) * MG_SLOTS);
     const Sell<double> A64 = sell_a64_view(ctx);
     k_mg_fine_ap<<<grid_for(A64.nslices, AP_WARPS), AP_WARPS * 32, 0, s>>>(
-        A64, upack, pk, ctx->A_dinv.get<double>(), ap, M.aph.ensure<__half>(U * MG_APH_STRIDE + 8));
+        A64, upack, pk, ctx->A_dinv.get<double>(), ap, M.aph.ensure<__half>(U * MG_APH_STRIDE + 8), dflag);
     LSMPS_CHECK_LAUNCH();
     k_mg_level1<<<grid_for(32 * n1, 256), 256, 0, s>>>(n1, ustart, ap, L1.val.ensure<float>(padded(n1) * MG_SLOTS),
                                                        L1.dinv.ensure<float>(n1));

@@ -30,6 +30,7 @@ constexpr long long MAX_CELLS = 1ll << 29;   // 2 GiB of int32 cell starts
 constexpr int SMALL_CELL = 64;                // in-place insertion sort up to this occupancy
 constexpr int BIG_CELL_MAX = 8192;            // shared-memory bitonic sort up to this occupancy
 constexpr int NB_WARPS = 8;                   // warps (= particles) per block in the passes
+constexpr double SLOT_BUDGET_BYTES = 4e9;     // slot rows of the single-pass build (n x maxn x 4 B)
 
 // ---- 1. cell coordinates --------------------------------------------------------------
 __global__ void k_cell_coords(const double* __restrict__ pos, size_t n, double re,
@@ -477,6 +478,194 @@ __global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_pass(SegGrid G, const in
     }
 }
 
+// ---- single pass: each query's kept list straight into its slot row ------------------------
+// The staging, the cell culling and the FP32 guard band of k_seg_pass, in one pass instead of
+// a count and a fill pass that repeat every distance test. A thread tests its row window 32
+// staged candidates at a time into a hit mask (no branch per candidate), then walks the set
+// bits in order: the rare guard-band hits are decided exactly in FP64, and each kept candidate
+// p < maxn goes to slots[k * maxn + p] with its sector bits. Counting continues past maxn for
+// the truncation statistic. k_slots_compact then packs the slot rows into the CSR once the
+// kept counts are scanned. The kept order is the staged order of the 9 row windows, which is
+// the reference's order, as in k_seg_pass.
+__device__ __forceinline__ void scan_query_global(const GridView& g, const double* __restrict__ sx,
+                                                  const double* __restrict__ sy, const double* __restrict__ sz,
+                                                  const int* __restrict__ scell, const uint8_t* __restrict__ stype,
+                                                  int k, double re2, int maxn, double l0, int classify,
+                                                  int* __restrict__ slots, int* __restrict__ cnt,
+                                                  unsigned long long* trunc_total, uint8_t* __restrict__ cls,
+                                                  int lane) {
+    const unsigned lt = (1u << lane) - 1u;
+    const int lin = scell[k];
+    const int cx = lin % g.nx, t = lin / g.nx, cy = t % g.ny, cz = t / g.ny;
+    const double xi = sx[k], yi = sy[k], zi = sz[k];
+    int* out = slots + (size_t)k * maxn;
+    int written = 0;
+    unsigned sec = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy) {
+            int beg, end;
+            if (!row_range(g, cx, cy, cz, dy, dz, beg, end)) continue;
+            for (int mb = beg; mb < end; mb += 32) {
+                const int m = mb + lane;
+                bool ok = false;
+                double dx = 0, dyv = 0, dzv = 0;
+                if (m < end && m != k) {
+                    dx = xsub(sx[m], xi);
+                    dyv = xsub(sy[m], yi);
+                    dzv = xsub(sz[m], zi);
+                    ok = xnorm2(dx, dyv, dzv) < re2;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) {
+                    const int p = written + __popc(bal & lt);
+                    if (p < maxn) {
+                        out[p] = m;
+                        if (classify) sec |= sector_bits(dx, dyv, dzv);
+                    }
+                }
+                written += __popc(bal);
+            }
+        }
+    if (lane == 0) {
+        cnt[k] = min(written, maxn);
+        if (written > maxn) atomicAdd(trunc_total, (unsigned long long)(written - maxn));
+    }
+    if (classify) {
+        sec = __reduce_or_sync(0xffffffffu, sec);
+        if (lane == 0) cls[k] = classify_rule(stype[k], min(written, maxn), sec, zi, l0);
+    }
+}
+
+__global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_scan(SegGrid G, const int* __restrict__ seg_list,
+                                                            const double* __restrict__ sx,
+                                                            const double* __restrict__ sy,
+                                                            const double* __restrict__ sz,
+                                                            const int* __restrict__ scell,
+                                                            const uint8_t* __restrict__ stype, double re2,
+                                                            int maxn, double l0, int classify,
+                                                            int* __restrict__ cnt,
+                                                            unsigned long long* trunc_total,
+                                                            int* __restrict__ slots, uint8_t* __restrict__ cls) {
+    __shared__ float4 cf[SEG_MAXC];
+    __shared__ int rbase[10], rfirst[9], rcs[9][SEG + 3];
+    const float re_f = (float)G.re;
+    const float re2f = (float)re2;
+    const float lo_th = re2f * (1.f - 2e-5f), hi_th = re2f * (1.f + 2e-5f);
+    const float cull = re2f * (1.f + 1e-4f);
+    const float margin = 4e-6f * re_f;
+    const int seg = seg_list[blockIdx.x];
+    const int sxi = seg % G.nsegx, tt = seg / G.nsegx, cy = tt % G.g.ny, cz = tt / G.g.ny;
+    const int cx0 = sxi * SEG, cx1 = min(cx0 + SEG, G.g.nx) - 1;
+    const int lo = max(cx0 - 1, 0), hi = min(cx1 + 1, G.g.nx - 1);
+    const int rowlin = (cz * G.g.ny + cy) * G.g.nx;
+    const int q0 = G.g.cell_start[rowlin + cx0], q1 = G.g.cell_start[rowlin + cx1 + 1];
+    for (int t = threadIdx.x; t < 9 * (SEG + 3); t += blockDim.x) {
+        const int r = t / (SEG + 3), c = lo + t % (SEG + 3);
+        const int y = cy + (r % 3 - 1), z = cz + (r / 3 - 1);
+        int v = 0;
+        if (y >= 0 && y < G.g.ny && z >= 0 && z < G.g.nz && c <= hi + 1) v = G.g.cell_start[(z * G.g.ny + y) * G.g.nx + c];
+        rcs[r][c - lo] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rbase[0] = 0;
+        for (int r = 0; r < 9; ++r) {
+            rfirst[r] = rcs[r][0];
+            rbase[r + 1] = rbase[r] + (rcs[r][hi + 1 - lo] - rcs[r][0]);
+        }
+    }
+    __syncthreads();
+    const int total = rbase[9];
+    if (total > SEG_MAXC) {
+        // crowded neighborhood: the global-memory form, one query per warp
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int k = q0 + warp; k < q1; k += SEG_THREADS / 32)
+            scan_query_global(G.g, sx, sy, sz, scell, stype, k, re2, maxn, l0, classify, slots, cnt, trunc_total, cls,
+                              lane);
+        return;
+    }
+    const double ox = (G.g0.x + cx0) * G.re, oy = (G.g0.y + cy) * G.re, oz = (G.g0.z + cz) * G.re;
+    for (int r = 0; r < 9; ++r) {  // row by row: consecutive threads load consecutive particles
+        const int n_r = rbase[r + 1] - rbase[r], f = rfirst[r], b = rbase[r];
+        for (int i = threadIdx.x; i < n_r; i += blockDim.x)
+            cf[b + i] = make_float4((float)(sx[f + i] - ox), (float)(sy[f + i] - oy), (float)(sz[f + i] - oz), 0.f);
+    }
+    __syncthreads();
+    for (int k = q0 + threadIdx.x; k < q1; k += blockDim.x) {
+        const int ck = scell[k] - rowlin;                   // the query's cell along x
+        const int kst = rbase[4] + (k - rfirst[4]);         // the query staged in the centre row
+        const float4 qf = cf[kst];
+        const float qx = qf.x - (ck - cx0) * re_f;          // position inside its own cell (x)
+        int* out = slots + (size_t)k * maxn;
+        int written = 0;
+        unsigned sec = 0;
+        for (int r = 0; r < 9; ++r) {
+            const int dy = r % 3 - 1, dz = r / 3 - 1;
+            const float gy = dy < 0 ? qf.y : (dy > 0 ? re_f - qf.y : 0.f);
+            const float gz = dz < 0 ? qf.z : (dz > 0 ? re_f - qf.z : 0.f);
+            const float gyz = gy * gy + gz * gz;
+            if (gyz > cull) continue;
+            // cells ck-1 .. ck+1 of this row, each kept when its box is within re
+            int clo = max(ck - 1, lo), chi = min(ck + 1, hi);
+            if (clo < ck && gyz + qx * qx > cull) clo = ck;
+            if (chi > ck && gyz + (re_f - qx) * (re_f - qx) > cull) chi = ck;
+            const int gb = rcs[r][clo - lo], ge = rcs[r][chi + 1 - lo];
+            const int sb = rbase[r] + (gb - rfirst[r]);
+            const int se = sb + (ge - gb);
+            const int mshift = rfirst[r] - rbase[r];  // global index = staged index + mshift
+            for (int c0 = sb; c0 < se; c0 += 32) {
+                const int len = min(32, se - c0);
+                unsigned hit = 0;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    if (i < len) {
+                        const float4 cj = cf[c0 + i];
+                        const float dx = cj.x - qf.x, dyf = cj.y - qf.y, dzf = cj.z - qf.z;
+                        const float d2 = dx * dx + dyf * dyf + dzf * dzf;
+                        if (d2 <= hi_th) hit |= 1u << i;
+                    }
+                }
+                if (r == 4 && kst >= c0 && kst < c0 + len) hit &= ~(1u << (kst - c0));
+                while (hit) {
+                    const int i = __ffs(hit) - 1;
+                    hit &= hit - 1;
+                    const float4 cj = cf[c0 + i];
+                    const float dx = cj.x - qf.x, dyf = cj.y - qf.y, dzf = cj.z - qf.z;
+                    const float d2 = dx * dx + dyf * dyf + dzf * dzf;
+                    const int m = c0 + i + mshift;
+                    if (d2 >= lo_th && !(xnorm2(xsub(sx[m], sx[k]), xsub(sy[m], sy[k]), xsub(sz[m], sz[k])) < re2))
+                        continue;
+                    if (written < maxn) {
+                        out[written] = m;
+                        if (classify) {
+                            unsigned bb;
+                            if (!sector_bits_f32(dx, dyf, dzf, margin, bb))
+                                bb = sector_bits(xsub(sx[m], sx[k]), xsub(sy[m], sy[k]), xsub(sz[m], sz[k]));
+                            sec |= bb;
+                        }
+                    }
+                    ++written;
+                }
+            }
+        }
+        cnt[k] = min(written, maxn);
+        if (written > maxn) atomicAdd(trunc_total, (unsigned long long)(written - maxn));
+        if (classify) cls[k] = classify_rule(stype[k], min(written, maxn), sec, sz[k], l0);
+    }
+}
+
+// Packs the slot rows into the CSR: eight lanes per row, row k's kept list from
+// slots[k * maxn] to col[row[k]].
+__global__ void __launch_bounds__(256) k_slots_compact(int n, int maxn, const int* __restrict__ slots,
+                                                       const int* __restrict__ row, int* __restrict__ col) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int k = (int)(g >> 3), sub = (int)(g & 7);
+    if (k >= n) return;
+    const int b = row[k], c = row[k + 1] - b;
+    const int* src = slots + (size_t)k * maxn;
+    for (int p = sub; p < c; p += 8) col[b + p] = __ldcs(src + p);
+}
+
 // Standalone classification over an existing CSR (warp per particle).
 __global__ void __launch_bounds__(NB_WARPS * 32) k_classify(const double* __restrict__ sx,
                                                           const double* __restrict__ sy,
@@ -699,10 +888,21 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     LSMPS_CUDA(cudaStreamSynchronize(s));
     ctx->nsegs = hsegs;
     const unsigned seg_grid = (unsigned)std::max(hsegs, 1);
+    const int do_cls = (flags & LSMPS_NBR_CLASSIFY) ? 1 : 0;
+    uint8_t* cls = ctx->cls.ensure<uint8_t>(n);
+    // one pass into maxn slots per particle while they fit (the usual case: 0.5 GB at 1M
+    // particles and maxn 128), else the count and fill passes
+    const bool single = !(flags & LSMPS_NBR_TWO_PASS) && (double)n * (double)maxn * 4.0 <= SLOT_BUDGET_BYTES;
+    ctx->nbr_single = single;
+    int* slots = single ? ctx->nbr_slots.ensure<int>((size_t)n * maxn + 1) : nullptr;
     if (n && hsegs) {
-        k_seg_pass<false><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
-                                                             ctx->re2, maxn, l0, 0, cnt, trunc_d, nullptr, nullptr,
-                                                             nullptr);
+        if (single)
+            k_seg_scan<<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype, ctx->re2, maxn, l0,
+                                                       do_cls, cnt, trunc_d, slots, cls);
+        else
+            k_seg_pass<false><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
+                                                                 ctx->re2, maxn, l0, 0, cnt, trunc_d, nullptr, nullptr,
+                                                                 nullptr);
         LSMPS_CHECK_LAUNCH();
     }
     scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
@@ -718,12 +918,13 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     ctx->truncated = htr;
     ctx->max_cell_occupancy = hocc;
     int* col = ctx->nbr_col.ensure<int>((size_t)hpairs + 1);
-    uint8_t* cls = ctx->cls.ensure<uint8_t>(n);
-    const int do_cls = (flags & LSMPS_NBR_CLASSIFY) ? 1 : 0;
     if (n && hsegs) {
-        k_seg_pass<true><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
-                                                            ctx->re2, maxn, l0, do_cls, nullptr, nullptr, row, col,
-                                                            cls);
+        if (single)
+            k_slots_compact<<<(unsigned)((8ull * n + 255) / 256), 256, 0, s>>>((int)n, maxn, slots, row, col);
+        else
+            k_seg_pass<true><<<seg_grid, SEG_THREADS, 0, s>>>(sg, seg_list, sx, sy, sz, scell, stype,
+                                                                ctx->re2, maxn, l0, do_cls, nullptr, nullptr, row, col,
+                                                                cls);
         LSMPS_CHECK_LAUNCH();
     }
     ctx->have_neighbors = true;
@@ -742,8 +943,25 @@ void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* b
     auto* trunc_d = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 16);
     const int* seg_list = ctx->seg_list.get<int>();
     const unsigned seg_grid = (unsigned)std::max(ctx->nsegs, 1);
+    int* slots = nullptr;
+    if (kernel == LSMPS_KB_NBR_SCAN || kernel == LSMPS_KB_NBR_COMPACT) {
+        LSMPS_REQUIRE((double)n * (double)ctx->maxn * 4.0 <= SLOT_BUDGET_BYTES, LSMPS_ERR_STATE,
+                      "single-pass neighbor bench: slot rows exceed the budget");
+        LSMPS_REQUIRE(kernel == LSMPS_KB_NBR_SCAN || ctx->nbr_single, LSMPS_ERR_STATE,
+                      "compaction bench needs a single-pass build");
+        slots = ctx->nbr_slots.ensure<int>((size_t)n * ctx->maxn + 1);
+    }
     auto launch = [&] {
-        if (kernel == LSMPS_KB_NBR_COUNT)
+        if (kernel == LSMPS_KB_NBR_SCAN)
+            k_seg_scan<<<seg_grid, SEG_THREADS, 0, s>>>(
+                sg, seg_list, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(), ctx->scell.get<int>(),
+                ctx->stype.get<uint8_t>(), ctx->re2, ctx->maxn, ctx->l0, ctx->have_classes ? 1 : 0,
+                ctx->nbr_cnt.get<int>(), trunc_d, slots, ctx->cls.get<uint8_t>());
+        else if (kernel == LSMPS_KB_NBR_COMPACT)
+            k_slots_compact<<<(unsigned)((8ull * n + 255) / 256), 256, 0, s>>>(n, ctx->maxn, slots,
+                                                                               ctx->nbr_row.get<int>(),
+                                                                               ctx->nbr_col.get<int>());
+        else if (kernel == LSMPS_KB_NBR_COUNT)
             k_seg_pass<false><<<seg_grid, SEG_THREADS, 0, s>>>(
                 sg, seg_list, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(), ctx->scell.get<int>(),
                 ctx->stype.get<uint8_t>(), ctx->re2, ctx->maxn, ctx->l0, 0, ctx->nbr_cnt.get<int>(), trunc_d, nullptr,
@@ -765,7 +983,12 @@ void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* b
     // the count pass writes 4 B per particle, the fill pass reads types and row pointers and
     // writes the columns and classes
     double N = (double)n, P = (double)ctx->pairs, cells = (double)ctx->ncells;
-    *bytes = kernel == LSMPS_KB_NBR_COUNT ? 32.0 * N + 4.0 * cells : 34.0 * N + 4.0 * P + 4.0 * cells;
+    if (kernel == LSMPS_KB_NBR_SCAN)  // + scell, types, counts, kept slots, classes
+        *bytes = 24.0 * N + 4.0 * N + 1.0 * N + 4.0 * N + 4.0 * P + 1.0 * N + 4.0 * cells;
+    else if (kernel == LSMPS_KB_NBR_COMPACT)  // row pointers, the kept slots read and the CSR written
+        *bytes = 4.0 * (N + 1) + 8.0 * P;
+    else
+        *bytes = kernel == LSMPS_KB_NBR_COUNT ? 32.0 * N + 4.0 * cells : 34.0 * N + 4.0 * P + 4.0 * cells;
 }
 
 void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out) {

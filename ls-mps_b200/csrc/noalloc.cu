@@ -11,7 +11,6 @@
 // partial sums.
 #include <algorithm>
 #include <climits>
-#include <mutex>
 
 #include "ops.cuh"
 
@@ -24,27 +23,20 @@ constexpr int NA_MAX_VEC = 8;     // vectors per call
 constexpr int NA_SLOTS = NA_MAX_VEC + 1;  // |r_v|^2 for each vector, then |b|^2
 constexpr int NA_TICKET = NA_SLOTS * NA_GRID;  // double offset of the ticket word
 constexpr int NA_DOUBLES = NA_TICKET + 32;     // 42,880 bytes
-constexpr int NA_MAX_DEVICES = 64;
 
 // Slot s of block k at [s * NA_GRID + k]; the ticket (an unsigned int) at [NA_TICKET]. The
 // ticket must be zero when a launch starts: the host clears it before every launch and the
 // last block clears it again. The partial sums need no initial value.
 static __device__ __align__(256) double g_residual_scratch[NA_DOUBLES];
 
-std::mutex g_addr_mu;
-double* g_addr[NA_MAX_DEVICES] = {};
-
-// Device address of the scratch on `device`, resolved once per device. The first
-// resolution may load this module onto the device.
+// Device address of the scratch on the current device (`device`), resolved on every call:
+// the lookup allocates nothing, and a cached address would go stale after a device reset or
+// a re-created primary context. The first lookup on a device may load this module onto it.
 double* scratch_address(int device) {
-    LSMPS_REQUIRE(device >= 0 && device < NA_MAX_DEVICES, LSMPS_ERR_ARG, "device ordinal beyond 63");
-    std::lock_guard<std::mutex> lock(g_addr_mu);
-    if (!g_addr[device]) {
-        void* p = nullptr;
-        LSMPS_CUDA(cudaGetSymbolAddress(&p, g_residual_scratch));
-        g_addr[device] = static_cast<double*>(p);
-    }
-    return g_addr[device];
+    LSMPS_REQUIRE(device >= 0, LSMPS_ERR_ARG, "negative device ordinal");
+    void* p = nullptr;
+    LSMPS_CUDA(cudaGetSymbolAddress(&p, g_residual_scratch));
+    return static_cast<double*>(p);
 }
 
 // One warp per row (grid-stride); lane 0 accumulates (b_i - (A p_v)_i)^2 and b_i^2, the

@@ -30,7 +30,7 @@ void nb_update_positions(lsmps_ctx* ctx, const double* xyz, size_t n, bool devic
 // wls.cu
 void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
 void wls_download(lsmps_ctx* ctx, double* x, int32_t* status, double* z, double* wsum);
-void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out);
+void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out, bool mirror_walls = false);
 void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* so,
                      double* d_vel_out, double* d_pressure, lsmps_projection_stats* out);
 

@@ -11,8 +11,9 @@
 // Each row holds its neighbors that are unknowns in neighbor-list order and the
 // diagonal last, like the reference (src/lsmps.cpp:40-57).
 //
-// Two passes, one thread per row: count (row lengths, scan -> row pointers), then fill
-// (columns, values, p*, and b = A p* in entry order). The reference variant uses exactly
+// One pass over the rows (a group of lanes per row) computes every coefficient once and
+// writes the kept entries, p*, b = A p* in entry order and D^-1; a pack kernel moves the
+// rows into the CSR after the row lengths are scanned. The reference variant uses exactly
 // rounded FP64 operations in the reference's order, so its CSR values and b are
 // bit-identical to the reference.
 #include <cmath>
@@ -27,6 +28,7 @@ struct PpeParams {
     int variant;
     double re, l0, shift;
     int pinned_ref;  // reference variant: the unknown of rank 0 is an identity row
+    int neumann;     // WLS rows: wall neighbors take the row's own value (no entry, no diagonal term)
 };
 
 __global__ void k_elig_orig(const int* __restrict__ iperm, const uint8_t* __restrict__ cls, size_t n,
@@ -91,128 +93,149 @@ __device__ __forceinline__ bool row_coeff(const PpeParams& P, double xi, double 
 
 __device__ __forceinline__ bool wls_row_valid(int st) { return st == 0 || st == 1; }
 
-// Count pass: entries per row (diagonal included).
-__global__ void k_ppe_count(PpeParams P, long long U, const int* __restrict__ sorted_of_u,
-                            const int* __restrict__ ref_of_u, const int* __restrict__ uidx,
-                            const double* __restrict__ sx, const double* __restrict__ sy,
-                            const double* __restrict__ sz, const int* __restrict__ row,
-                            const int* __restrict__ col, const int* __restrict__ wst,
-                            const double* __restrict__ wz, const double* __restrict__ wws,
-                            int* __restrict__ cnt) {
-    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (u >= U) return;
-    int k = sorted_of_u[u];
-    if (P.variant == LSMPS_PPE_REFERENCE && ref_of_u[u] == P.pinned_ref) { cnt[u] = 1; return; }
-    if (P.variant == LSMPS_PPE_WLS && !wls_row_valid(wst[k])) { cnt[u] = 1; return; }
-    double xi = sx[k], yi = sy[k], zi = sz[k];
+// p*(x) of the variant at one particle (reference: x^2 + y^2, src/lsmps.cpp:29; otherwise
+// the smooth manufactured field), the same expression for a row's own value and its
+// neighbors' so that b = A p* is computed from the entries as they are written.
+__device__ __forceinline__ double exact_p(int variant, double x, double y, double z) {
+    return variant == LSMPS_PPE_REFERENCE ? xadd(xmul(x, x), xmul(y, y)) : sin(0.3 * x) * cos(0.2 * y) + 0.1 * z;
+}
+
+// One pass over the rows, PPE_G lanes per row: the lanes of a row's group take its neighbors
+// PPE_G at a time and compute their coefficients; every lane then replays the group's
+// coefficients in neighbor order, so the diagonal and b = A p* are the sequential sums of
+// the reference's order (exact FP64 operations), identical in all lanes. Kept off-diagonal
+// entries go, in order, to the row's slot range at nbr_row[k] + k (room for every neighbor
+// plus the diagonal); k_ppe_pack moves them into the CSR once the row lengths are scanned.
+// Writes cnt[u] (entries with the diagonal), p*[u], b[u], D^-1[u].
+// stats (u64): [0] neumann, [1] failed rows.
+constexpr int PPE_G = 8;
+__global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, const int* __restrict__ sorted_of_u,
+                                                  const int* __restrict__ ref_of_u, const int* __restrict__ uidx,
+                                                  const double* __restrict__ sx, const double* __restrict__ sy,
+                                                  const double* __restrict__ sz, const uint8_t* __restrict__ cls,
+                                                  const int* __restrict__ row, const int* __restrict__ col,
+                                                  const int* __restrict__ wst, const double* __restrict__ wz,
+                                                  const double* __restrict__ wws, int* __restrict__ cnt,
+                                                  int* __restrict__ scol, double* __restrict__ sval,
+                                                  double* __restrict__ xexact, double* __restrict__ b,
+                                                  double* __restrict__ dinv, unsigned long long* stats) {
+    const int lane = threadIdx.x & 31, sub = lane & (PPE_G - 1), gbase = lane & ~(PPE_G - 1);
+    const long long u = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / PPE_G;
+    const bool live = u < U;
+    int k = 0, e0 = 0, e1 = 0;
+    bool pinned = false, identity = false;
+    double xi = 0, yi = 0, zi = 0, ws = 0;
+    if (live) {
+        k = sorted_of_u[u];
+        xi = sx[k], yi = sy[k], zi = sz[k];
+        pinned = P.variant == LSMPS_PPE_REFERENCE && ref_of_u[u] == P.pinned_ref;
+        identity = P.variant == LSMPS_PPE_WLS && !wls_row_valid(wst[k]);
+        if (!pinned && !identity) e0 = row[k], e1 = row[k + 1];
+    }
     double zk[K];
-    double ws = 0;
-    if (P.variant == LSMPS_PPE_WLS) {
+#pragma unroll
+    for (int a = 0; a < K; ++a) zk[a] = 0.0;
+    if (live && P.variant == LSMPS_PPE_WLS && !pinned && !identity) {
 #pragma unroll
         for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a];
         ws = wws[k];
     }
-    int c = 0;
-    double diag = 0.0;
-    for (int e = row[k]; e < row[k + 1]; ++e) {
-        int m = col[e];
-        bool is_u = uidx[m] >= 0;
-        if (P.variant != LSMPS_PPE_WLS && !is_u) continue;
-        double a;
-        if (!row_coeff(P, xi, yi, zi, sx[m], sy[m], sz[m], zk, ws, a)) continue;
-        diag = xadd(diag, a);
-        if (is_u) ++c;
-    }
-    // WLS rows without a positive, finite diagonal become identity rows (same test in fill)
-    if (P.variant == LSMPS_PPE_WLS && !(diag > 0 && isfinite(diag))) c = 0;
-    cnt[u] = c + 1;
-}
-
-// Fill pass. stats (u64): [0] neumann, [1] failed rows.
-__global__ void k_ppe_fill(PpeParams P, long long U, const int* __restrict__ sorted_of_u,
-                           const int* __restrict__ ref_of_u, const int* __restrict__ uidx,
-                           const double* __restrict__ sx, const double* __restrict__ sy,
-                           const double* __restrict__ sz, const uint8_t* __restrict__ cls,
-                           const int* __restrict__ row, const int* __restrict__ col,
-                           const int* __restrict__ wst, const double* __restrict__ wz,
-                           const double* __restrict__ wws, const int* __restrict__ arow,
-                           int* __restrict__ acol, double* __restrict__ aval, double* __restrict__ xexact,
-                           unsigned long long* stats) {
-    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    int neumann = 0, failed = 0;
-    if (u < U) {
-        int k = sorted_of_u[u];
-        double xi = sx[k], yi = sy[k], zi = sz[k];
-        xexact[u] = P.variant == LSMPS_PPE_REFERENCE ? xadd(xmul(xi, xi), xmul(yi, yi))
-                                                     : sin(0.3 * xi) * cos(0.2 * yi) + 0.1 * zi;
-        int o = arow[u], oe = arow[u + 1];
-        bool pinned = P.variant == LSMPS_PPE_REFERENCE && ref_of_u[u] == P.pinned_ref;
-        if (pinned) {
-            acol[o] = (int)u;
-            aval[o] = 1.0;
-        } else {
-            double diag = 0.0;
-            bool identity = P.variant == LSMPS_PPE_WLS && !wls_row_valid(wst[k]);
-            if (!identity) {
-                double zk[K];
-                double ws = 0;
-                if (P.variant == LSMPS_PPE_WLS) {
+    const long long sbase = live ? (long long)row[k] + k : 0;  // the row's slot range
+    // the warp walks the longest of its groups' rows; shorter rows idle (flags stay 0)
+    const int chunks = __reduce_max_sync(0xffffffffu, (e1 - e0 + PPE_G - 1) / PPE_G);
+    double diag = 0.0, bsum = 0.0;
+    int written = 0;
+    for (int c = 0; c < chunks; ++c) {
+        const int e = e0 + c * PPE_G + sub;
+        bool contrib = false, keep = false;
+        double a = 0.0, xem = 0.0;
+        int cj = -1;
+        if (e < e1) {
+            const int m = col[e];
+            cj = uidx[m];
+            if ((P.variant == LSMPS_PPE_WLS || cj >= 0) && !(P.neumann && cls[m] == LSMPS_WALL)) {
+                const double xm = sx[m], ym = sy[m], zm = sz[m];
+                contrib = row_coeff(P, xi, yi, zi, xm, ym, zm, zk, ws, a);
+                keep = contrib && cj >= 0;
+                if (keep) xem = exact_p(P.variant, xm, ym, zm);
+            }
+        }
+        const unsigned kb = (__ballot_sync(0xffffffffu, keep) >> gbase) & ((1u << PPE_G) - 1u);
+        if (keep) {
+            const long long p = sbase + written + __popc(kb & ((1u << sub) - 1u));
+            scol[p] = cj;
+            sval[p] = -a;
+        }
+        written += __popc(kb);
+        // the group's coefficients in neighbor order: diagonal and b as sequential sums
 #pragma unroll
-                    for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a];
-                    ws = wws[k];
-                }
-                int p = o;
-                for (int e = row[k]; e < row[k + 1]; ++e) {
-                    int m = col[e];
-                    int cj = uidx[m];
-                    if (P.variant != LSMPS_PPE_WLS && cj < 0) continue;
-                    double a;
-                    if (!row_coeff(P, xi, yi, zi, sx[m], sy[m], sz[m], zk, ws, a)) continue;
-                    diag = xadd(diag, a);
-                    if (cj >= 0 && p < oe - 1) {  // the count pass sized the row
-                        acol[p] = cj;
-                        aval[p] = -a;
-                        ++p;
-                    }
-                }
-                if (P.variant == LSMPS_PPE_WLS && oe - o == 1) {
-                    // count pass found no positive finite diagonal, or only Dirichlet neighbors
-                    if (!(diag > 0 && isfinite(diag))) identity = true;
-                }
-                if (P.variant != LSMPS_PPE_REFERENCE) diag = diag * (1.0 + P.shift);
-            }
-            if (identity) {
-                failed = 1;
-                diag = 1.0;
-            } else if (diag <= 0 || !isfinite(diag)) {  // src/lsmps.cpp:52
-                failed = 1;
-                diag = 1.0;
-            }
-            acol[oe - 1] = (int)u;
-            aval[oe - 1] = diag;
-            if (cls[k] == LSMPS_NEAR_WALL) neumann = 1;
+        for (int j = 0; j < PPE_G; ++j) {
+            const double aj = __shfl_sync(0xffffffffu, a, gbase + j);
+            const double xj = __shfl_sync(0xffffffffu, xem, gbase + j);
+            const int fj = __shfl_sync(0xffffffffu, (contrib ? 1 : 0) | (keep ? 2 : 0), gbase + j);
+            if (fj & 1) diag = xadd(diag, aj);
+            if (fj & 2) bsum = xadd(bsum, xmul(-aj, xj));
         }
     }
+    int neumann = 0, failed = 0;
+    if (live) {
+        const double xe = exact_p(P.variant, xi, yi, zi);
+        int c = written;
+        if (pinned) {
+            c = 0;
+            diag = 1.0;
+            bsum = 0.0;
+        } else {
+            // WLS rows without a positive, finite diagonal become identity rows
+            if (P.variant == LSMPS_PPE_WLS && !identity && !(diag > 0 && isfinite(diag))) identity = true;
+            if (identity) {
+                c = 0;
+                bsum = 0.0;
+                failed = 1;
+                diag = 1.0;
+            } else {
+                if (P.variant != LSMPS_PPE_REFERENCE) diag = diag * (1.0 + P.shift);
+                if (diag <= 0 || !isfinite(diag)) {  // src/lsmps.cpp:52
+                    failed = 1;
+                    diag = 1.0;
+                }
+            }
+            if (cls[k] == LSMPS_NEAR_WALL) neumann = 1;
+        }
+        if (sub == 0) {
+            scol[sbase + c] = (int)u;
+            sval[sbase + c] = diag;
+            cnt[u] = c + 1;
+            xexact[u] = xe;
+            b[u] = xadd(bsum, xmul(diag, xe));
+            dinv[u] = 1.0 / diag;
+        }
+    }
+    if (sub != 0) neumann = failed = 0;
     neumann = __reduce_add_sync(0xffffffffu, neumann);
     failed = __reduce_add_sync(0xffffffffu, failed);
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         if (neumann) atomicAdd(&stats[0], (unsigned long long)neumann);
         if (failed) atomicAdd(&stats[1], (unsigned long long)failed);
     }
 }
 
-// b = A p* in entry order (src/lsmps.cpp:59-61); also the inverse diagonal for Jacobi.
-__global__ void k_ppe_rhs(long long U, const int* __restrict__ arow, const int* __restrict__ acol,
-                          const double* __restrict__ aval, const double* __restrict__ xexact,
-                          double* __restrict__ b, double* __restrict__ dinv) {
-    long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+// Moves each row's slot range into the CSR (PPE_G lanes per row, coalesced).
+__global__ void __launch_bounds__(256) k_ppe_pack(long long U, const int* __restrict__ sorted_of_u,
+                                                  const int* __restrict__ nrow, const int* __restrict__ arow,
+                                                  const int* __restrict__ scol, const double* __restrict__ sval,
+                                                  int* __restrict__ acol, double* __restrict__ aval) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long u = g / PPE_G;
+    const int sub = (int)(g % PPE_G);
     if (u >= U) return;
-    double s = 0;
-    int e0 = arow[u], e1 = arow[u + 1];
-    for (int e = e0; e < e1; ++e) s = xadd(s, xmul(aval[e], xexact[acol[e]]));
-    b[u] = s;
-    double d = aval[e1 - 1];
-    dinv[u] = d != 0.0 ? 1.0 / d : 1.0;
+    const int k = sorted_of_u[u];
+    const long long sb = (long long)nrow[k] + k;
+    const int o = arow[u], c = arow[u + 1] - o;
+    for (int p = sub; p < c; p += PPE_G) {
+        acol[o + p] = __ldcs(scol + sb + p);
+        aval[o + p] = __ldcs(sval + sb + p);
+    }
 }
 
 // ---- download in the reference numbering ----
@@ -285,40 +308,43 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
                                                              ref_of_u, u_of_ref);
         LSMPS_CHECK_LAUNCH();
     }
-    PpeParams P{o->variant, o->re, o->l0, o->diag_shift, 0};
+    LSMPS_REQUIRE((o->flags & ~LSMPS_PPE_WALL_NEUMANN) == 0 &&
+                      (!(o->flags & LSMPS_PPE_WALL_NEUMANN) || o->variant == LSMPS_PPE_WLS),
+                  LSMPS_ERR_ARG, "PPE flags: LSMPS_PPE_WALL_NEUMANN is for the WLS variant");
+    const int neumann = (o->flags & LSMPS_PPE_WALL_NEUMANN) ? 1 : 0;
+    PpeParams P{o->variant, o->re, o->l0, o->diag_shift, 0, neumann};
     int* cnt = ctx->vtmp.ensure<int>(U + 1);
     int* arow = ctx->A_row.ensure<int>(U + 1);
     const int* wst = ctx->have_wls ? ctx->wls_status.get<int>() : nullptr;
     const double* wz = ctx->have_wls ? ctx->wls_z.get<double>() : nullptr;
     const double* wws = ctx->have_wls ? ctx->wls_wsum.get<double>() : nullptr;
-    if (U) {
-        k_ppe_count<<<blocks_for(U, 128), 128, 0, s>>>(P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(),
-                                                       ctx->sy.get<double>(), ctx->sz.get<double>(),
-                                                       ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), wst, wz,
-                                                       wws, cnt);
-        LSMPS_CHECK_LAUNCH();
-    }
-    scan_exclusive<int>(cnt, arow, U, s, ctx->scan_tmp, dflag);
-    int hnnz = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hnnz, arow + U, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "PPE row count");
-    const long long nnz = hnnz;
-    int* acol = ctx->A_col.ensure<int>(nnz + 1);
-    double* aval = ctx->A_val.ensure<double>(nnz + 1);
+    // slot ranges: a row of sorted particle k at nbr_row[k] + k, room for its neighbors and the diagonal
+    const size_t slots = (size_t)ctx->pairs + n + 1;
+    int* scol = ctx->A_slot_col.ensure<int>(slots);
+    double* sval = ctx->A_slot_val.ensure<double>(slots);
     double* xe = ctx->A_xexact.ensure<double>(U + 1);
     double* b = ctx->A_b.ensure<double>(U + 1);
     double* dinv = ctx->A_dinv.ensure<double>(U + 1);
     auto* st = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 32);
     LSMPS_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), s));
     if (U) {
-        k_ppe_fill<<<blocks_for(U, 128), 128, 0, s>>>(P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(),
-                                                      ctx->sy.get<double>(), ctx->sz.get<double>(),
-                                                      ctx->cls.get<uint8_t>(), ctx->nbr_row.get<int>(),
-                                                      ctx->nbr_col.get<int>(), wst, wz, wws, arow, acol, aval,
-                                                      xe, st);
+        k_ppe_rows<<<blocks_for((size_t)U * PPE_G, 128), 128, 0, s>>>(
+            P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
+            ctx->cls.get<uint8_t>(), ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), wst, wz, wws, cnt, scol, sval,
+            xe, b, dinv, st);
         LSMPS_CHECK_LAUNCH();
-        k_ppe_rhs<<<blocks_for(U, 256), 256, 0, s>>>(U, arow, acol, aval, xe, b, dinv);
+    }
+    scan_exclusive<int>(cnt, arow, U, s, ctx->scan_tmp, dflag);
+    int hnnz = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&hnnz, arow + U, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    check_device_flags(ctx, "PPE rows");
+    const long long nnz = hnnz;
+    int* acol = ctx->A_col.ensure<int>(nnz + 1);
+    double* aval = ctx->A_val.ensure<double>(nnz + 1);
+    if (U) {
+        k_ppe_pack<<<blocks_for((size_t)U * PPE_G, 256), 256, 0, s>>>(U, sorted_of_u, ctx->nbr_row.get<int>(), arow,
+                                                                      scol, sval, acol, aval);
         LSMPS_CHECK_LAUNCH();
     }
     ev_record(ctx, 9);
@@ -336,6 +362,7 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     ctx->U = U;
     ctx->nnz = nnz;
     ctx->ppe_variant = o->variant;
+    ctx->ppe_wall_neumann = neumann != 0;
     ctx->ppe_loaded = false;
     ctx->have_ppe = true;
     ctx->have_solution = false;

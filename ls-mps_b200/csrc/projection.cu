@@ -29,20 +29,28 @@ __global__ void k_unknown_mask(long long U, const int* __restrict__ sorted_of_u,
         mask[perm[sorted_of_u[u]]] = 1;
 }
 
-// hop[k] (sorted order) = HOP_FAR for Interior unknowns, 0 for every other particle (boundary:
-// free surface, splash, wall, near-wall); then three passes of hop = min(hop, 1 + min over
-// neighbors) (hop counts up to 3 are exact)
+// Neighbor-hop distances (sorted order) from a seed set, exact up to 3: seed particles 0,
+// the others HOP_FAR, then three passes of hop = min(hop, 1 + min over neighbors). Seeds:
+//   SEED_BOUNDARY  every particle but the Interior unknowns (free surface, splash, wall, near-wall)
+//   SEED_SURFACE   free-surface and splash particles
+//   SEED_WALL      wall particles
 constexpr uint8_t HOP_FAR = 255;
-__global__ void k_hop_init(long long U, const int* __restrict__ sorted_of_u, size_t n, uint8_t* __restrict__ hop) {
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-        hop[k] = 0;
-}
-__global__ void k_hop_mark(long long U, const int* __restrict__ sorted_of_u, const uint8_t* __restrict__ cls,
+enum { SEED_BOUNDARY = 0, SEED_SURFACE = 1, SEED_WALL = 2 };
+__global__ void k_hop_seed(size_t n, int mode, const uint8_t* __restrict__ cls, const uint8_t* __restrict__ isu,
                            uint8_t* __restrict__ hop) {
-    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < U; u += (long long)gridDim.x * blockDim.x) {
-        const int k = sorted_of_u[u];
-        if (cls[k] == LSMPS_INTERIOR) hop[k] = HOP_FAR;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const uint8_t c = cls[k];
+        bool seed;
+        if (mode == SEED_BOUNDARY) seed = !(isu[k] && c == LSMPS_INTERIOR);
+        else if (mode == SEED_SURFACE) seed = c == LSMPS_FREE_SURFACE || c == LSMPS_SPLASH;
+        else seed = c == LSMPS_WALL;
+        hop[k] = seed ? 0 : HOP_FAR;
     }
+}
+// isu[k] = 1 for the sorted particles that are unknowns
+__global__ void k_unknown_sorted(long long U, const int* __restrict__ sorted_of_u, uint8_t* __restrict__ isu) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < U; u += (long long)gridDim.x * blockDim.x)
+        isu[sorted_of_u[u]] = 1;
 }
 __global__ void k_hop_pass(size_t n, const int* __restrict__ row, const int* __restrict__ col,
                            const uint8_t* __restrict__ in, uint8_t* __restrict__ out) {
@@ -52,19 +60,30 @@ __global__ void k_hop_pass(size_t n, const int* __restrict__ row, const int* __r
         out[k] = (uint8_t)h;
     }
 }
-// mask[i] (caller order): bit 0 unknown, bit 1 core (at least three hops from a non-unknown)
-__global__ void k_core_mask(size_t n, const int* __restrict__ iperm, const uint8_t* __restrict__ hop,
-                            uint8_t* __restrict__ mask) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        if (mask[i] && hop[iperm[i]] >= 3) mask[i] |= 2;
+// mask[i] (caller order): bit 0 unknown, bit 1 core (at least three hops from any boundary
+// particle), bit 2 wall band 1 and bit 3 wall band 2 (unknowns one / two hops from a wall and
+// at least three from the free surface)
+__global__ void k_region_mask(size_t n, const int* __restrict__ iperm, const uint8_t* __restrict__ hb,
+                              const uint8_t* __restrict__ hs, const uint8_t* __restrict__ hw,
+                              uint8_t* __restrict__ mask) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!mask[i]) continue;
+        const int k = iperm[i];
+        uint8_t m = mask[i];
+        if (hb[k] >= 3) m |= 2;
+        if (hs[k] >= 3 && hw[k] == 1) m |= 4;
+        if (hs[k] >= 3 && hw[k] == 2) m |= 8;
+        mask[i] = m;
+    }
 }
 
 // div[i] = d u_x / dx + d u_y / dy + d u_z / dz from the WLS solutions of the three fields;
-// stats: [0] sum div^2, [1] max |div| (bits), [2] count over the unknowns, [3] sum div^2 over
-// the core, [4] count over the core
+// stats: [0] sum div^2, [1] max |div| (bits), [2] count over the unknowns, then sum div^2 and
+// count over the core [3, 4], wall band 1 [5, 6] and wall band 2 [7, 8]
 __global__ void k_divergence(size_t n, const double* __restrict__ G, const uint8_t* __restrict__ mask,
                              double* __restrict__ div, double* stats) {
-    double s2 = 0, mx = 0, cnt = 0, c2 = 0, ccnt = 0;
+    double s2 = 0, mx = 0, cnt = 0;
+    double rs[3] = {0, 0, 0}, rc[3] = {0, 0, 0};  // core, wall band 1, wall band 2
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const double* g = G + i * 3 * KB;
         const double d = g[0] + g[KB + 1] + g[2 * KB + 2];
@@ -74,22 +93,30 @@ __global__ void k_divergence(size_t n, const double* __restrict__ G, const uint8
             mx = fmax(mx, fabs(d));
             cnt += 1;
         }
-        if (mask[i] & 2) {
-            c2 += d * d;
-            ccnt += 1;
-        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            if (mask[i] & (2 << r)) {
+                rs[r] += d * d;
+                rc[r] += 1;
+            }
     }
     s2 = warp_sum(s2);
     cnt = warp_sum(cnt);
-    c2 = warp_sum(c2);
-    ccnt = warp_sum(ccnt);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        rs[r] = warp_sum(rs[r]);
+        rc[r] = warp_sum(rc[r]);
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&stats[0], s2);
         atomicAdd(&stats[2], cnt);
-        atomicAdd(&stats[3], c2);
-        atomicAdd(&stats[4], ccnt);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            atomicAdd(&stats[3 + 2 * r], rs[r]);
+            atomicAdd(&stats[4 + 2 * r], rc[r]);
+        }
         atomicMax(reinterpret_cast<unsigned long long*>(&stats[1]), (unsigned long long)__double_as_longlong(mx));
     }
 }
@@ -133,26 +160,32 @@ void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho,
     double* G = ctx->pj_grad.ensure<double>(n * 3 * KB + 1);
     double* div = ctx->pj_div.ensure<double>(n + 1);
     uint8_t* mask = ctx->pj_mask.ensure<uint8_t>(n + 1);
-    double* stats = ctx->pj_stats.ensure<double>(16);
+    double* stats = ctx->pj_stats.ensure<double>(32);
     const long long U = ctx->U;
+    const bool neumann = ctx->ppe_wall_neumann;
     LSMPS_CUDA(cudaMemsetAsync(mask, 0, n + 1, s));
-    LSMPS_CUDA(cudaMemsetAsync(stats, 0, 16 * sizeof(double), s));
+    LSMPS_CUDA(cudaMemsetAsync(stats, 0, 32 * sizeof(double), s));
     if (U) {
         k_unknown_mask<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), ctx->perm.get<int>(), mask);
-        uint8_t* hop = ctx->pj_hop.ensure<uint8_t>(2 * n + 2);
-        uint8_t* hop2 = hop + n + 1;
-        k_hop_init<<<grid_n(n), 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), n, hop);
-        k_hop_mark<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), ctx->cls.get<uint8_t>(), hop);
-        for (int pass = 0; pass < 3; ++pass) {
-            k_hop_pass<<<grid_n(n), 256, 0, s>>>(n, ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(),
-                                                 pass % 2 ? hop2 : hop, pass % 2 ? hop : hop2);
+        uint8_t* hop = ctx->pj_hop.ensure<uint8_t>(5 * (n + 1));
+        uint8_t* isu = hop + 3 * (n + 1);
+        uint8_t* tmp = isu + (n + 1);
+        LSMPS_CUDA(cudaMemsetAsync(isu, 0, n + 1, s));
+        k_unknown_sorted<<<1184, 256, 0, s>>>(U, ctx->sorted_of_u.get<int>(), isu);
+        for (int mode = 0; mode < 3; ++mode) {  // three passes ping-pong between tmp and the result
+            uint8_t* h = hop + mode * (n + 1);
+            k_hop_seed<<<grid_n(n), 256, 0, s>>>(n, mode, ctx->cls.get<uint8_t>(), isu, h);
+            for (int pass = 0; pass < 3; ++pass)
+                k_hop_pass<<<grid_n(n), 256, 0, s>>>(n, ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(),
+                                                     pass % 2 ? tmp : h, pass % 2 ? h : tmp);
+            LSMPS_CUDA(cudaMemcpyAsync(h, tmp, n, cudaMemcpyDeviceToDevice, s));  // after an odd pass count
         }
-        k_core_mask<<<grid_n(n), 256, 0, s>>>(n, ctx->iperm.get<int>(), hop2, mask);
-        note_launches(6);
+        k_region_mask<<<grid_n(n), 256, 0, s>>>(n, ctx->iperm.get<int>(), hop, hop + (n + 1), hop + 2 * (n + 1), mask);
+        note_launches(15);
         LSMPS_CHECK_LAUNCH();
     }
     // 1. div u*
-    wls_fields(ctx, d_vel, 3, G);
+    wls_fields(ctx, d_vel, 3, G, neumann);
     if (n) {
         k_divergence<<<grid_n(n), 256, 0, s>>>(n, G, mask, div, stats);
         LSMPS_CHECK_LAUNCH();
@@ -172,31 +205,38 @@ void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho,
     }
     // 3. u = u* - dt / rho grad p
     double* Gp = ctx->pj_gradp.ensure<double>(n * KB + 1);
-    wls_fields(ctx, d_pressure, 1, Gp);
+    wls_fields(ctx, d_pressure, 1, Gp, neumann);
     if (n) {
         k_correct<<<grid_n(n), 256, 0, s>>>(n, ctx->type_in.get<uint8_t>(), d_vel, Gp, dt / rho, d_vel_out);
         LSMPS_CHECK_LAUNCH();
     }
     // 4. div u
-    wls_fields(ctx, d_vel_out, 3, G);
+    wls_fields(ctx, d_vel_out, 3, G, neumann);
     if (n) {
-        k_divergence<<<grid_n(n), 256, 0, s>>>(n, G, mask, nullptr, stats + 8);
+        k_divergence<<<grid_n(n), 256, 0, s>>>(n, G, mask, nullptr, stats + 16);
         LSMPS_CHECK_LAUNCH();
     }
     ev_record(ctx, 13);
-    double h[16];
+    double h[32];
     LSMPS_CUDA(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, s));
     LSMPS_CUDA(cudaStreamSynchronize(s));
     const double cnt = std::max(h[2], 1.0), ccnt = std::max(h[4], 1.0);
+    const double w1 = std::max(h[6], 1.0), w2 = std::max(h[8], 1.0);
     st.unknowns = (uint64_t)U;
     st.measured = (uint64_t)h[2];
     st.div_before_rms = std::sqrt(h[0] / cnt);
     st.div_before_max = h[1];
-    st.div_after_rms = std::sqrt(h[8] / cnt);
-    st.div_after_max = h[9];
+    st.div_after_rms = std::sqrt(h[16] / cnt);
+    st.div_after_max = h[17];
     st.core = (uint64_t)h[4];
     st.div_core_before_rms = std::sqrt(h[3] / ccnt);
-    st.div_core_after_rms = std::sqrt(h[11] / ccnt);
+    st.div_core_after_rms = std::sqrt(h[19] / ccnt);
+    st.wall_band1 = (uint64_t)h[6];
+    st.wall_band2 = (uint64_t)h[8];
+    st.div_wall1_before_rms = std::sqrt(h[5] / w1);
+    st.div_wall1_after_rms = std::sqrt(h[21] / w1);
+    st.div_wall2_before_rms = std::sqrt(h[7] / w2);
+    st.div_wall2_after_rms = std::sqrt(h[23] / w2);
     st.iterations = ps.iterations;
     st.converged = ps.converged;
     st.relative_residual = ps.relative_residual;

@@ -965,15 +965,17 @@ struct LoopCtl {
     int replacements, restarts, fallback;
     int act;            // 0 none, 1 replace, 2 restart: gates the replacement and init kernels
     int final_replace;  // the pending replacement ends the solve (iteration cap)
-    int state;          // 0 running, 1 converged, 2 failed, 3 iteration cap
+    int state;          // 0 running, 1 converged, 2 failed, 3 iteration cap, 4 multigrid gave up
     int trips, max_trips, max_iter, use_nn;
+    int use_mg;         // the body applies the multigrid: a breakdown or stall ends it (state 4)
+    int stall;          // stall window of the restarted runs (multigrid only)
 };
 
 // as set_scalar_caps on the host: a fresh scalar block with the remaining iteration budget
-__device__ void restart_caps(BcgScalars* S, int max_iter) {
+__device__ void restart_caps(BcgScalars* S, int max_iter, int stall) {
     BcgScalars z{};
     z.max_iter = max_iter;
-    z.stall_window = 0;
+    z.stall_window = stall;
     *S = z;
 }
 
@@ -993,12 +995,16 @@ __global__ void k_mix_after_chunk(BcgScalars* S, LoopCtl* C) {
         C->final_replace = 0;
         return;
     }
+    if (C->use_mg && (why == 2 || why == 4)) {  // the multigrid broke down or stalled: host falls back
+        C->state = 4;
+        return;
+    }
     if (why == 4 && C->use_nn) C->fallback = 1;
     if (S->nonfinite) {
         C->state = 2;
         return;
     }
-    restart_caps(S, C->max_iter - C->total);
+    restart_caps(S, C->max_iter - C->total, C->stall);
     C->act = 2;
 }
 
@@ -1016,11 +1022,15 @@ __global__ void k_mix_after_replace(BcgScalars* S, LoopCtl* C) {
         return;
     }
     if (S->done == 0) return;
+    if (C->use_mg) {  // breakdown after the replacement with the multigrid: host falls back
+        C->state = 4;
+        return;
+    }
     if (S->nonfinite) {  // breakdown after the replacement: restart, unless non-finite
         C->state = 2;
         return;
     }
-    restart_caps(S, C->max_iter - C->total);
+    restart_caps(S, C->max_iter - C->total, C->stall);
     C->act = 2;
 }
 
@@ -1574,7 +1584,9 @@ static void solve_mixed_f32(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_pp
 // stall (LEARNED: no 1 % progress in `stall_window` iterations) or an FP32-driven
 // convergence claim the FP64 residual denies restarts the Krylov space from the current
 // iterate; LEARNED starts from the network's guess and, after a stall, continues as plain
-// Jacobi-BiCGStab (fallback).
+// Jacobi-BiCGStab (fallback). With the multigrid preconditioner a stall (no 1 % progress in
+// `stall_window` iterations) or a breakdown ends the multigrid phase, and the solve continues
+// as Jacobi MIXED from the current iterate (from zero when it is no longer finite; fallback).
 static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;
@@ -1596,10 +1608,9 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         V.ph = ctx->vph.ensure<double>(U + 1);
         V.sh = ctx->vsh.ensure<double>(U + 1);
     }
-    const uint64_t kpi = (uint64_t)launches_per_iteration(ctx, mg);
     Sell<double> As = sell_scaled64(ctx);
     Sell<float> Af = sell_scaled32(ctx);
-    set_scalar_caps(E, o->max_iter, use_nn ? stall : 0);
+    set_scalar_caps(E, o->max_iter, (use_nn || mg) ? stall : 0);
     bool have_start = warm;
     double warm_rn = 0;  // |b - A x0| of a warm start the network corrected
     if (warm) {  // the iteration works on y = D x
@@ -1635,127 +1646,158 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
         LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
     }
     init<double, double>(E, As, b, V, have_start, o->tol, -1.0);
-    cudaGraphExec_t exec = nullptr;
-    if (o->use_graph == 2) {
-        cudaGraph_t graph;
-        LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mg);
-        note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
-        cudaError_t e = cudaStreamEndCapture(s, &graph);
-        LSMPS_CUDA(e);
-        LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        cudaGraphDestroy(graph);
-    }
     auto read = [&](BcgScalars& h) {
         LSMPS_CUDA(cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, s));
         LSMPS_CUDA(cudaStreamSynchronize(s));
     };
     BcgScalars h{};
     read(h);
-    int total = 0, base = 0, replacements = 0, restarts = 0, fallback = 0;
+    int total = 0, replacements = 0, restarts = 0, fallback = 0;
     if (use_nn && !warm && (!std::isfinite(h.rn) || h.rn >= h.bnorm)) {
         // the network's guess is worse than zero: discard it and run plain Jacobi-BiCGStab
         fallback = 1;
         LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
-        set_scalar_caps(E, o->max_iter, 0);
+        set_scalar_caps(E, o->max_iter, mg ? stall : 0);
         init<double, double>(E, As, b, V, false, o->tol, -1.0);
         read(h);
     } else if (use_nn && warm && (!std::isfinite(h.rn) || h.rn >= warm_rn)) {
         // the correction made the warm start worse: go back to it
         fallback = 1;
         LSMPS_CUDA(cudaMemcpyAsync(V.x, V.p, U * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        set_scalar_caps(E, o->max_iter, 0);
+        set_scalar_caps(E, o->max_iter, mg ? stall : 0);
         init<double, double>(E, As, b, V, true, o->tol, -1.0);
         read(h);
     }
-    double rn_upd = h.rn;
     bool converged = h.done == 1, failed = h.done == 2 && h.nonfinite;
     const long long max_chunks = (long long)o->max_iter / chunk + 4 + o->max_iter;  // bounded loop
-    if (o->use_graph == 1 && !converged && !failed) {
-        // the loop below, decided on the device: one graph launch for the whole solve
-        LoopCtl* C = engine_loop_ctl(ctx);
-        LoopCtl c0{};
-        c0.rn_upd = rn_upd;
-        c0.delta = delta;
-        c0.fallback = fallback;
-        c0.max_trips = (int)std::min<long long>(max_chunks, INT_MAX);
-        c0.max_iter = o->max_iter;
-        c0.use_nn = use_nn ? 1 : 0;
-        LSMPS_CUDA(cudaMemcpyAsync(C, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
-        cudaGraphExec_t wexec = build_while_graph(s, C, [&] {
-            for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mg);
-            k_mix_after_chunk<<<1, 1, 0, s>>>(E.S, C);
-            launch_replace(s, As, b, V, E, &C->act, 1);
-            k_mix_after_replace<<<1, 1, 0, s>>>(E.S, C);
-            if (As.dcol)
-                k_bcg_init<double, double, true><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P,
-                                                                      o->tol, -1.0, &C->act, 2);
-            else
-                k_bcg_init<double, double, false><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S, E.P,
-                                                                       o->tol, -1.0, &C->act, 2);
-            k_mix_after_restart<<<1, 1, 0, s>>>(E.S, C);
-        });
-        note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
-        cudaError_t e = cudaGraphLaunch(wexec, s);
-        LoopCtl hc{};
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, C, sizeof(hc), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        cudaGraphExecDestroy(wexec);
-        LSMPS_CUDA(e);
-        note_launches((uint64_t)hc.trips * (kpi * (uint64_t)chunk + 6));
-        total = hc.total;
-        replacements = hc.replacements;
-        restarts = hc.restarts;
-        fallback = hc.fallback;
-        converged = hc.state == 1;
-        failed = hc.state == 2;
-    }
-    for (long long guard = 0; o->use_graph != 1 && !converged && !failed && guard < max_chunks; ++guard) {
-        if (!h.done) {
-            if (exec) {
-                LSMPS_CUDA(cudaGraphLaunch(exec, s));
-                note_launches(kpi * (uint64_t)chunk);
-            } else {
-                for (int k = 0; k < chunk; ++k) iteration<double, float>(E, Af, V, mg);
-                LSMPS_CHECK_LAUNCH();
+    // Iterates from the scalars in h until converged, failed or the iteration cap; with the
+    // multigrid (mgp), a breakdown or a stall ends the phase early and returns true instead
+    // (the caller then continues without it).
+    auto phase = [&](bool mgp) -> bool {
+        const uint64_t kpi = (uint64_t)launches_per_iteration(ctx, mgp);
+        const int restart_stall = mgp ? stall : 0;
+        double rn_upd = h.rn;
+        if (o->use_graph == 1) {
+            if (converged || failed) return false;
+            // the loop below, decided on the device: one graph launch for the whole solve
+            LoopCtl* C = engine_loop_ctl(ctx);
+            LoopCtl c0{};
+            c0.rn_upd = rn_upd;
+            c0.delta = delta;
+            c0.fallback = fallback;
+            c0.max_trips = (int)std::min<long long>(max_chunks, INT_MAX);
+            c0.max_iter = o->max_iter;
+            c0.total = total;
+            c0.use_nn = use_nn ? 1 : 0;
+            c0.use_mg = mgp ? 1 : 0;
+            c0.stall = restart_stall;
+            LSMPS_CUDA(cudaMemcpyAsync(C, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
+            cudaGraphExec_t wexec = build_while_graph(s, C, [&] {
+                for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mgp);
+                k_mix_after_chunk<<<1, 1, 0, s>>>(E.S, C);
+                launch_replace(s, As, b, V, E, &C->act, 1);
+                k_mix_after_replace<<<1, 1, 0, s>>>(E.S, C);
+                if (As.dcol)
+                    k_bcg_init<double, double, true><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S,
+                                                                          E.P, o->tol, -1.0, &C->act, 2);
+                else
+                    k_bcg_init<double, double, false><<<RGRID, RB, 0, s>>>(As, b, V.x, 1, V.r, V.r0, V.p, V.v, E.S,
+                                                                           E.P, o->tol, -1.0, &C->act, 2);
+                k_mix_after_restart<<<1, 1, 0, s>>>(E.S, C);
+            });
+            note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
+            cudaError_t e = cudaGraphLaunch(wexec, s);
+            LoopCtl hc{};
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, C, sizeof(hc), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&h, E.S, sizeof(h), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            cudaGraphExecDestroy(wexec);
+            LSMPS_CUDA(e);
+            note_launches((uint64_t)hc.trips * (kpi * (uint64_t)chunk + 6));
+            total = hc.total;
+            replacements += hc.replacements;
+            restarts += hc.restarts;
+            fallback = hc.fallback;
+            converged = hc.state == 1;
+            failed = hc.state == 2;
+            return hc.state == 4;
+        }
+        cudaGraphExec_t exec = nullptr;
+        if (o->use_graph == 2) {
+            cudaGraph_t graph;
+            LSMPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int c = 0; c < chunk; ++c) iteration<double, float>(E, Af, V, mgp);
+            note_launches(0 - kpi * (uint64_t)chunk);  // captured, not launched
+            cudaError_t e = cudaStreamEndCapture(s, &graph);
+            LSMPS_CUDA(e);
+            LSMPS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            cudaGraphDestroy(graph);
+        }
+        bool give_up = false;
+        int base = h.iters;
+        for (long long guard = 0; !converged && !failed && guard < max_chunks; ++guard) {
+            if (!h.done) {
+                if (exec) {
+                    LSMPS_CUDA(cudaGraphLaunch(exec, s));
+                    note_launches(kpi * (uint64_t)chunk);
+                } else {
+                    for (int k = 0; k < chunk; ++k) iteration<double, float>(E, Af, V, mgp);
+                    LSMPS_CHECK_LAUNCH();
+                }
+                read(h);
             }
+            total += h.iters - base;
+            base = h.iters;
+            if (!h.done && h.rn > delta * rn_upd) continue;
+            const int why = h.done;  // 0: drop by delta; else the iteration stopped
+            if (why == 3 || total >= o->max_iter) {
+                // iteration cap: report the true residual of the last iterate
+                launch_replace(s, As, b, V, E, nullptr, 0);
+                LSMPS_CHECK_LAUNCH();
+                read(h);
+                converged = h.done == 1;
+                break;
+            }
+            if (why == 0) {
+                launch_replace(s, As, b, V, E, nullptr, 0);
+                LSMPS_CHECK_LAUNCH();
+                ++replacements;
+                read(h);
+                rn_upd = h.rn;
+                if (h.done == 1) { converged = true; break; }
+                if (h.done == 0) continue;
+                // rho breakdown after the replacement: fall through to a restart
+            }
+            if (mgp && (h.done == 2 || h.done == 4)) { give_up = true; break; }
+            if (why == 4 && use_nn) fallback = 1;
+            if (h.nonfinite) { failed = true; break; }
+            // restart from the current iterate with the FP64 matrix (true residual)
+            set_scalar_caps(E, o->max_iter - total, restart_stall);
+            init<double, double>(E, As, b, V, true, o->tol, -1.0);
+            ++restarts;
             read(h);
-        }
-        total += h.iters - base;
-        base = h.iters;
-        if (!h.done && h.rn > delta * rn_upd) continue;
-        const int why = h.done;  // 0: drop by delta; else the iteration stopped
-        if (why == 3 || total >= o->max_iter) {
-            // iteration cap: report the true residual of the last iterate
-            launch_replace(s, As, b, V, E, nullptr, 0);
-            LSMPS_CHECK_LAUNCH();
-            read(h);
-            converged = h.done == 1;
-            break;
-        }
-        if (why == 0) {
-            launch_replace(s, As, b, V, E, nullptr, 0);
-            LSMPS_CHECK_LAUNCH();
-            ++replacements;
-            read(h);
+            base = 0;
             rn_upd = h.rn;
             if (h.done == 1) { converged = true; break; }
-            if (h.done == 0) continue;
-            // rho breakdown after the replacement: fall through to a restart
+            if (h.done) { failed = true; break; }
         }
-        if (why == 4 && use_nn) fallback = 1;
-        if (h.nonfinite) { failed = true; break; }
-        // restart from the current iterate with the FP64 matrix (true residual)
+        if (exec) cudaGraphExecDestroy(exec);
+        return give_up;
+    };
+    if (phase(mg)) {
+        // The multigrid broke down or stalled (near-singular aggregates can do this): continue
+        // as Jacobi MIXED from the current iterate, or from zero if it is no longer finite.
+        fallback = 1;
+        const bool keep_x = !h.nonfinite;
+        if (!keep_x) LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
         set_scalar_caps(E, o->max_iter - total, 0);
-        init<double, double>(E, As, b, V, true, o->tol, -1.0);
+        init<double, double>(E, As, b, V, keep_x, o->tol, -1.0);
         ++restarts;
         read(h);
-        base = 0;
-        rn_upd = h.rn;
-        if (h.done == 1) { converged = true; break; }
-        if (h.done) { failed = true; break; }
+        converged = h.done == 1;
+        failed = h.done == 2;
+        if (total < o->max_iter) phase(false);
     }
-    if (exec) cudaGraphExecDestroy(exec);
     k_unscale<<<1184, 256, 0, s>>>(U, V.x, dinv);
     LSMPS_CHECK_LAUNCH();
     ev_record(ctx, 11);

@@ -200,6 +200,7 @@ struct WlsParams {
     int nrhs;
     int precision;
     int store;
+    int mirror_walls;  // wall neighbors take the particle's own field values (zero normal gradient)
     double coef[30];  // nrhs x 10
 };
 
@@ -397,6 +398,7 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
                         fi[f] = fvals ? fvals[(size_t)k * NRHS + f] : quad_fast(P.coef + 10 * f, xi, yi, zi);
                     for (int e = row[k]; e < row[k + 1]; ++e) {
                         int m = col[e];
+                        if (P.mirror_walls && cls[m] == LSMPS_WALL) continue;  // f_m = f_k: no term
                         double xm = sx[m], ym = sy[m], zm = sz[m];
                         double dx = xm - xi, dy = ym - yi, dz = zm - zi;
                         double r = sqrt(dx * dx + dy * dy + dz * dz);
@@ -666,7 +668,7 @@ __global__ void k_solutions_to_caller(const int* __restrict__ iperm, size_t n, i
 }
 }  // namespace
 
-void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out) {
+void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out, bool mirror_walls) {
     LSMPS_REQUIRE(ctx->have_neighbors && ctx->have_classes, LSMPS_ERR_STATE,
                   "WLS of fields needs neighbor lists and classification first");
     LSMPS_REQUIRE(nrhs >= 1 && nrhs <= 3, LSMPS_ERR_ARG, "WLS of fields takes 1..3 fields");
@@ -680,6 +682,7 @@ void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out)
     P.nrhs = nrhs;
     P.precision = 0;
     P.store = 1;
+    P.mirror_walls = mirror_walls ? 1 : 0;
     double* fs = ctx->wf_in.ensure<double>(n * nrhs + 1);
     WlsOut o{ctx->wf_status.ensure<int>(n + 1), ctx->wf_z.ensure<double>(n * K + 1), ctx->wf_wsum.ensure<double>(n + 1),
              ctx->wf_x.ensure<double>(n * nrhs * K + 1)};

@@ -21,9 +21,11 @@ CLI_PATH = os.path.join(HERE, "bin", "lsmps-bench")
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_GRID, ERR_OVERFLOW, ERR_NONFINITE, ERR_TIMEOUT, ERR_IO = range(10)
 INTERIOR, FREE_SURFACE, SPLASH, NEAR_WALL, WALL = range(5)
 NBR_CLASSIFY = 1
+NBR_TWO_PASS = 2
+PPE_WALL_NEUMANN = 1
 PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
 SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED, SOLVER_MIXED_F32 = range(6)
-KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER, KB_MG_VCYCLE = range(7)
+KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER, KB_MG_VCYCLE, KB_NBR_SCAN, KB_NBR_COMPACT = range(9)
 PRECONDS = {"jacobi": 0, "multigrid": 1}
 SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4, "mixed_f32": 5}
 VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}
@@ -60,7 +62,7 @@ class WlsStats(C.Structure):
 
 
 class PpeOpts(C.Structure):
-    _fields_ = [("variant", C.c_int32), ("reserved", C.c_int32), ("max_unknowns", C.c_int64),
+    _fields_ = [("variant", C.c_int32), ("flags", C.c_int32), ("max_unknowns", C.c_int64),
                 ("re", C.c_double), ("l0", C.c_double), ("diag_shift", C.c_double)]
 
 
@@ -69,7 +71,10 @@ class ProjectionStats(C.Structure):
                 ("div_before_max", C.c_double), ("div_after_rms", C.c_double), ("div_after_max", C.c_double),
                 ("iterations", C.c_int32), ("converged", C.c_int32), ("relative_residual", C.c_double),
                 ("solve_ms", C.c_double), ("total_ms", C.c_double), ("core", C.c_uint64),
-                ("div_core_before_rms", C.c_double), ("div_core_after_rms", C.c_double)]
+                ("div_core_before_rms", C.c_double), ("div_core_after_rms", C.c_double),
+                ("wall_band1", C.c_uint64), ("wall_band2", C.c_uint64), ("div_wall1_before_rms", C.c_double),
+                ("div_wall1_after_rms", C.c_double), ("div_wall2_before_rms", C.c_double),
+                ("div_wall2_after_rms", C.c_double)]
 
 
 class SeriesParams(C.Structure):
@@ -325,10 +330,10 @@ class Context:
         self.n = len(self._types)
         self._check(self.L.lsmps_upload_particles(self.h, _p(self._xyz), _p(self._types), self.n))
 
-    def build_neighbors(self, re, max_neighbors, l0, classify=True):
+    def build_neighbors(self, re, max_neighbors, l0, classify=True, two_pass=False):
         st = NeighborStats()
-        self._check(self.L.lsmps_build_neighbors(self.h, re, max_neighbors, l0,
-                                                 NBR_CLASSIFY if classify else 0, C.byref(st)))
+        flags = (NBR_CLASSIFY if classify else 0) | (NBR_TWO_PASS if two_pass else 0)
+        self._check(self.L.lsmps_build_neighbors(self.h, re, max_neighbors, l0, flags, C.byref(st)))
         return st
 
     def classify(self, l0):
@@ -370,9 +375,9 @@ class Context:
         self._check(self.L.lsmps_wls(self.h, C.byref(o), C.byref(st)))
         return st
 
-    def ppe_assemble(self, variant, max_unknowns, re, l0, diag_shift=1e-3):
+    def ppe_assemble(self, variant, max_unknowns, re, l0, diag_shift=1e-3, wall_neumann=False):
         o = PpeOpts(variant=VARIANTS.get(variant, variant), max_unknowns=int(max_unknowns), re=re,
-                    l0=l0, diag_shift=diag_shift)
+                    l0=l0, diag_shift=diag_shift, flags=PPE_WALL_NEUMANN if wall_neumann else 0)
         st = PpeStats()
         self._check(self.L.lsmps_ppe_assemble(self.h, C.byref(o), C.byref(st)))
         self._last_ppe = st

@@ -6,7 +6,7 @@ Builds the workload of bench.py (case `mixed`, l0 = 1, re = 2.1, max_neighbors 1
 WLS-Laplacian PPE) with the library, then launches the chosen kernel `reps` times through
 lsmps_kernel_bench and prints its mean time and achieved bandwidth. Under ncu, select the
 kernel with -k (spmv32/spmv64: k_bcg_v, nbr_count: k_seg_pass<0>, nbr_fill: k_seg_pass<1>,
-wls: k_wls_all, mpnn_layer: k_layer_fwd, mg_vcycle: regex k_mg_). mpnn_layer loads --weights. --autotune prints the
+nbr_scan: k_seg_scan, nbr_compact: k_slots_compact, wls: k_wls_all, mpnn_layer: k_layer_fwd, mg_vcycle: regex k_mg_). mpnn_layer loads --weights. --autotune prints the
 launch shapes the autotuner timed and chose.
 """
 import argparse
@@ -17,8 +17,8 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import lsmps_b200 as lib  # noqa: E402
 
 KERNELS = {"spmv32": lib.KB_SPMV32, "spmv64": lib.KB_SPMV64, "nbr_count": lib.KB_NBR_COUNT,
-           "nbr_fill": lib.KB_NBR_FILL, "wls": lib.KB_WLS, "mpnn_layer": lib.KB_MPNN_LAYER,
-           "mg_vcycle": lib.KB_MG_VCYCLE}
+           "nbr_fill": lib.KB_NBR_FILL, "nbr_scan": lib.KB_NBR_SCAN, "nbr_compact": lib.KB_NBR_COMPACT,
+           "wls": lib.KB_WLS, "mpnn_layer": lib.KB_MPNN_LAYER, "mg_vcycle": lib.KB_MG_VCYCLE}
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "mpnn_rain200k.bin")
 
 
@@ -40,7 +40,13 @@ def main():
         if "mpnn_layer" in a.kernel or a.solve == "learned":
             ctx.mpnn_load(a.weights)
         ctx.upload(xyz, t)
-        ctx.build_neighbors(2.1, 128, 1.0)
+        import time
+        for rep in range(3):  # the whole build (host round trips included), warm after the first
+            t0 = time.perf_counter()
+            nst = ctx.build_neighbors(2.1, 128, 1.0)
+            t1 = time.perf_counter()
+            print(f"neighbor build {rep}: {(t1 - t0) * 1e3:.2f} ms wall, device phase {ctx.timings()[1]:.3f} ms, "
+                  f"pairs {nst.pairs}")
         ctx.wls(2.1, 1.0, mode=1)
         st = ctx.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
         print(f"particles {len(t)} unknowns {st.unknowns} nnz {st.nnz}")

@@ -2,7 +2,7 @@
 
     python ls-mps_b200/train_mpnn.py --out ls-mps_b200/weights/mpnn_rain200k.bin
 
-Data: rain-on-plate snapshots of --particles (200,000) particles, seeds
+Data (the learned-preconditioner workload): rain-on-plate snapshots of --particles (200,000) particles, seeds
 1000, 1001, ...; on each, --pairs right-hand sides b = A p* with smooth random fields p*
 (the first pair of every snapshot uses the benchmark's p* = sin(0.3x) cos(0.2y) + 0.1z),
 solved by the plain FP64 Jacobi-BiCGStab to relative residual 1e-10; the pair

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <random>
 #include <unordered_map>
 #include <vector>
 
@@ -224,9 +225,12 @@ void orc_classify(const double* xyz, const uint8_t* type_in, size_t n, const int
 // status: 0 ok, 1 regularised, 2 skipped type, 3 sum w <= 0, 4 Cholesky failed.
 // Field values either from the quadratics coef (nrhs x 10) or from the array fields
 // (n x nrhs, per particle).
+// mirror_walls: Wall neighbors take the particle's own value (f_j = f_i, a zero normal
+// gradient; python/rain_plate_lsmps_cpu.py:179), so they shape the moments but add nothing
+// to the right-hand sides.
 static void wls_impl(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr, const int* col,
                      double re, double l0, double reg, int nrhs, const double* coef, const double* fields,
-                     double* x_out, int* status, double* z_out, double* wsum_out) {
+                     double* x_out, int* status, double* z_out, double* wsum_out, int mirror_walls = 0) {
     auto fval = [&](int k, size_t p) {
         return fields ? fields[p * nrhs + k]
                       : quad_eval(coef + 10 * k, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2]);
@@ -249,7 +253,7 @@ static void wls_impl(const double* xyz, const uint8_t* type, size_t n, const int
             double q[K];
             basis(dx, dy, dz, r, l0, q);
             ws += w;
-            for (int k = 0; k < nrhs; ++k) {
+            for (int k = 0; k < nrhs && !(mirror_walls && type[j] == WALL); ++k) {
                 double df = fval(k, (size_t)j) - fval(k, i);
                 for (int a = 0; a < K; ++a) bb[k * K + a] += w * q[a] * df / r;
             }
@@ -282,8 +286,9 @@ void orc_wls(const double* xyz, const uint8_t* type, size_t n, const int* row_pt
 // gradients come from (lsmps_wls_fields).
 void orc_wls_fields(const double* xyz, const uint8_t* type, size_t n, const int* row_ptr, const int* col,
                     double re, double l0, double reg, int nrhs, const double* fields, double* x_out,
-                    int* status) {
-    wls_impl(xyz, type, n, row_ptr, col, re, l0, reg, nrhs, nullptr, fields, x_out, status, nullptr, nullptr);
+                    int* status, int mirror_walls) {
+    wls_impl(xyz, type, n, row_ptr, col, re, l0, reg, nrhs, nullptr, fields, x_out, status, nullptr, nullptr,
+             mirror_walls);
 }
 
 // Pressure-Poisson assembly. Unknowns are Interior or NearWall particles in index order,
@@ -302,6 +307,11 @@ void orc_wls_fields(const double* xyz, const uint8_t* type, size_t n, const int*
 //    (failed_rows). p* as in variant 1. Unclipped second-order WLS rows are not
 //    diagonally dominant near one-sided (wall, surface) stencils and BiCGStab breaks
 //    down on them; with the clip every row is an M-matrix row.
+//  3 WLS Laplacian with Neumann walls: as 2, but Wall neighbors take the row particle's
+//    own pressure (zero normal gradient, the mirrored wall value of
+//    python/rain_plate_lsmps_cpu.py:90-100,179), so their coefficients c_ij (p_i - p_i)
+//    vanish: they add neither an entry nor to the diagonal. Free-surface and splash
+//    neighbors stay Dirichlet.
 // Row diagonals that are <= 0 or non-finite count as failed rows and are set to 1
 // (src/lsmps.cpp:52). b = A p* in row order (src/lsmps.cpp:59-61).
 // stats: unknowns, nnz, dirichlet, neumann, failed_rows. Call with row == nullptr first
@@ -329,12 +339,14 @@ long long orc_ppe_assemble(int variant, const double* xyz, const uint8_t* type, 
         size_t row_begin = cl.size();
         double diag = 0.0;
         bool identity = false;
-        if (variant == 2 && !(wls_status[i] == 0 || wls_status[i] == 1)) identity = true;
+        const bool wls_rows = variant == 2 || variant == 3;
+        if (wls_rows && !(wls_status[i] == 0 || wls_status[i] == 1)) identity = true;
         if (!identity) {
             for (int e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
                 int j = col[e];
                 int cj = map[j];
-                if (variant != 2 && cj < 0) continue;
+                if (!wls_rows && cj < 0) continue;
+                if (variant == 3 && type[j] == WALL) continue;
                 double dx = xyz[3 * j] - xi, dy = xyz[3 * j + 1] - yi, dz = xyz[3 * j + 2] - zi;
                 double r = std::sqrt(sq3(dx, dy, dz)), w = weight(r, re);
                 if (w <= 0) continue;
@@ -356,7 +368,7 @@ long long orc_ppe_assemble(int variant, const double* xyz, const uint8_t* type, 
             }
             if (variant != 0) diag = diag * (1.0 + diag_shift);
         }
-        if (variant == 2 && (identity || !(diag > 0) || !std::isfinite(diag))) {
+        if (wls_rows && (identity || !(diag > 0) || !std::isfinite(diag))) {
             cl.resize(row_begin); vl.resize(row_begin);
             failed++;
             diag = 1.0;
@@ -491,6 +503,87 @@ void orc_bicgstab(size_t n, const int* row, const int* col, const double* val, c
     double res = 0;
     for (size_t i = 0; i < n; ++i) { double d = Ax[i] - b[i]; res += d * d; }
     out4[0] = iters; out4[1] = conv ? 1.0 : 0.0; out4[2] = std::sqrt(res); out4[3] = now_ms() - t0;
+}
+
+// Particle-set generators of the bench and the tests, restated for the CPU side so that the
+// reference arm of bench.py builds its inputs without the product library. Positions must be
+// bit-identical to the library's generate_case (ls-mps_b200/csrc/host.cpp), so the draws come
+// from std::mt19937 + uniform_real_distribution<double> in the same order: that order is the
+// contract, pinned by tests/test_oracle.py against the library's positions.
+//   kind 0: the reference's default jittered lattice (src/lsmps.cpp:68,72; jitter .03)
+//   kind 1: rain on a 20-degree plate (3 wall layers, 4 film layers holding 70 % of the
+//           fluid, radius-3 droplets 10-40 l0 above; jitter .1)
+//   kind 2: 80 % jittered bulk lattice + 20 % rain on a plate 25 l0 beyond it (jitter .1)
+// jitter < 0 selects the kind's default. Returns the particle count written (n).
+size_t orc_generate(int kind, size_t n, double l0, double jitter, unsigned seed, double* xyz, uint8_t* type) {
+    std::mt19937 rng(seed);
+    size_t w = 0;
+    auto put = [&](double x, double y, double z, uint8_t t) {
+        xyz[3 * w] = x; xyz[3 * w + 1] = y; xyz[3 * w + 2] = z; type[w] = t; ++w;
+    };
+    auto grid = [&](size_t upto, int nx, int ny, int nz, double jit) {
+        std::uniform_real_distribution<double> u(-jit, jit);
+        for (int k = 0; k < nz && w < upto; ++k)
+            for (int j = 0; j < ny && w < upto; ++j)
+                for (int i = 0; i < nx && w < upto; ++i) {
+                    const double a = u(rng), b = u(rng), c = u(rng);
+                    put((i + .5 + a) * l0, (j + .5 + b) * l0, (k + .5 + c) * l0, INTERIOR);
+                }
+    };
+    auto plate = [&](size_t count, double jit, double x0) {
+        const double th = 20.0 * 3.14159265358979323846 / 180.0;
+        const double c = std::cos(th), sn = std::sin(th);
+        // a point at plate coordinates (s, y) and height h: s t1 + y t2 + h nrm
+        auto at = [&](double s, double y, double h, double* o) {
+            o[0] = (c * s + 0.0 * y) + -sn * h;
+            o[1] = (0.0 * s + 1.0 * y) + 0.0 * h;
+            o[2] = (sn * s + 0.0 * y) + c * h;
+        };
+        const int wall = 3, film = 4;
+        const int m = std::max(4, (int)std::floor(std::sqrt((double)count / (wall + film / 0.7))));
+        std::uniform_real_distribution<double> u(-jit, jit);
+        const size_t end = w + count;
+        auto layer = [&](double h, uint8_t t) {
+            for (int b = 0; b < m && w < end; ++b)
+                for (int a = 0; a < m && w < end; ++a) {
+                    const double ds = u(rng), dy = u(rng), dh = u(rng);
+                    double o[3];
+                    at((a + .5 + ds) * l0, (b + .5 + dy) * l0, (h + dh) * l0, o);
+                    put(o[0] + x0, o[1], o[2], t);
+                }
+        };
+        for (int k = 0; k < wall; ++k) layer(-(k + .5), WALL);
+        for (int k = 0; k < film; ++k) layer(k + .5, INTERIOR);
+        std::vector<std::array<int, 3>> ball;
+        for (int k = -3; k <= 3; ++k)
+            for (int j = -3; j <= 3; ++j)
+                for (int i = -3; i <= 3; ++i)
+                    if (i * i + j * j + k * k <= 9.0) ball.push_back({i, j, k});
+        std::uniform_real_distribution<double> us(0.0, m * l0), uh(10.0 * l0, 40.0 * l0);
+        while (w < end) {
+            const double s0 = us(rng), y0 = us(rng), h0 = uh(rng);
+            double ctr[3];
+            at(s0, y0, h0, ctr);
+            ctr[0] += x0;
+            for (const auto& o : ball) {
+                if (w >= end) break;
+                const double a = u(rng), b = u(rng), d = u(rng);
+                put(ctr[0] + (o[0] + a) * l0, ctr[1] + (o[1] + b) * l0, ctr[2] + (o[2] + d) * l0, INTERIOR);
+            }
+        }
+    };
+    if (kind == 1) {
+        plate(n, jitter >= 0 ? jitter : .1, 0.0);
+    } else if (kind == 2) {
+        const size_t nbulk = (size_t)(0.8 * (double)n);
+        const int nb = std::max(4, (int)std::ceil(std::cbrt((double)nbulk)));
+        grid(nbulk, nb, nb, nb, jitter >= 0 ? jitter : .1);
+        plate(n - w, jitter >= 0 ? jitter : .1, (nb + 25) * l0);
+    } else {
+        const int nx = std::max(4, (int)std::ceil(std::cbrt((double)n)));
+        grid(n, nx, nx, nx, jitter >= 0 ? jitter : .03);
+    }
+    return w;
 }
 
 }  // extern "C"

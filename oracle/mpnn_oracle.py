@@ -1,7 +1,7 @@
 """ORACLE — test infrastructure, not product code.
 
 numpy restatement of the learned preconditioner's network (no reference counterpart: the
-network is this repository's), used to check the GPU forward pass and
+network is this repository's learned preconditioner), used to check the GPU forward pass and
 gradients. It follows the GPU's arithmetic where it rounds: activations h, the aggregated
 messages m and the ReLU-masked gradients are rounded to BF16 where the GPU stores them in
 BF16, and the layer matrices are used in BF16; everything else is FP64 (the GPU accumulates

@@ -201,7 +201,7 @@ class Oracle:
             L.orc_wls.argtypes = [_dp, _up, C.c_size_t, _ip, _ip, C.c_double, C.c_double, C.c_double,
                                   C.c_int, _dp, C.c_void_p, _ip, C.c_void_p, C.c_void_p]
             L.orc_wls_fields.argtypes = [_dp, _up, C.c_size_t, _ip, _ip, C.c_double, C.c_double, C.c_double,
-                                         C.c_int, _dp, _dp, _ip]
+                                         C.c_int, _dp, _dp, _ip, C.c_int]
             L.orc_ppe_assemble.restype = C.c_longlong
             L.orc_ppe_assemble.argtypes = [C.c_int, _dp, _up, C.c_size_t, _ip, _ip, C.c_double,
                                            C.c_double, C.c_longlong, C.c_double, C.c_void_p,
@@ -211,8 +211,20 @@ class Oracle:
             L.orc_spmv.argtypes = [C.c_size_t, _ip, _ip, _dp, _dp, _dp, C.c_int]
             L.orc_bicgstab.argtypes = [C.c_size_t, _ip, _ip, _dp, _dp, C.c_void_p, C.c_int, C.c_double,
                                        C.c_int, C.c_int, _dp, _dp]
+            L.orc_generate.restype = C.c_size_t
+            L.orc_generate.argtypes = [C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_uint, _dp, _up]
             cls._lib = L
         return cls._lib
+
+    GENERATORS = {"bulk": 0, "rain_plate": 1, "mixed": 2}
+
+    @classmethod
+    def generate(cls, case, n, l0=1.0, seed=7, jitter=-1.0):
+        """Positions and types of the bench/test particle sets (bulk lattice, rain_plate,
+        mixed), bit-identical to the library's generator, without loading the library."""
+        xyz = np.zeros((n, 3)); t = np.zeros(n, np.uint8)
+        w = cls.lib().orc_generate(cls.GENERATORS[case], n, l0, jitter, seed, xyz.reshape(-1), t)
+        return xyz[:w], t[:w]
 
     @classmethod
     def neighbors(cls, xyz, re, maxn):
@@ -246,14 +258,15 @@ class Oracle:
         return x, st, z, ws
 
     @classmethod
-    def wls_fields(cls, xyz, types, row, col, re, l0, fields, reg=1e-8):
-        """WLS solutions (n x nfields x 9) of per-particle fields (n x nfields), and the status."""
+    def wls_fields(cls, xyz, types, row, col, re, l0, fields, reg=1e-8, mirror_walls=False):
+        """WLS solutions (n x nfields x 9) of per-particle fields (n x nfields), and the status.
+        mirror_walls: Wall neighbors take the particle's own value (zero normal gradient)."""
         fields = np.ascontiguousarray(np.atleast_2d(np.asarray(fields, dtype=np.float64).T).T)
         n, nf = fields.shape
         x = np.zeros((n, nf, 9)); st = np.zeros(n, np.int32)
         cls.lib().orc_wls_fields(np.ascontiguousarray(xyz, dtype=np.float64),
                                  np.ascontiguousarray(types, dtype=np.uint8), n, row, col, re, l0, reg, nf, fields,
-                                 x.reshape(-1), st)
+                                 x.reshape(-1), st, 1 if mirror_walls else 0)
         return x, st
 
     @classmethod

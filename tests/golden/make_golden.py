@@ -27,7 +27,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 from oracle import REF_BIN, Ref, build  # noqa: E402
 
-REF_ROOT = "/root/reference"
+REF_ROOT = os.environ.get("LSMPS_REFERENCE", "/root/reference")  # the reference source tree
 CASES = ["smoke", "bulk_uniform", "wall_film", "rain_injection", "narrow_gap"]
 
 

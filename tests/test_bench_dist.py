@@ -55,3 +55,5 @@ def test_reference_arm_under_torchrun(built):
     out = json.loads(lines[0])
     assert out["impl"] == "reference" and out["value"] > 0 and out["e2e"]["h2d_bytes_per_step"] == 0
     assert out["cpu_baseline"]["kind"] == "reference"
+    assert out["product_library_loaded"] is False  # inputs come from the oracle's generator
+    assert out["config"]["seeds"] == [7, 8, 9, 10]  # the GPU arm's particle sets

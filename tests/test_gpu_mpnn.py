@@ -1,6 +1,7 @@
 """Learned preconditioner on the GPU: forward pass and gradients against the numpy oracle
 (agreement to BF16 rounding: 2e-2 relative), training, and the learned solver with its
-fallback. The network has no reference counterpart."""
+fallback. The network has no reference counterpart (it is this library's learned
+preconditioner, trained on 200k-particle rain-on-plate snapshots)."""
 import numpy as np
 import pytest
 

@@ -99,3 +99,31 @@ def test_standalone_classify_matches_fused(ctx, cfg_dir):
     st2 = ctx.classify(0.01)
     assert np.array_equal(ctx.types(), fused)
     assert list(st2.type_count) == list(st.type_count)
+
+
+def test_crowded_segment_global_path(ctx):
+    """A segment whose 9 cell rows stage more than 1,536 candidates takes the warp-per-query
+    global scan: 2,000 coincident particles plus a lattice, lists longer than 1,536."""
+    xyz = np.concatenate([np.tile([[3.3, 3.3, 3.3]], (2000, 1)),
+                          lib.generate(None, case="bulk_uniform", particles=1500, l0=1.0, seed=6)[0]])
+    t = np.zeros(len(xyz), np.uint8)
+    st = check_against_oracle(ctx, xyz, t, 2.1, 2500, 1.0)
+    assert st.max_count > 1536
+    st = check_against_oracle(ctx, xyz, t, 2.1, 700, 1.0)  # and truncated there
+    assert st.truncated > 0
+
+
+@pytest.mark.parametrize("maxn", [128, 20])
+def test_single_pass_equals_two_pass(ctx, maxn):
+    """The single-pass build (slot rows, then compaction) and the count + fill passes give the
+    same lists, counts, truncation and classes."""
+    xyz, t, _ = lib.generate(None, case="mixed", particles=300_000, l0=1.0, seed=8)
+    ctx.upload(xyz, t)
+    a = ctx.build_neighbors(2.1, maxn, 1.0)
+    ra, ca = ctx.neighbors(a.pairs)
+    ta = ctx.types()
+    b = ctx.build_neighbors(2.1, maxn, 1.0, two_pass=True)
+    rb, cb = ctx.neighbors(b.pairs)
+    assert (a.pairs, a.truncated, list(a.type_count)) == (b.pairs, b.truncated, list(b.type_count))
+    assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
+    assert np.array_equal(ta, ctx.types())

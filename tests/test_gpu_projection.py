@@ -90,3 +90,61 @@ def test_projection_step(block):
     assert st.measured == ps.unknowns and 0 < st.core < st.measured
     assert st.div_core_after_rms <= 0.05 * st.div_core_before_rms, (st.div_core_before_rms, st.div_core_after_rms)
     assert np.isfinite(st.div_after_rms)
+
+
+def _wall_fields(xyz):
+    """u* = grad(phi) + w with phi = sin(0.2x) cos(0.15y) + 0.02 (z - 3)^2 and w = (sin(0.1y),
+    sin(0.1z), 0): div w = 0, and the normal component vanishes on the wall plane z = 3."""
+    x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    gx = 0.2 * np.cos(0.2 * x) * np.cos(0.15 * y) + np.sin(0.1 * y)
+    gy = -0.15 * np.sin(0.2 * x) * np.sin(0.15 * y) + np.sin(0.1 * z)
+    gz = 0.04 * (z - 3.0)
+    return np.stack([gx, gy, gz], 1)
+
+
+def test_projection_neumann_walls(built):
+    """A lattice block on three wall layers (z < 3) with a free surface elsewhere. With Dirichlet
+    walls (p = 0 at the wall particles) the band next to the wall keeps its divergence; with
+    Neumann walls (LSMPS_PPE_WALL_NEUMANN: wall neighbors take the particle's own value, as the
+    reference's mirrored virtual points) the divergence drops next to the wall too, and two hops
+    in as much as in the core. The Neumann system and the corrected velocity equal the oracle's
+    (variant 3, mirrored wall values)."""
+    pytest.importorskip("torch")
+    xyz = jittered_lattice(26, jitter=0.1, seed=4)
+    t = np.zeros(len(xyz), np.uint8)
+    t[xyz[:, 2] < 3.0] = lib.WALL
+    ustar = _wall_fields(xyz)
+    dt, rho = 0.01, 1000.0
+    res = {}
+    with lib.Context(0) as ctx:
+        ctx.upload(xyz, t)
+        ctx.build_neighbors(RE, 128, L0)
+        ctx.wls(RE, L0, mode=1)
+        cls = ctx.types()
+        for neumann in (False, True):
+            ps = ctx.ppe_assemble("wls", 10**12, RE, L0, diag_shift=0.0, wall_neumann=neumann)
+            system = ctx.ppe(ps.unknowns, ps.nnz)
+            u, p, st = ctx.projection_step(ustar, dt, rho, solver="fp64", tol=1e-12)
+            res[neumann] = (ps, system, u.cpu().numpy(), p.cpu().numpy(), st)
+    d, nm = res[False][4], res[True][4]
+    assert nm.converged and nm.wall_band1 > 300 and nm.wall_band2 > 300 and nm.core > 300
+    assert d.div_wall1_after_rms > 0.5 * d.div_wall1_before_rms, (d.div_wall1_before_rms, d.div_wall1_after_rms)
+    assert nm.div_wall1_after_rms <= 0.25 * nm.div_wall1_before_rms, (nm.div_wall1_before_rms, nm.div_wall1_after_rms)
+    assert nm.div_wall2_after_rms <= 0.05 * nm.div_wall2_before_rms, (nm.div_wall2_before_rms, nm.div_wall2_after_rms)
+    assert nm.div_core_after_rms <= 0.05 * nm.div_core_before_rms
+    # the Neumann rows against the oracle's variant 3 (built from the oracle's own WLS vectors)
+    ps, (prow, pcol, val, b, _, part), u, p, _ = res[True]
+    row, col, _ = Oracle.neighbors(xyz, RE, 128)
+    _, wst, z, ws = Oracle.wls(xyz, cls, row, col, RE, L0)
+    orow, ocol, oval, _, _, oup, ost = Oracle.ppe_assemble(3, xyz, cls, row, col, RE, L0, len(t), 0.0, z, ws, wst)
+    assert np.array_equal(part, oup) and abs(ps.nnz - ost["nnz"]) <= max(2, ps.nnz // 100000)
+    A = sp.csr_matrix((val.copy(), pcol.copy(), prow.copy()), shape=(ps.unknowns, ps.unknowns))
+    O = sp.csr_matrix((oval, ocol, orow), shape=(ps.unknowns, ps.unknowns))
+    assert abs(A - O).max() <= 1e-8 * abs(O).max()
+    pref = spla.spsolve(A.tocsc(), b)
+    assert np.linalg.norm(p[part] - pref) <= 1e-6 * np.linalg.norm(pref)
+    xp, _ = Oracle.wls_fields(xyz, cls, row, col, RE, L0, p, mirror_walls=True)
+    uref = ustar - dt / rho * xp[:, 0, :3]
+    walls = cls == lib.WALL
+    uref[walls] = ustar[walls]
+    assert np.linalg.norm(u - uref) <= 1e-6 * np.linalg.norm(uref)

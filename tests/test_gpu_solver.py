@@ -65,7 +65,7 @@ def test_fast_fp64_solver_tracks_reference(ctx, golden, cfg_dir, name):
 
 @pytest.fixture(scope="module")
 def lattice_system(ctx):
-    """BASELINE config-0 shape: 37^3 jittered lattice (+-0.1 l0), l0 = 1, re = 2.1."""
+    """The bulk lattice workload: 37^3 jittered lattice (+-0.1 l0), l0 = 1, re = 2.1."""
     xyz = jittered_lattice(37, 0.1, seed=7)
     return xyz, np.zeros(len(xyz), np.uint8)
 

@@ -70,3 +70,15 @@ def test_mixed_case_sizes(built):
     bulk, rain = xyz[: int(0.8 * n)], xyz[int(0.8 * n):]
     assert bulk[:, 0].max() < nb + 0.2
     assert rain[:, 0].min() > nb + 2.1  # no pair between the two parts
+
+
+@pytest.mark.parametrize("case,n,seed,jitter", [("mixed", 60_000, 7, -1.0), ("mixed", 1_000_000, 10, -1.0),
+                                                 ("rain_plate", 40_000, 3, -1.0), ("rain_plate", 25_000, 5, 0.05),
+                                                 ("bulk", 30_000, 1, -1.0)])
+def test_oracle_generators_match_library(built, case, n, seed, jitter):
+    """The oracle's generator restatement (used by bench.py's reference arm, which must not load
+    the library) yields the library's positions and types bit for bit."""
+    kw = {"jitter": jitter} if jitter >= 0 else {}
+    a = lib.generate(None, case="bulk_uniform" if case == "bulk" else case, particles=n, l0=1.0, seed=seed, **kw)
+    b = Oracle.generate(case, n, 1.0, seed, jitter)
+    assert sha(a[0], a[1]) == sha(*b)
