@@ -14,8 +14,10 @@ Workload (one "step" = the whole per-step path on one particle set):
   (126 MB) so no flush is needed.
 
 `value` = particles x GPUs / (device step time, CUDA events on the library's stream, max
-over ranks) with the headline solver (--solver, default `multigrid`: mixed-precision
-BiCGStab with the cell-aggregation multigrid V-cycle as preconditioner). `e2e` = the same
+over ranks) with the metric's solver (--solver, default `learned_multigrid`: the learned +
+mixed-precision solver, i.e. mixed-precision BiCGStab started from the message-passing
+network's guess, with the cell-aggregation multigrid V-cycle as its preconditioner; the same
+without the network is `multigrid` in ppe_compare). `e2e` = the same
 through the C ABI with host buffers: upload from pinned memory, the step, and the download of
 the pressure inside the timed region. The plain FP64 GPU BiCGStab (the reference iteration),
 Jacobi FP64, MIXED, LEARNED and both with the multigrid preconditioner are timed on the same
@@ -69,7 +71,7 @@ def parse_args():
     ap.add_argument("--case", default="mixed")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--sets", type=int, default=4, help="seeded particle sets the steps cycle through")
-    ap.add_argument("--solver", default="multigrid", choices=sorted(SOLVER_SPECS))
+    ap.add_argument("--solver", default="learned_multigrid", choices=sorted(SOLVER_SPECS))
     ap.add_argument("--weights", default=os.path.join(ROOT, "ls-mps_b200", "weights", "mpnn_rain200k.bin"),
                     help="network weights for the learned solver (trained by ls-mps_b200/train_mpnn.py)")
     ap.add_argument("--tol", type=float, default=3e-11,
@@ -362,13 +364,28 @@ def run_mine(args, dist):
     # ---- roofline of the dominant kernel (the solver's SpMV) and the other kernels ----
     peak, peak_kind = measured_hbm_peak()
     kern = {}
-    for name, kid in (("spmv32", lib.KB_SPMV32), ("spmv64", lib.KB_SPMV64), ("nbr_count", lib.KB_NBR_COUNT),
-                      ("nbr_fill", lib.KB_NBR_FILL), ("wls", lib.KB_WLS)) + (
+    for name, kid in (("spmv32", lib.KB_SPMV32), ("spmv64", lib.KB_SPMV64), ("nbr_scan", lib.KB_NBR_SCAN),
+                      ("nbr_compact", lib.KB_NBR_COMPACT), ("wls", lib.KB_WLS)) + (
                           (("mpnn_layer", lib.KB_MPNN_LAYER),) if "learned" in args.solver else ()) + (
                           (("mg_vcycle", lib.KB_MG_VCYCLE),) if "multigrid" in args.solver else ()):
         ms, nbytes = ctx.kernel_bench(kid, 20)
         gbs = nbytes / (ms * 1e-3) / 1e9
         kern[name] = {"ms": ms, "alg_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    # the all-particle WLS against the measured FP64 peak (its bound): ~170 FLOPs per pair (the
+    # moment and right-hand-side passes) and ~800 per particle (9 x 9 Cholesky and two solves)
+    pk_ms, pk_flops = ctx.kernel_bench(lib.KB_FP64_PEAK, 5)
+    fp64_peak = pk_flops / (pk_ms * 1e-3) / 1e12
+    wls_flops = 170.0 * float(nst.pairs) + 800.0 * n
+    kern["wls"].update({"fp64_tflops": wls_flops / (kern["wls"]["ms"] * 1e-3) / 1e12, "alg_flops": wls_flops})
+    kern["wls"]["fp64_frac"] = kern["wls"]["fp64_tflops"] / fp64_peak
+    result["fp64_peak_tflops"] = {"value": fp64_peak, "how": "independent FP64 FMA chains on every SM "
+                                  "(lsmps_kernel_bench LSMPS_KB_FP64_PEAK), CUDA events"}
+    # the neighbor build as one unit (scan + compaction) against the algorithmic bytes of the
+    # build + classification: positions once, row pointers, columns, classes (24 N + 4 (N + 1) + 4 P + N)
+    nb_ms = kern["nbr_scan"]["ms"] + kern["nbr_compact"]["ms"]
+    nb_bytes = 24.0 * n + 4.0 * (n + 1) + 4.0 * float(nst.pairs) + 1.0 * n
+    kern["nbr_build"] = {"ms": nb_ms, "alg_bytes": nb_bytes, "achieved_gbs": nb_bytes / (nb_ms * 1e-3) / 1e9,
+                         "frac": nb_bytes / (nb_ms * 1e-3) / 1e9 / peak}
     dom = "spmv64" if args.solver in ("fp64", "jacobi") else "spmv32"
     # the mixed solver's SpMV: FP32 values of A D^-1, FP64 vectors
     traffic = committed_traffic().get(dom)

@@ -81,7 +81,9 @@ enum {
     LSMPS_KB_MG_VCYCLE = 6,  /* one multigrid V-cycle (all its kernels) on the assembled system's
                                hierarchy: 92 U + 464 (rows of the coarse levels) */
     LSMPS_KB_NBR_SCAN = 7,
-    LSMPS_KB_NBR_COMPACT = 8
+    LSMPS_KB_NBR_COMPACT = 8,
+    LSMPS_KB_FP64_PEAK = 9   /* independent FP64 FMA chains on every SM: the measured FP64 peak; the
+                               second output holds FLOPs per launch, not bytes. Needs no data. */
 };
 int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 

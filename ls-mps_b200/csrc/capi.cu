@@ -198,6 +198,8 @@ int lsmps_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms_per_laun
             mpnn_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
         else if (kernel == LSMPS_KB_MG_VCYCLE)
             mg_kernel_bench(ctx, reps, ms_per_launch, bytes_per_launch);
+        else if (kernel == LSMPS_KB_FP64_PEAK)
+            fp64_peak_bench(ctx, reps, ms_per_launch, bytes_per_launch);
         else
             throw Error{LSMPS_ERR_ARG, "unknown kernel id"};
     });

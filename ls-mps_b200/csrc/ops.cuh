@@ -81,6 +81,7 @@ void mg_apply_host(lsmps_ctx* ctx, const double* z, double* out, size_t n);
 // Profiling hooks behind lsmps_kernel_bench (mean ms per launch, algorithmic bytes).
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
 void wls_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
+void fp64_peak_bench(lsmps_ctx* ctx, int reps, double* ms, double* flops);
 void solver_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes);
 void mpnn_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);
 void mg_kernel_bench(lsmps_ctx* ctx, int reps, double* ms, double* bytes);

@@ -25,7 +25,8 @@ NBR_TWO_PASS = 2
 PPE_WALL_NEUMANN = 1
 PPE_REFERENCE, PPE_SHIFTED, PPE_WLS = range(3)
 SOLVER_REFERENCE, SOLVER_FP64, SOLVER_JACOBI, SOLVER_MIXED, SOLVER_LEARNED, SOLVER_MIXED_F32 = range(6)
-KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER, KB_MG_VCYCLE, KB_NBR_SCAN, KB_NBR_COMPACT = range(9)
+(KB_SPMV64, KB_SPMV32, KB_NBR_COUNT, KB_NBR_FILL, KB_WLS, KB_MPNN_LAYER, KB_MG_VCYCLE, KB_NBR_SCAN, KB_NBR_COMPACT,
+ KB_FP64_PEAK) = range(10)
 PRECONDS = {"jacobi": 0, "multigrid": 1}
 SOLVERS = {"reference": 0, "fp64": 1, "jacobi": 2, "mixed": 3, "learned": 4, "mixed_f32": 5}
 VARIANTS = {"reference": 0, "shifted": 1, "wls": 2}

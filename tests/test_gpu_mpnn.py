@@ -119,6 +119,33 @@ def test_training_reduces_loss_and_helps_the_solver(ctx):
     print(f"\nheld-out 20k: mixed {m.iterations} it, learned {le.iterations} it")
 
 
+def test_trained_network_gain_on_held_out_snapshots(ctx):
+    """What the shipped network (ls-mps_b200/weights, trained on 200k-particle rain-on-plate
+    snapshots, seeds 1000-1039) gains over the same solver without it, on held-out snapshots of
+    its training distribution (seeds 9000-9007, 200k particles): LEARNED needs fewer BiCGStab
+    iterations than MIXED in total and reaches the same accuracy. The wall time is printed
+    beside it: the network's inference costs more than the iterations it saves (the measured
+    result this library reports)."""
+    ctx.mpnn_load(lib.DEFAULT_WEIGHTS)
+    its = {"mixed": [], "learned": []}
+    ms = {"mixed": [], "learned": []}
+    for seed in range(9000, 9008):
+        xyz, t, _ = lib.generate(None, case="rain_plate", particles=200_000, l0=1.0, seed=seed)
+        ctx.upload(xyz, t)
+        ctx.build_neighbors(2.1, 128, 1.0)
+        ctx.wls(2.1, 1.0, mode=1)
+        ctx.ppe_assemble("wls", 10**9, 2.1, 1.0, diag_shift=0.0)
+        for name in ("mixed", "learned"):
+            ctx.ppe_solve(name, 20000, 3e-11)  # warm (graphs, autotuning)
+            s = ctx.ppe_solve(name, 20000, 3e-11)
+            assert s.converged and s.relative_l2_error <= 1e-8, (name, seed)
+            its[name].append(s.iterations)
+            ms[name].append(s.solve_ms)
+    assert sum(its["learned"]) < sum(its["mixed"]), its
+    print(f"\nheld-out rain_plate 200k x8: iterations mixed {np.mean(its['mixed']):.1f} learned "
+          f"{np.mean(its['learned']):.1f}; solve ms mixed {np.mean(ms['mixed']):.2f} learned {np.mean(ms['learned']):.2f}")
+
+
 def test_bad_network_falls_back(ctx):
     xyz = jittered_lattice(14, 0.1, seed=9)
     setup_system(ctx, xyz, np.zeros(len(xyz), np.uint8))

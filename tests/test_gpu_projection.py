@@ -123,8 +123,8 @@ def test_projection_neumann_walls(built):
         cls = ctx.types()
         for neumann in (False, True):
             ps = ctx.ppe_assemble("wls", 10**12, RE, L0, diag_shift=0.0, wall_neumann=neumann)
-            system = ctx.ppe(ps.unknowns, ps.nnz)
             u, p, st = ctx.projection_step(ustar, dt, rho, solver="fp64", tol=1e-12)
+            system = ctx.ppe(ps.unknowns, ps.nnz)  # b = -rho / dt div u* after the step
             res[neumann] = (ps, system, u.cpu().numpy(), p.cpu().numpy(), st)
     d, nm = res[False][4], res[True][4]
     assert nm.converged and nm.wall_band1 > 300 and nm.wall_band2 > 300 and nm.core > 300

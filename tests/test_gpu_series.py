@@ -203,3 +203,26 @@ def test_rain_validation_outputs(series_runs):
         if len(thick):
             assert abs(fmean - thick.mean()) <= 1e-12 and abs(fp90 - np.quantile(thick, 0.9)) <= 1e-12
             assert abs(fmax - thick.max()) <= 1e-12  # d = x n_x + z n_z: FMA on the GPU
+
+
+def test_rain_tables_reproduce_the_validated_fixture(series_runs):
+    """A fresh run reproduces tests/golden/rain_validation, the tables on which the reference's
+    own python/validate_outputs.py passes (tests/test_reference_tools.py)."""
+    import csv
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_rain_validation_fixture as fx
+
+    assert fx.SERIES == SMALL and fx.PLATE == {"particles": 60_000, "seed": 3}
+    rows, _ = series_runs["fp64"]
+    tabs = fx.tables(rows, series_runs["fp64_rain"])
+    for name, tab in tabs.items():
+        ref = list(csv.DictReader(open(os.path.join(fx.OUT, name))))
+        assert len(ref) == len(tab), name
+        for got, want in zip(tab, ref):
+            assert set(want) == {str(k) for k in got}, name
+            for k, v in got.items():
+                if k in ("window", "section"):
+                    assert str(v) == want[k]
+                else:
+                    assert math.isclose(float(v), float(want[k]), rel_tol=1e-12, abs_tol=1e-300), (name, k, v, want[k])

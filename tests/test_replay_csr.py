@@ -80,3 +80,18 @@ def test_load_csr_and_replay(built, tmp_path):
         assert s["converged"] and s["relative_l2_error"] <= 1e-8, (name, s)
     assert all(k["achieved_gbs"] > 0 for k in res["kernels"].values())
     assert res["timeline"]["steps"] == 12
+
+
+@pytest.mark.gpu
+def test_replay_the_reference_tool_output(built):
+    """The replay on the file set the reference's python/workload_calibration.py wrote
+    (tests/golden/calibration): every solver reaches p* = 1, the SpMV kernels run, and the
+    tool's 200-step timeline replays."""
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "calibration")
+    res = replay_csr.replay(d, ("mixed", "fp64", "jacobi"), tol=1e-11)
+    meta = json.load(open(os.path.join(d, "metadata.json")))
+    assert res["rows"] == meta["particles"] and res["entries"] == meta["csr_nnz"]
+    for name, s in res["solvers"].items():
+        assert s["converged"] and s["relative_l2_error"] <= 1e-8, (name, s)
+    assert all(k["achieved_gbs"] > 0 for k in res["kernels"].values())
+    assert res["timeline"]["steps"] == 200
