@@ -158,7 +158,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->fr0, &ctx->fp, &ctx->fv, &ctx->fs, &ctx->ft, &ctx->fph, &ctx->fsh,
                                  &ctx->red, &ctx->S_ptr, &ctx->S_len,
                                  &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf, &ctx->nbr_slots,
-                                 &ctx->A_slot_col, &ctx->A_slot_val};
+                                 &ctx->A_slot_col, &ctx->A_slot_val, &ctx->A_xep};
     for (auto* b : bufs) b->release();
     mpnn_destroy(ctx);
     mg_destroy(ctx);

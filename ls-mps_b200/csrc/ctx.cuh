@@ -94,7 +94,7 @@ struct lsmps_ctx {
     long long U = 0, nnz = 0;
     lsmps_gpu::DevBuf ref_rank, u_of_sorted, sorted_of_u, ref_of_u, u_of_ref;
     lsmps_gpu::DevBuf A_row, A_col, A_val, A_valf, A_b, A_xexact, A_dinv, A_dinvf, A_cnt;
-    lsmps_gpu::DevBuf A_slot_col, A_slot_val;
+    lsmps_gpu::DevBuf A_slot_col, A_slot_val, A_xep;  // A_xep: p* per sorted particle
     bool ppe_wall_neumann = false;  // the assembled WLS rows treat walls as Neumann boundaries  // assembly: rows at their neighbor-row slots before packing
     lsmps_ppe_stats ppe_assembly{};
     bool ppe_loaded = false;        // the system came from lsmps_ppe_load_csr (no particles behind it)

@@ -546,7 +546,10 @@ __global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_scan(SegGrid G, const in
                                                             int* __restrict__ cnt,
                                                             unsigned long long* trunc_total,
                                                             int* __restrict__ slots, uint8_t* __restrict__ cls) {
-    __shared__ float4 cf[SEG_MAXC];
+    // staged candidates in pairs, for the packed FP32x2 arithmetic: pair p holds the x and y
+    // of candidates 2p and 2p + 1 in cxy[p] and their z in cz[p]
+    __shared__ float4 cxy[SEG_MAXC / 2 + 1];
+    __shared__ float2 cz[SEG_MAXC / 2 + 1];
     __shared__ int rbase[10], rfirst[9], rcs[9][SEG + 3];
     const float re_f = (float)G.re;
     const float re2f = (float)re2;
@@ -554,14 +557,14 @@ __global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_scan(SegGrid G, const in
     const float cull = re2f * (1.f + 1e-4f);
     const float margin = 4e-6f * re_f;
     const int seg = seg_list[blockIdx.x];
-    const int sxi = seg % G.nsegx, tt = seg / G.nsegx, cy = tt % G.g.ny, cz = tt / G.g.ny;
+    const int sxi = seg % G.nsegx, tt = seg / G.nsegx, cy = tt % G.g.ny, cz0 = tt / G.g.ny;
     const int cx0 = sxi * SEG, cx1 = min(cx0 + SEG, G.g.nx) - 1;
     const int lo = max(cx0 - 1, 0), hi = min(cx1 + 1, G.g.nx - 1);
-    const int rowlin = (cz * G.g.ny + cy) * G.g.nx;
+    const int rowlin = (cz0 * G.g.ny + cy) * G.g.nx;
     const int q0 = G.g.cell_start[rowlin + cx0], q1 = G.g.cell_start[rowlin + cx1 + 1];
     for (int t = threadIdx.x; t < 9 * (SEG + 3); t += blockDim.x) {
         const int r = t / (SEG + 3), c = lo + t % (SEG + 3);
-        const int y = cy + (r % 3 - 1), z = cz + (r / 3 - 1);
+        const int y = cy + (r % 3 - 1), z = cz0 + (r / 3 - 1);
         int v = 0;
         if (y >= 0 && y < G.g.ny && z >= 0 && z < G.g.nz && c <= hi + 1) v = G.g.cell_start[(z * G.g.ny + y) * G.g.nx + c];
         rcs[r][c - lo] = v;
@@ -584,25 +587,33 @@ __global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_scan(SegGrid G, const in
                               lane);
         return;
     }
-    const double ox = (G.g0.x + cx0) * G.re, oy = (G.g0.y + cy) * G.re, oz = (G.g0.z + cz) * G.re;
+    const double ox = (G.g0.x + cx0) * G.re, oy = (G.g0.y + cy) * G.re, oz = (G.g0.z + cz0) * G.re;
+    float* fxy = reinterpret_cast<float*>(cxy);
+    float* fz = reinterpret_cast<float*>(cz);
     for (int r = 0; r < 9; ++r) {  // row by row: consecutive threads load consecutive particles
         const int n_r = rbase[r + 1] - rbase[r], f = rfirst[r], b = rbase[r];
-        for (int i = threadIdx.x; i < n_r; i += blockDim.x)
-            cf[b + i] = make_float4((float)(sx[f + i] - ox), (float)(sy[f + i] - oy), (float)(sz[f + i] - oz), 0.f);
+        for (int i = threadIdx.x; i < n_r; i += blockDim.x) {
+            const int si = b + i, p = si >> 1, h = si & 1;
+            fxy[4 * p + h] = (float)(sx[f + i] - ox);
+            fxy[4 * p + 2 + h] = (float)(sy[f + i] - oy);
+            fz[2 * p + h] = (float)(sz[f + i] - oz);
+        }
     }
     __syncthreads();
     for (int k = q0 + threadIdx.x; k < q1; k += blockDim.x) {
         const int ck = scell[k] - rowlin;                   // the query's cell along x
         const int kst = rbase[4] + (k - rfirst[4]);         // the query staged in the centre row
-        const float4 qf = cf[kst];
-        const float qx = qf.x - (ck - cx0) * re_f;          // position inside its own cell (x)
+        const float qxs = fxy[4 * (kst >> 1) + (kst & 1)], qys = fxy[4 * (kst >> 1) + 2 + (kst & 1)];
+        const float qzs = fz[2 * (kst >> 1) + (kst & 1)];
+        const float2 nqx = make_float2(-qxs, -qxs), nqy = make_float2(-qys, -qys), nqz = make_float2(-qzs, -qzs);
+        const float qx = qxs - (ck - cx0) * re_f;          // position inside its own cell (x)
         int* out = slots + (size_t)k * maxn;
         int written = 0;
         unsigned sec = 0;
         for (int r = 0; r < 9; ++r) {
             const int dy = r % 3 - 1, dz = r / 3 - 1;
-            const float gy = dy < 0 ? qf.y : (dy > 0 ? re_f - qf.y : 0.f);
-            const float gz = dz < 0 ? qf.z : (dz > 0 ? re_f - qf.z : 0.f);
+            const float gy = dy < 0 ? qys : (dy > 0 ? re_f - qys : 0.f);
+            const float gz = dz < 0 ? qzs : (dz > 0 ? re_f - qzs : 0.f);
             const float gyz = gy * gy + gz * gz;
             if (gyz > cull) continue;
             // cells ck-1 .. ck+1 of this row, each kept when its box is within re
@@ -613,26 +624,37 @@ __global__ void __launch_bounds__(SEG_THREADS, 8) k_seg_scan(SegGrid G, const in
             const int sb = rbase[r] + (gb - rfirst[r]);
             const int se = sb + (ge - gb);
             const int mshift = rfirst[r] - rbase[r];  // global index = staged index + mshift
-            for (int c0 = sb; c0 < se; c0 += 32) {
-                const int len = min(32, se - c0);
+            const int pend = (se + 1) >> 1;
+            for (int pb = sb >> 1; pb < pend; pb += 16) {
+                const int c0 = pb << 1;  // first staged candidate of this chunk of 32
+                const int np = min(16, pend - pb);
                 unsigned hit = 0;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    if (i < len) {
-                        const float4 cj = cf[c0 + i];
-                        const float dx = cj.x - qf.x, dyf = cj.y - qf.y, dzf = cj.z - qf.z;
-                        const float d2 = dx * dx + dyf * dyf + dzf * dzf;
-                        if (d2 <= hi_th) hit |= 1u << i;
+                for (int j = 0; j < 16; ++j) {
+                    if (j < np) {
+                        const float4 a = cxy[pb + j];
+                        const float2 dxv = __fadd2_rn(make_float2(a.x, a.y), nqx);
+                        const float2 dyv = __fadd2_rn(make_float2(a.z, a.w), nqy);
+                        const float2 dzv = __fadd2_rn(cz[pb + j], nqz);
+                        float2 d2 = __fmul2_rn(dxv, dxv);
+                        d2 = __ffma2_rn(dyv, dyv, d2);
+                        d2 = __ffma2_rn(dzv, dzv, d2);
+                        if (d2.x <= hi_th) hit |= 1u << (2 * j);
+                        if (d2.y <= hi_th) hit |= 2u << (2 * j);
                     }
                 }
-                if (r == 4 && kst >= c0 && kst < c0 + len) hit &= ~(1u << (kst - c0));
+                // keep the window [sb, se) and drop the query itself
+                const int wlo = sb - c0, whi = se - c0;
+                if (whi < 32) hit &= (1u << whi) - 1u;
+                if (wlo > 0) hit &= ~((1u << wlo) - 1u);
+                if (r == 4 && kst >= c0 && kst < c0 + 32) hit &= ~(1u << (kst - c0));
                 while (hit) {
                     const int i = __ffs(hit) - 1;
                     hit &= hit - 1;
-                    const float4 cj = cf[c0 + i];
-                    const float dx = cj.x - qf.x, dyf = cj.y - qf.y, dzf = cj.z - qf.z;
+                    const int si = c0 + i, p = si >> 1, h = si & 1;
+                    const float dx = fxy[4 * p + h] - qxs, dyf = fxy[4 * p + 2 + h] - qys, dzf = fz[2 * p + h] - qzs;
                     const float d2 = dx * dx + dyf * dyf + dzf * dzf;
-                    const int m = c0 + i + mshift;
+                    const int m = si + mshift;
                     if (d2 >= lo_th && !(xnorm2(xsub(sx[m], sx[k]), xsub(sy[m], sy[k]), xsub(sz[m], sz[k])) < re2))
                         continue;
                     if (written < maxn) {

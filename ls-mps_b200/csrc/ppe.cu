@@ -66,10 +66,24 @@ __global__ void k_number_unknowns(const int* __restrict__ perm, const uint8_t* _
 }
 
 // Off-diagonal coefficient a_ij (> 0 means the row gets -a_ij at column j) of row k for
-// neighbor m; returns false when the pair contributes nothing.
+// neighbor m; returns false when the pair contributes nothing. For the WLS rows, zk holds the
+// row's Laplacian vector z prescaled (z0..z2, z3..z5 times 1 / (2 l0), z6..z8 times 1 / l0)
+// and ws holds 1 / (sum_w l0).
 __device__ __forceinline__ bool row_coeff(const PpeParams& P, double xi, double yi, double zi, double xm,
                                           double ym, double zm, const double* zk, double ws, double& a) {
     double dx = xsub(xm, xi), dy = xsub(ym, yi), dz = xsub(zm, zi);
+    if (P.variant == LSMPS_PPE_WLS) {
+        // c = w (q . z) / (r sum_w l0) with w = (re / r - 1)^2 and q . z = P / r, where P is the
+        // polynomial below: c = (re - r)^2 P / (r^4 sum_w l0), one square root and one division
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double r = sqrt(d2);
+        if (r <= 1e-12 || r >= P.re) return false;
+        const double t = P.re - r;
+        const double poly = dx * zk[0] + dy * zk[1] + dz * zk[2] + dx * dx * zk[3] + dy * dy * zk[4] +
+                            dz * dz * zk[5] + dx * dy * zk[6] + dx * dz * zk[7] + dy * dz * zk[8];
+        a = (t * t * poly * ws) / (d2 * d2);
+        return a > 0;  // clipped: only c > 0 contributes
+    }
     double r = __dsqrt_rn(xnorm2(dx, dy, dz));
     double w = xweight(r, P.re);
     if (w <= 0) return false;
@@ -77,18 +91,8 @@ __device__ __forceinline__ bool row_coeff(const PpeParams& P, double xi, double 
         a = xdiv(w, xmul(r, r));  // src/lsmps.cpp:48
         return true;
     }
-    if (P.variant == LSMPS_PPE_SHIFTED) {
-        a = w;
-        return true;
-    }
-    // WLS Laplacian: c = w (q . z) / (r sum_w l0), clipped: only c > 0 contributes.
-    double ir = 1.0 / r;
-    double s = ir / P.l0;
-    double hs = 0.5 * s;
-    double qz = dx * ir * zk[0] + dy * ir * zk[1] + dz * ir * zk[2] + dx * dx * hs * zk[3] + dy * dy * hs * zk[4] +
-                dz * dz * hs * zk[5] + dx * dy * s * zk[6] + dx * dz * s * zk[7] + dy * dz * s * zk[8];
-    a = w * qz / (r * ws * P.l0);
-    return a > 0;
+    a = w;  // shifted graph Laplacian
+    return true;
 }
 
 __device__ __forceinline__ bool wls_row_valid(int st) { return st == 0 || st == 1; }
@@ -98,6 +102,13 @@ __device__ __forceinline__ bool wls_row_valid(int st) { return st == 0 || st == 
 // neighbors' so that b = A p* is computed from the entries as they are written.
 __device__ __forceinline__ double exact_p(int variant, double x, double y, double z) {
     return variant == LSMPS_PPE_REFERENCE ? xadd(xmul(x, x), xmul(y, y)) : sin(0.3 * x) * cos(0.2 * y) + 0.1 * z;
+}
+
+// p* at every sorted particle, once (the rows read it for their own and their neighbors' values)
+__global__ void k_ppe_exact(size_t n, int variant, const double* __restrict__ sx, const double* __restrict__ sy,
+                            const double* __restrict__ sz, double* __restrict__ xep) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        xep[k] = exact_p(variant, sx[k], sy[k], sz[k]);
 }
 
 // One pass over the rows, PPE_G lanes per row: the lanes of a row's group take its neighbors
@@ -117,7 +128,8 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
                                                   const int* __restrict__ wst, const double* __restrict__ wz,
                                                   const double* __restrict__ wws, int* __restrict__ cnt,
                                                   int* __restrict__ scol, double* __restrict__ sval,
-                                                  double* __restrict__ xexact, double* __restrict__ b,
+                                                  const double* __restrict__ xep, double* __restrict__ xexact,
+                                                  double* __restrict__ b,
                                                   double* __restrict__ dinv, unsigned long long* stats) {
     const int lane = threadIdx.x & 31, sub = lane & (PPE_G - 1), gbase = lane & ~(PPE_G - 1);
     const long long u = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / PPE_G;
@@ -136,9 +148,10 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
 #pragma unroll
     for (int a = 0; a < K; ++a) zk[a] = 0.0;
     if (live && P.variant == LSMPS_PPE_WLS && !pinned && !identity) {
+        const double h = 0.5 / P.l0, g = 1.0 / P.l0;
 #pragma unroll
-        for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a];
-        ws = wws[k];
+        for (int a = 0; a < K; ++a) zk[a] = wz[(size_t)k * K + a] * (a < 3 ? 1.0 : a < 6 ? h : g);
+        ws = 1.0 / (wws[k] * P.l0);
     }
     const long long sbase = live ? (long long)row[k] + k : 0;  // the row's slot range
     // the warp walks the longest of its groups' rows; shorter rows idle (flags stay 0)
@@ -151,13 +164,16 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
         double a = 0.0, xem = 0.0;
         int cj = -1;
         if (e < e1) {
+            // every load of the pair at once (one dependent round trip after col)
             const int m = col[e];
             cj = uidx[m];
-            if ((P.variant == LSMPS_PPE_WLS || cj >= 0) && !(P.neumann && cls[m] == LSMPS_WALL)) {
-                const double xm = sx[m], ym = sy[m], zm = sz[m];
+            const double xm = sx[m], ym = sy[m], zm = sz[m];
+            const double xpm = xep[m];
+            const bool wall = P.neumann && cls[m] == LSMPS_WALL;
+            if ((P.variant == LSMPS_PPE_WLS || cj >= 0) && !wall) {
                 contrib = row_coeff(P, xi, yi, zi, xm, ym, zm, zk, ws, a);
                 keep = contrib && cj >= 0;
-                if (keep) xem = exact_p(P.variant, xm, ym, zm);
+                if (keep) xem = xpm;
             }
         }
         const unsigned kb = (__ballot_sync(0xffffffffu, keep) >> gbase) & ((1u << PPE_G) - 1u);
@@ -179,7 +195,7 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
     }
     int neumann = 0, failed = 0;
     if (live) {
-        const double xe = exact_p(P.variant, xi, yi, zi);
+        const double xe = xep[k];
         int c = written;
         if (pinned) {
             c = 0;
@@ -328,10 +344,13 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     auto* st = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 32);
     LSMPS_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), s));
     if (U) {
+        double* xep = ctx->A_xep.ensure<double>(n + 1);
+        k_ppe_exact<<<std::min<unsigned>(blocks_for(n, 256), 148 * 8), 256, 0, s>>>(
+            n, o->variant, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(), xep);
         k_ppe_rows<<<blocks_for((size_t)U * PPE_G, 128), 128, 0, s>>>(
             P, U, sorted_of_u, ref_of_u, uidx, ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
             ctx->cls.get<uint8_t>(), ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), wst, wz, wws, cnt, scol, sval,
-            xe, b, dinv, st);
+            xep, xe, b, dinv, st);
         LSMPS_CHECK_LAUNCH();
     }
     scan_exclusive<int>(cnt, arow, U, s, ctx->scan_tmp, dflag);
