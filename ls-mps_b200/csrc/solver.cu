@@ -690,74 +690,96 @@ __global__ void k_sell_len(long long n, long long nslices, const int* __restrict
     }
 }
 
-// one thread per slot row (padding rows of the last slice included): entries in CSR
-// order, padding with value 0 and the row's own column (always a valid index)
-__global__ void k_sell_fill(long long n, long long nslices, const int* __restrict__ row,
-                            const int* __restrict__ acol, const double* __restrict__ aval,
-                            const int* __restrict__ sptr, const int* __restrict__ slen, int* __restrict__ col,
-                            double* __restrict__ val) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= nslices * 32) return;
-    long long s = i >> 5;
-    int lane = (int)(i & 31);
+// All SELL arrays of a slice in one pass, one warp per slice of 32 rows: the slice's CSR entries
+// (one contiguous range) are staged in shared memory with coalesced loads, then each lane writes
+// its row four entries at a time with 16-byte stores: columns (the diagonal moved to its place
+// in column order, padding repeating the last column), values A (padding 0), the column steps
+// and the row's first column (any row that does not ascend or steps by more than 65535 sets
+// *bad), and the column-scaled copies A D^-1 in FP64 and FP32. Slices of more than SB_CAP
+// entries read their rows from global memory instead. Same values as a per-row fill followed
+// by the column-scaling passes (each scaled value is the same single product, rounded once).
+constexpr int SB_CAP = 1024;
+__global__ void __launch_bounds__(128) k_sell_build(long long n, long long nslices, const int* __restrict__ row,
+                                                    const int* __restrict__ acol, const double* __restrict__ aval,
+                                                    const double* __restrict__ dinv, const int* __restrict__ sptr,
+                                                    const int* __restrict__ slen, int* __restrict__ col,
+                                                    double* __restrict__ val, unsigned short* __restrict__ dcol,
+                                                    int* __restrict__ rbase, double* __restrict__ vals,
+                                                    float* __restrict__ valf, int* bad) {
+    __shared__ int scol[4][SB_CAP];
+    __shared__ double sval[4][SB_CAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long s = blockIdx.x * 4LL + w;
+    if (s >= nslices) return;  // whole warp
+    const long long u0 = s << 5, i = u0 + lane;
+    const int b0 = row[u0], b1 = row[min(u0 + 32, n)];
+    const bool staged = b1 - b0 <= SB_CAP;
+    if (staged) {
+        for (int t = lane; t < b1 - b0; t += 32) {
+            scol[w][t] = acol[b0 + t];
+            sval[w][t] = aval[b0 + t];
+        }
+    }
+    __syncwarp();
     int e0 = 0, len = 0;
     if (i < n) {
         e0 = row[i];
         len = row[i + 1] - e0;
     }
-    // the CSR row's last entry is its diagonal; it goes where it belongs in column order (the
-    // off-diagonals come ascending from the assembly), padding repeats the last column
+    auto C = [&](int e) { return staged ? scol[w][e - b0] : acol[e]; };
+    auto V = [&](int e) { return staged ? sval[w][e - b0] : aval[e]; };
+    // the CSR row's last entry is its diagonal: it goes where it belongs in column order
     int pos = 0;
     if (len > 0)
-        while (pos < len - 1 && acol[e0 + pos] < (int)i) ++pos;
-    int last = i < n ? (int)i : 0;
-    long long base = (long long)sptr[s] + 4 * lane;
-    for (int k = 0; k < slen[s]; ++k) {
-        long long e = base + 128LL * (k >> 2) + (k & 3);
-        if (k < len) {
-            const int src = k < pos ? e0 + k : (k == pos ? e0 + len - 1 : e0 + k - 1);
-            last = acol[src];
-            col[e] = last;
-            val[e] = aval[src];
-        } else {
-            col[e] = last;
-            val[e] = 0.0;
-        }
-    }
-}
-
-// 16-bit column steps of the SELL layout: per slot row, rbase = its first column and dcol[k] =
-// col[k] - col[k - 1] (0 for the first entry); a row that does not ascend or steps by more
-// than 65535 sets *bad (the 32-bit columns are used then).
-__global__ void k_sell_steps(long long nslices, const int* __restrict__ sptr, const int* __restrict__ slen,
-                             const int* __restrict__ col, unsigned short* __restrict__ dcol, int* __restrict__ rbase,
-                             int* bad) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= nslices * 32) return;
-    long long s = i >> 5;
-    int lane = (int)(i & 31);
-    long long base = (long long)sptr[s] + 4 * lane;
-    int prev = col[base];
-    rbase[i] = prev;
+        while (pos < len - 1 && C(e0 + pos) < (int)i) ++pos;
+    int last = i < n ? (int)i : 0, prev = 0;
     bool ok = true;
-    for (int k = 0; k < slen[s]; ++k) {
-        long long e = base + 128LL * (k >> 2) + (k & 3);
-        const int c = col[e];
-        const int d = c - prev;
-        ok = ok && d >= 0 && d <= 65535;
-        dcol[e] = (unsigned short)(d >= 0 && d <= 65535 ? d : 0);
-        prev = c;
+    const int L = slen[s];
+    const long long base = (long long)sptr[s] + 4 * lane;
+    for (int k4 = 0; k4 < L; k4 += 4) {
+        int cc[4];
+        double vv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = k4 + j;
+            if (k < len) {
+                const int src = k < pos ? e0 + k : (k == pos ? e0 + len - 1 : e0 + k - 1);
+                cc[j] = C(src);
+                vv[j] = V(src);
+                last = cc[j];
+            } else {
+                cc[j] = last;
+                vv[j] = 0.0;
+            }
+        }
+        if (k4 == 0) {
+            prev = cc[0];
+            rbase[i] = cc[0];
+        }
+        unsigned short dd[4];
+        double sv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int d = cc[j] - prev;
+            ok = ok && d >= 0 && d <= 65535;
+            dd[j] = (unsigned short)(d >= 0 && d <= 65535 ? d : 0);
+            prev = cc[j];
+            sv[j] = vv[j] * dinv[cc[j]];
+        }
+        const long long e = base + 128LL * (k4 >> 2);
+        *reinterpret_cast<int4*>(col + e) = make_int4(cc[0], cc[1], cc[2], cc[3]);
+        *reinterpret_cast<double2*>(val + e) = make_double2(vv[0], vv[1]);
+        *reinterpret_cast<double2*>(val + e + 2) = make_double2(vv[2], vv[3]);
+        *reinterpret_cast<ushort4*>(dcol + e) = make_ushort4(dd[0], dd[1], dd[2], dd[3]);
+        *reinterpret_cast<double2*>(vals + e) = make_double2(sv[0], sv[1]);
+        *reinterpret_cast<double2*>(vals + e + 2) = make_double2(sv[2], sv[3]);
+        *reinterpret_cast<float4*>(valf + e) =
+            make_float4((float)sv[0], (float)sv[1], (float)sv[2], (float)sv[3]);
     }
     if (!ok) atomicOr(bad, 1);
 }
 
-// Column scaling A D^-1 (Jacobi right preconditioning folded into the matrix).
-template <class T>
-__global__ void k_scale_cols(long long nnz, const int* __restrict__ col, const double* __restrict__ val,
-                             const double* __restrict__ dinv, T* __restrict__ out) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
-        out[e] = (T)(val[e] * dinv[col[e]]);
-}
+
 
 // ---------------------------------------------------------------------------------------
 // Mixed-precision helpers
@@ -1357,27 +1379,26 @@ static void sell_structure(lsmps_ctx* ctx) {
     check_device_flags(ctx, "SELL layout");
     ctx->sell_nslices = ns;
     ctx->sell_entries = total;
-    int* col = ctx->S_col.ensure<int>((size_t)total + 1);
-    double* val = ctx->S_val.ensure<double>((size_t)total + 1);
-    if (ns) {
-        k_sell_fill<<<blocks_for(ns * 32, 256), 256, 0, s>>>(U, ns, ctx->A_row.get<int>(), ctx->A_col.get<int>(),
-                                                             ctx->A_val.get<double>(), sptr, slen, col, val);
-        LSMPS_CHECK_LAUNCH();
-    }
-    // 16-bit column steps when every row ascends with steps below 65536
+    int* col = ctx->S_col.ensure<int>((size_t)total + 8);
+    double* val = ctx->S_val.ensure<double>((size_t)total + 8);
+    double* vals = ctx->S_vals.ensure<double>((size_t)total + 8);
+    float* valf = ctx->S_valf.ensure<float>((size_t)total + 8);
+    unsigned short* dcol = ctx->S_dcol.ensure<unsigned short>((size_t)total + 8);
+    int* rbase = ctx->S_rbase.ensure<int>(ns * 32 + 1);
     ctx->have_steps = false;
     if (ns) {
-        unsigned short* dcol = ctx->S_dcol.ensure<unsigned short>((size_t)total + 8);
-        int* rbase = ctx->S_rbase.ensure<int>(ns * 32 + 1);
         int* bad = ctx->scratch.get<int>() + 46;
         LSMPS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
-        k_sell_steps<<<blocks_for(ns * 32, 256), 256, 0, s>>>(ns, sptr, slen, col, dcol, rbase, bad);
+        k_sell_build<<<(unsigned)((ns + 3) / 4), 128, 0, s>>>(U, ns, ctx->A_row.get<int>(), ctx->A_col.get<int>(),
+                                                              ctx->A_val.get<double>(), ctx->A_dinv.get<double>(), sptr,
+                                                              slen, col, val, dcol, rbase, vals, valf, bad);
         LSMPS_CHECK_LAUNCH();
         int hbad = 1;
         LSMPS_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
         LSMPS_CUDA(cudaStreamSynchronize(s));
         ctx->have_steps = hbad == 0 && ctx->sell_steps_enabled;
     }
+    ctx->have_sell_s = ctx->have_sell_f = true;  // the scaled copies come with the structure
     ctx->have_sell = true;
 }
 
@@ -1398,27 +1419,13 @@ static Sell<double> sell_a64(lsmps_ctx* ctx) {
 
 Sell<double> sell_a64_view(lsmps_ctx* ctx) { return sell_a64(ctx); }
 
-static Sell<double> sell_scaled64(lsmps_ctx* ctx) {
+static Sell<double> sell_scaled64(lsmps_ctx* ctx) {  // A D^-1 in FP64 (built with the structure)
     sell_structure(ctx);
-    if (!ctx->have_sell_s) {
-        double* v = ctx->S_vals.ensure<double>((size_t)ctx->sell_entries + 1);
-        k_scale_cols<double><<<1184, 256, 0, ctx->stream>>>(ctx->sell_entries, ctx->S_col.get<int>(),
-                                                           ctx->S_val.get<double>(), ctx->A_dinv.get<double>(), v);
-        LSMPS_CHECK_LAUNCH();
-        ctx->have_sell_s = true;
-    }
     return sell_view<double>(ctx, ctx->S_vals.get<double>());
 }
 
-static Sell<float> sell_scaled32(lsmps_ctx* ctx) {
+static Sell<float> sell_scaled32(lsmps_ctx* ctx) {  // A D^-1 in FP32 (built with the structure)
     sell_structure(ctx);
-    if (!ctx->have_sell_f) {
-        float* v = ctx->S_valf.ensure<float>((size_t)ctx->sell_entries + 1);
-        k_scale_cols<float><<<1184, 256, 0, ctx->stream>>>(ctx->sell_entries, ctx->S_col.get<int>(),
-                                                          ctx->S_val.get<double>(), ctx->A_dinv.get<double>(), v);
-        LSMPS_CHECK_LAUNCH();
-        ctx->have_sell_f = true;
-    }
     return sell_view<float>(ctx, ctx->S_valf.get<float>());
 }
 

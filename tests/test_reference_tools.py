@@ -1,5 +1,5 @@
 """The reference's own Python tools run on this repository's files (CPU, where the reference
-tree is present; LSMPS_REFERENCE names it, default /root/reference):
+tree is present; the LSMPS_REFERENCE environment variable names it):
 
 * python/validate_outputs.py, unmodified, on the rain validation tables that the GPU step
   series wrote (tests/golden/rain_validation, made by tests/golden/make_rain_validation_fixture.py;
