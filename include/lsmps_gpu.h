@@ -103,6 +103,16 @@ int lsmps_autotune_report(lsmps_ctx* ctx, char* buf, size_t cap, size_t* needed)
 int lsmps_upload_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n);
 /* Same from device pointers already on the context's device (no host copy). */
 int lsmps_upload_particles_device(lsmps_ctx* ctx, const double* d_xyz, const uint8_t* d_type, size_t n);
+/* Double-buffered upload for callers that stream particle sets (the next step's snapshot while
+ * this one is processed): lsmps_prefetch_particles enqueues the host-to-device copies of a set
+ * (from pinned memory, to overlap) on the context's copy stream and returns without waiting;
+ * lsmps_use_prefetched_particles makes it the context's particle set, as lsmps_upload_particles
+ * would, ordering the context stream after the copies. The host buffers must stay unchanged
+ * until the copies are done (the next lsmps_use_prefetched_particles or lsmps_sync). The copy
+ * into the staging buffers waits for the context stream's work enqueued so far, which may still
+ * read the set they held. No reference counterpart (the reference generates its particles). */
+int lsmps_prefetch_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n);
+int lsmps_use_prefetched_particles(lsmps_ctx* ctx);
 
 /* ---- neighbor build + classification ---------------------------------------------- */
 typedef struct lsmps_neighbor_stats {

@@ -80,6 +80,41 @@ void particles_upload(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, si
     ctx->timings[0] = ev_elapsed(ctx, 0, 1);
 }
 
+void particles_prefetch(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n) {
+    LSMPS_REQUIRE(n == 0 || (xyz && type), LSMPS_ERR_ARG, "null particle buffers");
+    LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
+    if (!ctx->copy_stream) {
+        LSMPS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->stage_done, cudaEventDisableTiming));
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming));
+    }
+    // the staging buffers held the set before the last swap: work already enqueued on the
+    // context stream may still read them
+    LSMPS_CUDA(cudaEventRecord(ctx->stage_free, ctx->stream));
+    LSMPS_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->stage_free, 0));
+    double* pos = ctx->stage_pos.ensure<double>(3 * n + 1);
+    uint8_t* t = ctx->stage_type.ensure<uint8_t>(n + 1);
+    if (n) {
+        LSMPS_CUDA(cudaMemcpyAsync(pos, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_stream));
+        LSMPS_CUDA(cudaMemcpyAsync(t, type, n, cudaMemcpyHostToDevice, ctx->copy_stream));
+    }
+    LSMPS_CUDA(cudaEventRecord(ctx->stage_done, ctx->copy_stream));
+    ctx->stage_n = n;
+    ctx->have_stage = true;
+}
+
+void particles_use_prefetched(lsmps_ctx* ctx) {
+    LSMPS_REQUIRE(ctx->have_stage, LSMPS_ERR_STATE, "no prefetched particle set (lsmps_prefetch_particles first)");
+    LSMPS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->stage_done, 0));
+    std::swap(ctx->pos, ctx->stage_pos);
+    std::swap(ctx->type_in, ctx->stage_type);
+    ctx->n = ctx->stage_n;
+    ctx->have_stage = false;
+    ctx->have_neighbors = ctx->have_classes = ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+    ctx->have_candidates = false;
+    ctx->timings[0] = 0.0;  // the copies overlapped other work
+}
+
 }  // namespace lsmps_gpu
 
 using namespace lsmps_gpu;
@@ -141,6 +176,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     lsmps_gpu::DevBuf* bufs[] = {&ctx->dflags, &ctx->scratch, &ctx->scan_tmp, &ctx->host_dummy, &ctx->pos,
                                  &ctx->type_in, &ctx->cell_of, &ctx->slot, &ctx->cell_count, &ctx->cell_start,
                                  &ctx->perm, &ctx->iperm, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->stype,
@@ -158,13 +194,17 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->fr0, &ctx->fp, &ctx->fv, &ctx->fs, &ctx->ft, &ctx->fph, &ctx->fsh,
                                  &ctx->red, &ctx->S_ptr, &ctx->S_len,
                                  &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf, &ctx->nbr_slots,
-                                 &ctx->A_slot_col, &ctx->A_slot_val, &ctx->A_xep};
+                                 &ctx->A_slot_col, &ctx->A_slot_val, &ctx->A_xep, &ctx->stage_pos,
+                                 &ctx->stage_type};
     for (auto* b : bufs) b->release();
     mpnn_destroy(ctx);
     mg_destroy(ctx);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->stage_done) cudaEventDestroy(ctx->stage_done);
+    if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -232,6 +272,14 @@ int lsmps_upload_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* typ
 
 int lsmps_upload_particles_device(lsmps_ctx* ctx, const double* d_xyz, const uint8_t* d_type, size_t n) {
     return guarded(ctx, [&] { particles_upload(ctx, d_xyz, d_type, n, true); });
+}
+
+int lsmps_prefetch_particles(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n) {
+    return guarded(ctx, [&] { particles_prefetch(ctx, xyz, type, n); });
+}
+
+int lsmps_use_prefetched_particles(lsmps_ctx* ctx) {
+    return guarded(ctx, [&] { particles_use_prefetched(ctx); });
 }
 
 int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l0, int flags,

@@ -45,6 +45,12 @@ struct lsmps_ctx {
     cudaStream_t stream = nullptr;
     std::string last_error;
     cudaEvent_t ev[18] = {};
+    // double-buffered particle upload (lsmps_prefetch_particles): staging buffers, copy stream,
+    // copy-done and buffer-free events, created at first use
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t stage_done = nullptr, stage_free = nullptr;
+    size_t stage_n = 0;
+    bool have_stage = false;
     double timings[8] = {};
 
     lsmps_gpu::DevBuf dflags;      // int device error flags
@@ -55,6 +61,7 @@ struct lsmps_ctx {
     // ---- particles ----
     size_t n = 0;
     lsmps_gpu::DevBuf pos, type_in;
+    lsmps_gpu::DevBuf stage_pos, stage_type;  // the prefetched set (swapped in by use_prefetched)
 
     // ---- grid + neighbors ----
     double re = 0, re2 = 0, l0 = 0;

@@ -217,6 +217,8 @@ SIGNATURES = {
     "lsmps_mpnn_save": (C.c_int, [_vp, C.c_char_p]),
     "lsmps_mpnn_load": (C.c_int, [_vp, C.c_char_p]),
     "lsmps_host_generate": (C.c_int, [C.c_char_p, C.c_char_p, _vp, _vp, _vp, C.POINTER(C.c_size_t)]),
+    "lsmps_prefetch_particles": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "lsmps_use_prefetched_particles": (C.c_int, [_vp]),
 }
 
 _LIB = None
@@ -330,6 +332,20 @@ class Context:
         self._types = np.ascontiguousarray(types, dtype=np.uint8)
         self.n = len(self._types)
         self._check(self.L.lsmps_upload_particles(self.h, _p(self._xyz), _p(self._types), self.n))
+
+    def prefetch(self, xyz, types):
+        """lsmps_prefetch_particles: enqueue the copies of the next particle set (keep the arrays
+        alive and unchanged until use_prefetched; pinned arrays let the copies overlap)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        types = np.ascontiguousarray(types, dtype=np.uint8)
+        self._staged = (xyz, types)
+        self._check(self.L.lsmps_prefetch_particles(self.h, _p(xyz), _p(types), len(types)))
+
+    def use_prefetched(self):
+        """lsmps_use_prefetched_particles: the prefetched set becomes the context's particles."""
+        self._check(self.L.lsmps_use_prefetched_particles(self.h))
+        self._xyz, self._types = self._staged
+        self.n = len(self._types)
 
     def build_neighbors(self, re, max_neighbors, l0, classify=True, two_pass=False):
         st = NeighborStats()

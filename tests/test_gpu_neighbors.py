@@ -127,3 +127,30 @@ def test_single_pass_equals_two_pass(ctx, maxn):
     assert (a.pairs, a.truncated, list(a.type_count)) == (b.pairs, b.truncated, list(b.type_count))
     assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
     assert np.array_equal(ta, ctx.types())
+
+
+def test_prefetched_particles_equal_upload(ctx):
+    """lsmps_prefetch_particles / lsmps_use_prefetched_particles: a prefetched set leaves the
+    current one untouched until it is used, then gives the same lists and classes as a plain
+    upload; the staging buffers swap back and forth across repeated prefetches."""
+    sets = [lib.generate(None, case="mixed", particles=120_000, l0=1.0, seed=s)[:2] for s in (1, 2, 3)]
+    want = []
+    for xyz, t in sets:
+        ctx.upload(xyz, t)
+        st = ctx.build_neighbors(2.1, 128, 1.0)
+        want.append((ctx.neighbors(st.pairs), ctx.types()))
+    ctx.upload(*sets[0])
+    ctx.prefetch(*sets[1])
+    st = ctx.build_neighbors(2.1, 128, 1.0)  # still the uploaded set
+    assert np.array_equal(ctx.neighbors(st.pairs)[1], want[0][0][1])
+    for k in (1, 2, 0, 1):
+        ctx.use_prefetched()
+        ctx.prefetch(*sets[(k + 1) % 3])  # overlaps the build of set k
+        st = ctx.build_neighbors(2.1, 128, 1.0)
+        (row, col), cls = ctx.neighbors(st.pairs), ctx.types()
+        assert np.array_equal(row, want[k][0][0]) and np.array_equal(col, want[k][0][1])
+        assert np.array_equal(cls, want[k][1])
+    ctx.use_prefetched()
+    with pytest.raises(lib.LsmpsError) as e:
+        ctx.use_prefetched()  # nothing prefetched
+    assert e.value.code == lib.ERR_STATE
