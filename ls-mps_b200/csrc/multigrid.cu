@@ -491,9 +491,27 @@ __global__ void __launch_bounds__(UP0_THREADS) k_mg_up0(long long U, const int* 
     const int I = agg0[live ? i : i0];
     const int I0 = agg0[i0];
     const int na = agg0[min(i0 + UP0_THREADS - 1, U - 1)] - I0 + 1;  // <= UP0_THREADS
-    for (int q = threadIdx.x; q < na * MG_SLOTS; q += UP0_THREADS) {
-        const int a = q / MG_SLOTS;
-        E[q] = e1[max(nbr1[slot_index(I0 + a, q - a * MG_SLOTS)], 0)];  // empty slots: AP is 0 there
+    const int nq = na * MG_SLOTS;
+    if (nq <= 4 * UP0_THREADS) {
+        // the usual block (up to 37 aggregates): all neighbor-slot indices first, then all
+        // gathers, so that each step's loads are in flight together
+        int idx[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = threadIdx.x + r * UP0_THREADS;
+            const int a = q / MG_SLOTS;
+            idx[r] = q < nq ? nbr1[slot_index(I0 + a, q - a * MG_SLOTS)] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = threadIdx.x + r * UP0_THREADS;
+            if (q < nq) E[q] = e1[max(idx[r], 0)];  // empty slots: AP is 0 there
+        }
+    } else {
+        for (int q = threadIdx.x; q < nq; q += UP0_THREADS) {
+            const int a = q / MG_SLOTS;
+            E[q] = e1[max(nbr1[slot_index(I0 + a, q - a * MG_SLOTS)], 0)];
+        }
     }
     const float eI = e1[I];
     __syncthreads();
