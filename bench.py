@@ -367,6 +367,21 @@ def run_mine(args, dist):
         result["l2_target"] = {"bound": 1e-8, "met": bool(rel_l2 <= 1e-8 and all(
             c["converged"] and c["relative_l2_error"] <= 1e-8 for c in cmp.values()))}
 
+    # ---- the precision form's error against FP64, per result (WLS on the reference's quadratic
+    # field: gradient and Laplacian RMS; the solvers' PPE relative L2 is in ppe_compare) ----
+    if not args.no_compare:
+        re = RE_RATIO * L0
+        wp = {}
+        for name, prec in (("fp64", 0), ("fp32_refined", 1)):
+            ctx.wls(re, L0, mode=1, precision=prec)  # warm (autotuning)
+            w = ctx.wls(re, L0, mode=1, precision=prec)
+            wp[name] = {"ms": ctx.timings()[3], "rms_gradient_error": w.rms_gradient_error,
+                        "max_gradient_error": w.max_gradient_error, "rms_laplacian_error": w.rms_laplacian_error,
+                        "max_laplacian_error": w.max_laplacian_error, "fp64_fallback": int(w.fp64_fallback)}
+        result["wls_precision"] = wp
+        ctx.wls(re, L0, mode=1)  # back to the step's FP64 WLS and its system for the kernel benches
+        ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
+
     # ---- roofline of the dominant kernel (the solver's SpMV) and the other kernels ----
     peak, peak_kind = measured_hbm_peak()
     kern = {}

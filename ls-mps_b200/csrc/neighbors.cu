@@ -688,6 +688,59 @@ __global__ void __launch_bounds__(256) k_slots_compact(int n, int maxn, const in
     for (int p = sub; p < c; p += 8) col[b + p] = __ldcs(src + p);
 }
 
+// Refresh of skin lists in one pass (warp per particle): the candidates j != i of the candidate
+// CSR (radius re + skin, ascending sorted index) that pass the build's exact FP64 test
+// |r_j - r_i|^2 < re^2, in candidate order, go to the particle's slot row (the first maxn),
+// with the sector bits of the kept ones for the classification; counting continues past maxn.
+__global__ void __launch_bounds__(256) k_filter_slots(int n, const int* __restrict__ crow,
+                                                      const int* __restrict__ ccol, const double* __restrict__ sx,
+                                                      const double* __restrict__ sy, const double* __restrict__ sz,
+                                                      const uint8_t* __restrict__ stype, double re2, int maxn,
+                                                      double l0, int classify, int* __restrict__ slots,
+                                                      int* __restrict__ cnt, unsigned long long* trunc,
+                                                      uint8_t* __restrict__ cls) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int nw = (int)((gridDim.x * (size_t)blockDim.x) >> 5);
+    for (int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5); i < n; i += nw) {
+        const double xi = sx[i], yi = sy[i], zi = sz[i];
+        const int c0 = crow[i], c1 = crow[i + 1];
+        int* out = slots + (size_t)i * maxn;
+        int kept = 0;
+        unsigned sec = 0;
+        for (int b = c0; b < c1; b += 32) {
+            const int e = b + lane;
+            bool ok = false;
+            int j = 0;
+            double dx = 0, dy = 0, dz = 0;
+            if (e < c1) {
+                j = ccol[e];
+                dx = xsub(sx[j], xi);
+                dy = xsub(sy[j], yi);
+                dz = xsub(sz[j], zi);
+                ok = j != i && xnorm2(dx, dy, dz) < re2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int p = kept + __popc(m & lt);
+                if (p < maxn) {
+                    out[p] = j;
+                    if (classify) sec |= sector_bits(dx, dy, dz);
+                }
+            }
+            kept += __popc(m);
+        }
+        if (lane == 0) {
+            cnt[i] = min(kept, maxn);
+            if (kept > maxn) atomicAdd(trunc, (unsigned long long)(kept - maxn));
+        }
+        if (classify) {
+            sec = __reduce_or_sync(0xffffffffu, sec);
+            if (lane == 0) cls[i] = classify_rule(stype[i], min(kept, maxn), sec, zi, l0);
+        }
+    }
+}
+
 // Standalone classification over an existing CSR (warp per particle).
 __global__ void __launch_bounds__(NB_WARPS * 32) k_classify(const double* __restrict__ sx,
                                                           const double* __restrict__ sy,
@@ -954,6 +1007,43 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     nb_stats(ctx, out);
     LSMPS_CUDA(cudaStreamSynchronize(s));
     check_device_flags(ctx, "neighbor fill");
+}
+
+bool nb_filter_single(lsmps_ctx* ctx, int classify) {
+    const size_t n = ctx->n;
+    const int maxn = ctx->maxn;
+    if ((double)n * (double)maxn * 4.0 > SLOT_BUDGET_BYTES) return false;
+    cudaStream_t s = ctx->stream;
+    int* dflag = ctx->dflags.get<int>();
+    int* cnt = ctx->nbr_cnt.ensure<int>(n + 1);
+    int* row = ctx->nbr_row.ensure<int>(n + 1);
+    int* slots = ctx->nbr_slots.ensure<int>(n * maxn + 1);
+    uint8_t* cls = ctx->cls.ensure<uint8_t>(n + 1);
+    auto* trunc_d = reinterpret_cast<unsigned long long*>(ctx->scratch.get<int>() + 16);
+    LSMPS_CUDA(cudaMemsetAsync(trunc_d, 0, sizeof(unsigned long long), s));
+    if (n) {
+        const unsigned grid = std::max(1u, std::min<unsigned>(blocks_for(n * 32, 256), 148 * 16));
+        k_filter_slots<<<grid, 256, 0, s>>>((int)n, ctx->cand_row.get<int>(), ctx->cand_col.get<int>(),
+                                            ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
+                                            ctx->stype.get<uint8_t>(), ctx->re2, maxn, ctx->l0, classify, slots, cnt,
+                                            trunc_d, cls);
+        LSMPS_CHECK_LAUNCH();
+    }
+    scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
+    int hpairs = 0;
+    unsigned long long htr = 0;
+    LSMPS_CUDA(cudaMemcpyAsync(&hpairs, row + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaMemcpyAsync(&htr, trunc_d, sizeof(htr), cudaMemcpyDeviceToHost, s));
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    check_device_flags(ctx, "neighbor filter");
+    ctx->pairs = (uint64_t)hpairs;
+    ctx->truncated = htr;
+    int* col = ctx->nbr_col.ensure<int>((size_t)hpairs + 1);
+    if (n) {
+        k_slots_compact<<<(unsigned)((8ull * n + 255) / 256), 256, 0, s>>>((int)n, maxn, slots, row, col);
+        LSMPS_CHECK_LAUNCH();
+    }
+    return true;
 }
 
 void nb_kernel_bench(lsmps_ctx* ctx, int kernel, int reps, double* ms, double* bytes) {

@@ -24,6 +24,9 @@ void nb_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);
 void nb_build_skin(lsmps_ctx* ctx, double re, double skin, int maxn, int maxc, double l0, int flags,
                    lsmps_neighbor_stats* out);
 void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out);
+// the exact lists from the candidate lists in one pass (slot rows, compaction), with the
+// classes when `classify`; false (nothing done) when the slot rows exceed their budget
+bool nb_filter_single(lsmps_ctx* ctx, int classify);
 double nb_max_displacement(lsmps_ctx* ctx);
 void nb_update_positions(lsmps_ctx* ctx, const double* xyz, size_t n, bool device);
 

@@ -139,6 +139,15 @@ void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out) {
     LSMPS_REQUIRE(disp <= 0.5 * ctx->skin * (1.0 - 1e-9), LSMPS_ERR_STATE,
                   "a particle moved " + std::to_string(disp) + " since the candidate build, more than half the skin " +
                       std::to_string(ctx->skin) + ": rebuild with lsmps_build_neighbors_skin");
+    const int classify = (flags & LSMPS_NBR_CLASSIFY) ? 1 : 0;
+    if (nb_filter_single(ctx, classify)) {  // one pass, classes fused
+        ctx->have_neighbors = true;
+        ctx->have_classes = classify != 0;
+        ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
+        nb_stats(ctx, out);
+        check_device_flags(ctx, "neighbor filter");
+        return;
+    }
     cudaStream_t s = ctx->stream;
     const int n = (int)ctx->n;
     const int maxn = ctx->maxn;
