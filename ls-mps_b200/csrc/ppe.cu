@@ -74,14 +74,14 @@ __device__ __forceinline__ bool row_coeff(const PpeParams& P, double xi, double 
     double dx = xsub(xm, xi), dy = xsub(ym, yi), dz = xsub(zm, zi);
     if (P.variant == LSMPS_PPE_WLS) {
         // c = w (q . z) / (r sum_w l0) with w = (re / r - 1)^2 and q . z = P / r, where P is the
-        // polynomial below: c = (re - r)^2 P / (r^4 sum_w l0), one square root and one division
+        // polynomial below: c = (re - r)^2 P / (r^4 sum_w l0), from one reciprocal square root
         const double d2 = dx * dx + dy * dy + dz * dz;
-        const double r = sqrt(d2);
-        if (r <= 1e-12 || r >= P.re) return false;
-        const double t = P.re - r;
+        if (!(d2 > 1e-24) || d2 >= P.re * P.re) return false;  // r <= 1e-12 or r >= re: weight 0
+        const double ir = rsqrt(d2), ir2 = ir * ir;
+        const double t = P.re - d2 * ir;
         const double poly = dx * zk[0] + dy * zk[1] + dz * zk[2] + dx * dx * zk[3] + dy * dy * zk[4] +
                             dz * dz * zk[5] + dx * dy * zk[6] + dx * dz * zk[7] + dy * dz * zk[8];
-        a = (t * t * poly * ws) / (d2 * d2);
+        a = t * t * poly * ws * (ir2 * ir2);
         return a > 0;  // clipped: only c > 0 contributes
     }
     double r = __dsqrt_rn(xnorm2(dx, dy, dz));

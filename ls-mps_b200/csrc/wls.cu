@@ -239,9 +239,8 @@ __device__ __forceinline__ double accumulate_moments(int k, const double* __rest
         int m = col[e];
         double dx = sx[m] - xi, dy = sy[m] - yi, dz = sz[m] - zi;
         double r2 = dx * dx + dy * dy + dz * dz;
-        double r = sqrt(r2);
-        if (r <= 1e-12 || r >= re) continue;
-        double ir = 1.0 / r;
+        if (!(r2 > 1e-24) || r2 >= re * re) continue;  // r <= 1e-12 or r >= re: weight 0
+        double ir = rsqrt(r2);                           // 1 / r without a square root and a division
         double qq = re * ir - 1.0;
         double w = qq * qq;
         double q[K];
@@ -285,9 +284,9 @@ __device__ __forceinline__ double accumulate_moments_rhs(int k, const double* __
         const int m = col[e];
         const double xm = sx[m], ym = sy[m], zm = sz[m];
         const double dx = xm - xi, dy = ym - yi, dz = zm - zi;
-        const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        if (r <= 1e-12 || r >= P.re) continue;
-        const double ir = 1.0 / r;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 > 1e-24) || r2 >= P.re * P.re) continue;  // r <= 1e-12 or r >= re: weight 0
+        const double ir = rsqrt(r2);                         // 1 / r without a square root and a division
         const double qq = P.re * ir - 1.0;
         const double w = qq * qq;
         double q[K];
