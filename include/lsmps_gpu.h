@@ -376,6 +376,15 @@ typedef struct lsmps_projection_stats {
  * with 0). */
 int lsmps_projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* opts,
                           double* d_vel_out, double* d_pressure, lsmps_projection_stats* out);
+/* The viscous and gravity predictor of the fractional-step scheme (the reference's 2-D
+ * provisional_velocity, python/rain_plate_lsmps_cpu.py:184-196, in 3-D): u* = u + dt (nu lap u
+ * + gravity) with lap u of each component from the all-particle WLS of the velocity,
+ * (x3 + x4 + x5) / l0; walls keep u; splash particles (no WLS) fall freely (u + dt gravity).
+ * d_vel / d_vel_out: n x 3 device arrays, caller order; gravity: 3 host doubles; flags:
+ * LSMPS_PPE_WALL_NEUMANN gives wall neighbors the particle's own velocity in the WLS (the
+ * mirrored wall value). Needs neighbor lists and classes. */
+int lsmps_predict_velocity(lsmps_ctx* ctx, const double* d_vel, double dt, double nu, const double* gravity, int flags,
+                           double* d_vel_out);
 
 /* ---- step series (rain-on-plate proxy) ------------------------------------------------ */
 /* A 3-D step series on one context: wall fixed, droplets fall droplet_speed l0 per step and

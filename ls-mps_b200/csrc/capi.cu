@@ -460,6 +460,11 @@ int lsmps_projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double
     return guarded(ctx, [&] { projection_step(ctx, d_vel, dt, rho, opts, d_vel_out, d_pressure, out); });
 }
 
+int lsmps_predict_velocity(lsmps_ctx* ctx, const double* d_vel, double dt, double nu, const double* gravity, int flags,
+                           double* d_vel_out) {
+    return guarded(ctx, [&] { predict_velocity(ctx, d_vel, dt, nu, gravity, flags, d_vel_out); });
+}
+
 int lsmps_ppe_manufacture(lsmps_ctx* ctx, const double* params, int nmodes) {
     return guarded(ctx, [&] { ppe_manufacture(ctx, params, nmodes); });
 }

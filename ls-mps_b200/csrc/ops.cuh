@@ -36,6 +36,8 @@ void wls_download(lsmps_ctx* ctx, double* x, int32_t* status, double* z, double*
 void wls_fields(lsmps_ctx* ctx, const double* d_fields, int nrhs, double* d_out, bool mirror_walls = false);
 void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* so,
                      double* d_vel_out, double* d_pressure, lsmps_projection_stats* out);
+void predict_velocity(lsmps_ctx* ctx, const double* d_vel, double dt, double nu, const double* g, int flags,
+                      double* d_vel_out);
 
 // ppe.cu
 void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);

@@ -141,9 +141,45 @@ __global__ void k_correct(size_t n, const uint8_t* __restrict__ type, const doub
     }
 }
 
+// u* = u + dt (nu lap u + g); lap u of each component from its WLS solution, (x3 + x4 + x5) / l0
+// (zero where the WLS is skipped or failed: splash particles fall freely); walls keep u
+__global__ void k_predict(size_t n, const uint8_t* __restrict__ type, const double* __restrict__ u,
+                          const double* __restrict__ G, double l0inv, double dt, double nu, double3 g,
+                          double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const bool wall = type[i] == LSMPS_WALL;
+        const double ga[3] = {g.x, g.y, g.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double* x = G + (i * 3 + a) * KB;
+            const double lap = (x[3] + x[4] + x[5]) * l0inv;
+            out[3 * i + a] = wall ? u[3 * i + a] : u[3 * i + a] + dt * (nu * lap + ga[a]);
+        }
+    }
+}
+
 unsigned grid_n(size_t n) { return std::max(1u, std::min<unsigned>(blocks_for(n, 256), 148 * 8)); }
 
 }  // namespace
+
+void predict_velocity(lsmps_ctx* ctx, const double* d_vel, double dt, double nu, const double* g, int flags,
+                      double* d_vel_out) {
+    LSMPS_REQUIRE(ctx->have_neighbors && ctx->have_classes, LSMPS_ERR_STATE,
+                  "the predictor needs neighbor lists and classification first");
+    LSMPS_REQUIRE(dt > 0 && std::isfinite(dt) && nu >= 0 && std::isfinite(nu) && g, LSMPS_ERR_ARG,
+                  "predictor: dt > 0, nu >= 0 and a gravity vector");
+    LSMPS_REQUIRE((flags & ~LSMPS_PPE_WALL_NEUMANN) == 0, LSMPS_ERR_ARG, "predictor flags");
+    const size_t n = ctx->n;
+    LSMPS_REQUIRE(n == 0 || (d_vel && d_vel_out), LSMPS_ERR_ARG, "null velocity buffer");
+    double* G = ctx->pj_grad.ensure<double>(n * 3 * KB + 1);
+    wls_fields(ctx, d_vel, 3, G, (flags & LSMPS_PPE_WALL_NEUMANN) != 0);
+    if (n) {
+        k_predict<<<grid_n(n), 256, 0, ctx->stream>>>(n, ctx->type_in.get<uint8_t>(), d_vel, G, 1.0 / ctx->l0, dt, nu,
+                                                      make_double3(g[0], g[1], g[2]), d_vel_out);
+        LSMPS_CHECK_LAUNCH();
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
 
 void projection_step(lsmps_ctx* ctx, const double* d_vel, double dt, double rho, const lsmps_solver_opts* so,
                      double* d_vel_out, double* d_pressure, lsmps_projection_stats* out) {

@@ -218,6 +218,7 @@ SIGNATURES = {
     "lsmps_mpnn_load": (C.c_int, [_vp, C.c_char_p]),
     "lsmps_host_generate": (C.c_int, [C.c_char_p, C.c_char_p, _vp, _vp, _vp, C.POINTER(C.c_size_t)]),
     "lsmps_prefetch_particles": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "lsmps_predict_velocity": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]),
     "lsmps_use_prefetched_particles": (C.c_int, [_vp]),
 }
 
@@ -479,6 +480,18 @@ class Context:
         self._check(self.L.lsmps_wls_fields(self.h, C.c_void_p(f.data_ptr()), f.shape[1],
                                             C.c_void_p(out.data_ptr())))
         self.sync()
+        return out
+
+    def predict_velocity(self, vel, dt, nu, gravity=(0.0, 0.0, -9.81), wall_neumann=False):
+        """lsmps_predict_velocity: u* = u + dt (nu lap u + gravity) (n x 3, caller order; torch tensor out)."""
+        import torch
+
+        u = torch.as_tensor(vel, dtype=torch.float64, device="cuda").reshape(-1, 3).contiguous()
+        out = torch.empty_like(u)
+        g = np.ascontiguousarray(gravity, dtype=np.float64)
+        torch.cuda.synchronize()
+        self._check(self.L.lsmps_predict_velocity(self.h, C.c_void_p(u.data_ptr()), dt, nu, _p(g),
+                                                  PPE_WALL_NEUMANN if wall_neumann else 0, C.c_void_p(out.data_ptr())))
         return out
 
     def projection_step(self, vel, dt, rho, solver="mixed", max_iter=20000, tol=1e-10, warm_start=False):

@@ -270,6 +270,20 @@ class Oracle:
         return x, st
 
     @classmethod
+    def predict_velocity(cls, xyz, types, row, col, re, l0, vel, dt, nu, gravity, mirror_walls=False):
+        """The viscous / gravity predictor (python/rain_plate_lsmps_cpu.py:184-196, in 3-D):
+        u* = u + dt (nu lap u + g), lap u of each component = (x3 + x4 + x5) / l0 of its WLS
+        solution (the basis keeps l0 f_aa in x3..x5), zero where the WLS is skipped or failed;
+        wall particles keep u."""
+        vel = np.asarray(vel, dtype=np.float64).reshape(-1, 3)
+        x, st = cls.wls_fields(xyz, types, row, col, re, l0, vel, mirror_walls=mirror_walls)
+        lap = (x[:, :, 3] + x[:, :, 4] + x[:, :, 5]) / l0
+        out = vel + dt * (nu * lap + np.asarray(gravity, dtype=np.float64)[None, :])
+        walls = np.asarray(types) == 4  # Wall
+        out[walls] = vel[walls]
+        return out
+
+    @classmethod
     def ppe_assemble(cls, variant, xyz, types, row, col, re, l0, max_unknowns, diag_shift=0.0,
                      z=None, wsum=None, wls_status=None):
         L = cls.lib()

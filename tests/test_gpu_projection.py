@@ -148,3 +148,38 @@ def test_projection_neumann_walls(built):
     walls = cls == lib.WALL
     uref[walls] = ustar[walls]
     assert np.linalg.norm(u - uref) <= 1e-6 * np.linalg.norm(uref)
+
+
+def _quadratic_velocity(xyz):
+    """A quadratic velocity field: lap u = (0.2, 0.06, 0.08) everywhere."""
+    x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    return np.stack([0.1 * x * x + 0.05 * y * z, 0.03 * y * y - 0.02 * x * z, 0.04 * z * z + 0.01 * x * y], 1)
+
+
+@pytest.mark.parametrize("neumann", [False, True])
+def test_predict_velocity(built, neumann):
+    """lsmps_predict_velocity (the reference's provisional_velocity, in 3-D) on a lattice block on
+    three wall layers: equals the oracle's u + dt (nu lap u + g) to 1e-12 of |u*|, walls keep u,
+    and deep inside the fluid the WLS Laplacian of the quadratic field is the exact one."""
+    pytest.importorskip("torch")
+    xyz = jittered_lattice(20, jitter=0.1, seed=11)
+    t = np.zeros(len(xyz), np.uint8)
+    t[xyz[:, 2] < 3.0] = lib.WALL
+    u = _quadratic_velocity(xyz)
+    dt, nu, g = 0.01, 0.5, (0.0, 0.0, -9.81)
+    with lib.Context(0) as ctx:
+        ctx.upload(xyz, t)
+        ctx.build_neighbors(RE, 128, L0)
+        cls = ctx.types()
+        us = ctx.predict_velocity(u, dt, nu, g, wall_neumann=neumann).cpu().numpy()
+    row, col, _ = Oracle.neighbors(xyz, RE, 128)
+    ref = Oracle.predict_velocity(xyz, cls, row, col, RE, L0, u, dt, nu, g, mirror_walls=neumann)
+    assert np.abs(us - ref).max() <= 1e-12 * np.abs(ref).max()
+    walls = cls == lib.WALL
+    assert walls.sum() > 1000 and np.array_equal(us[walls], u[walls])
+    # interior particles whose support lies inside the fluid: the quadratic is reproduced
+    lo, hi = xyz.min(0), xyz.max(0)
+    deep = (~walls) & np.all(xyz > lo + np.array([3, 3, 6]), 1) & np.all(xyz < hi - 3, 1)
+    assert deep.sum() > 100
+    lap = (us[deep] - u[deep]) / dt - np.array(g)
+    assert np.abs(lap / nu - np.array([0.2, 0.06, 0.08])).max() < 1e-5

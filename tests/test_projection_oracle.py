@@ -66,3 +66,30 @@ def test_neumann_walls_remove_the_divergence_next_to_the_wall(built):
     n1b, n1a, n2b, n2a = out[3]
     assert d1a > 0.5 * d1b
     assert n1a <= 0.25 * n1b and n2a <= 0.05 * n2b
+
+
+def test_predictor_reproduces_a_quadratic_laplacian(built):
+    """The oracle's predictor (python/rain_plate_lsmps_cpu.py:184-196, in 3-D): deep in the fluid
+    the WLS Laplacian of a quadratic velocity is exact (the second-order basis reproduces it), so
+    u* - u = dt (nu lap u + g) to round-off; wall particles keep u; with Dirichlet walls the
+    predictor differs next to the wall from the mirrored (Neumann) one."""
+    xyz = jittered_lattice(16, jitter=0.1, seed=11)
+    t = np.zeros(len(xyz), np.uint8)
+    t[xyz[:, 2] < 3.0] = WALL
+    row, col, _ = Oracle.neighbors(xyz, RE, 128)
+    cls = Oracle.classify(xyz, t, row, col, L0)
+    x, y, z = xyz.T
+    u = np.stack([0.1 * x * x + 0.05 * y * z, 0.03 * y * y - 0.02 * x * z, 0.04 * z * z + 0.01 * x * y], 1)
+    dt, nu, g = 0.01, 0.5, np.array([0.0, 0.0, -9.81])
+    us = {m: Oracle.predict_velocity(xyz, cls, row, col, RE, L0, u, dt, nu, g, mirror_walls=m) for m in (False, True)}
+    walls = cls == WALL
+    lo, hi = xyz.min(0), xyz.max(0)
+    deep = (~walls) & np.all(xyz > lo + np.array([3, 3, 6]), 1) & np.all(xyz < hi - 3, 1)
+    assert deep.sum() > 50 and walls.sum() == 16 * 16 * 3
+    for m in (False, True):
+        assert np.array_equal(us[m][walls], u[walls])
+        lap = ((us[m][deep] - u[deep]) / dt - g) / nu
+        assert np.abs(lap - np.array([0.2, 0.06, 0.08])).max() < 1e-9
+    near = (~walls) & (xyz[:, 2] < 4.5)
+    assert np.abs(us[False][near] - us[True][near]).max() > 1e-4
+    assert np.array_equal(us[False][deep], us[True][deep])
