@@ -113,13 +113,17 @@ __device__ __forceinline__ T warp_sum(T v) {
 }
 
 // Programmatic dependent launch (sm_90+): a kernel launched with launch_pdl may start while
-// the kernel before it in the stream drains. It calls pdl_begin() first: that lets the next
-// PDL kernel launch once every block of this one has started, then waits until the previous
-// kernel has completed and its writes are visible. Launched without the attribute, both
-// instructions return at once.
+// the kernel before it in the stream drains. It calls pdl_begin() first: that waits until the
+// previous kernel has completed and its writes are visible, then lets the next PDL kernel
+// launch once every block of this one has passed the wait. So at most one grid waits ahead of
+// the running one. Triggering before the wait let a whole chain of dependent grids launch
+// ahead and hold SM slots while the running kernel still worked, and the grids that then found
+// their slots late ran unevenly spread over the SMs (measured on the multigrid BiCGStab at 1M:
+// 12.8 ms per solve against 10.1 ms with the wait first, 10.8 ms without PDL). Launched
+// without the attribute, both instructions return at once.
 __device__ __forceinline__ void pdl_begin() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 template <class... KArgs, class... Args>

@@ -668,7 +668,7 @@ int mg_launches_per_apply(lsmps_ctx* ctx, bool restricted) {
 
 MgFine mg_fine(lsmps_ctx* ctx) {
     MgState& M = *ctx->mg;
-    return MgFine{M.L[1].n, M.ustart.get<int>(), M.L[1].r.get<float>()};
+    return MgFine{M.L[1].n, M.ustart.get<int>(), M.agg0.get<int>(), M.L[1].r.get<float>()};
 }
 
 // out = D M z on the context stream (z, out: U doubles); gated by the solver scalars S

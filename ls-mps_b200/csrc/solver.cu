@@ -445,41 +445,91 @@ __global__ void __launch_bounds__(RB) k_bcg_s(long long n, const T* __restrict__
     }
 }
 
-// With the multigrid: p = r + beta (p - omega v) and its restriction r1 = P^T p in one pass,
-// one thread per level-1 aggregate over its contiguous rows.
+// With the multigrid, the p and s updates also restrict the new vector to level 1
+// (r1 = P^T p, a sum over each aggregate's contiguous rows). A warp takes AGG_W consecutive
+// aggregates, i.e. the rows ustart[Ia] .. ustart[Ia + AGG_W], and walks them 32 consecutive rows
+// per step, so every load and store is coalesced. A segmented shuffle scan sums each step's
+// rows per aggregate and the segment's last lane adds that sum into the aggregate's shared-
+// memory slot; steps run in order, so the summation order is fixed.
+constexpr int AGG_W = 16;  // aggregates per warp task
+
+inline unsigned agg_blocks(long long n1) {
+    return (unsigned)(((n1 + AGG_W - 1) / AGG_W + RB / 32 - 1) / (RB / 32));
+}
+
+// Calls f(i) (which returns the new value of row i) for every row of aggregates [Ia, Ib) and
+// returns, in lane l < Ib - Ia, the sum over aggregate Ia + l. `sh` is the warp's AGG_W slots.
+template <class F>
+__device__ __forceinline__ double warp_agg_sums(const MgFine& G, long long Ia, long long Ib, double* sh, F&& f) {
+    const int lane = threadIdx.x & 31;
+    if (lane < AGG_W) sh[lane] = 0.0;
+    __syncwarp();
+    const int rb = G.ustart[Ia], re = G.ustart[Ib];
+    for (int base = rb; base < re; base += 32) {
+        const int i = base + lane;
+        double x = 0.0;
+        int a = AGG_W + lane;  // past the last row: a key of its own, never part of a segment
+        if (i < re) {
+            x = f(i);
+            a = G.agg0[i] - (int)Ia;
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {  // inclusive scan within runs of equal a
+            const double y = __shfl_up_sync(0xffffffffu, x, o);
+            const int ay = __shfl_up_sync(0xffffffffu, a, o);
+            if (lane >= o && ay == a) x += y;
+        }
+        const int an = __shfl_down_sync(0xffffffffu, a, 1);
+        if (i < re && (lane == 31 || an != a)) sh[a] += x;
+        __syncwarp();
+    }
+    const double sum = lane < AGG_W ? sh[lane] : 0.0;
+    __syncwarp();  // before the next task clears the slots
+    return sum;
+}
+
 __global__ void __launch_bounds__(RB) k_bcg_p_agg(MgFine G, const double* __restrict__ r, double* __restrict__ p,
                                                   const double* __restrict__ v, const BcgScalars* S) {
     pdl_begin();
     if (S->done) return;
+    __shared__ double sh[RB / 32][AGG_W];
     const double beta = S->beta, omega = S->omega;
-    for (long long I = blockIdx.x * (long long)RB + threadIdx.x; I < G.n1; I += (long long)gridDim.x * RB) {
-        double a = 0;
-        for (int i = G.ustart[I], e = G.ustart[I + 1]; i < e; ++i) {
+    const int lane = threadIdx.x & 31;
+    const long long nt = (G.n1 + AGG_W - 1) / AGG_W;
+    for (long long task = (blockIdx.x * (long long)RB + threadIdx.x) >> 5; task < nt;
+         task += ((long long)gridDim.x * RB) >> 5) {
+        const long long Ia = task * AGG_W, Ib = min(Ia + AGG_W, G.n1);
+        const double a = warp_agg_sums(G, Ia, Ib, sh[threadIdx.x >> 5], [&](int i) {
             const double pi = r[i] + beta * (p[i] - omega * v[i]);
             p[i] = pi;
-            a += pi;
-        }
-        G.r1[I] = (float)a;
+            return pi;
+        });
+        if (Ia + lane < Ib) G.r1[Ia + lane] = (float)a;
     }
 }
 
-// With the multigrid: s = r - alpha v, |s|, and r1 = P^T s in one pass (as k_bcg_p_agg).
+// s = r - alpha v, |s|, and r1 = P^T s in one pass (grid at most RGRID blocks: one partial
+// sum of |s|^2 per block).
 __global__ void __launch_bounds__(RB) k_bcg_s_agg(MgFine G, const double* __restrict__ r,
                                                   const double* __restrict__ v, double* __restrict__ s,
                                                   BcgScalars* S, Partials P) {
     pdl_begin();
     if (S->done) return;
+    __shared__ double sh[RB / 32][AGG_W];
     const double alpha = S->alpha;
+    const int lane = threadIdx.x & 31;
+    const long long nt = (G.n1 + AGG_W - 1) / AGG_W;
     double acc = 0;
-    for (long long I = blockIdx.x * (long long)RB + threadIdx.x; I < G.n1; I += (long long)gridDim.x * RB) {
-        double a = 0;
-        for (int i = G.ustart[I], e = G.ustart[I + 1]; i < e; ++i) {
+    for (long long task = (blockIdx.x * (long long)RB + threadIdx.x) >> 5; task < nt;
+         task += ((long long)gridDim.x * RB) >> 5) {
+        const long long Ia = task * AGG_W, Ib = min(Ia + AGG_W, G.n1);
+        const double a = warp_agg_sums(G, Ia, Ib, sh[threadIdx.x >> 5], [&](int i) {
             const double si = r[i] - alpha * v[i];
             s[i] = si;
             acc += si * si;
-            a += si;
-        }
-        G.r1[I] = (float)a;
+            return si;
+        });
+        if (Ia + lane < Ib) G.r1[Ia + lane] = (float)a;
     }
     if (block_partials(acc, 0.0, P, &S->counter[1])) {
         double ss, unused;
@@ -1157,7 +1207,8 @@ void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V, bool mg = false) 
     const T* sv = V.s;
     if constexpr (std::is_same<T, double>::value) {
         if (mg) {  // p and its level-1 restriction in one pass, then the rest of the V-cycle
-            launch_pdl(k_bcg_p_agg, RGRID, RB, 0, E.s, mg_fine(E.ctx), V.r, V.p, V.v, E.S);
+            const MgFine G = mg_fine(E.ctx);
+            launch_pdl(k_bcg_p_agg, agg_blocks(G.n1), RB, 0, E.s, G, V.r, V.p, V.v, E.S);
             mg_apply(E.ctx, V.p, V.ph, E.S, 0, true);
             pv = V.ph;
         }
@@ -1167,7 +1218,9 @@ void iteration(Engine& E, const Sell<TM>& A, const Vecs<T>& V, bool mg = false) 
     else launch_pdl(k_bcg_v<T, TM, false>, RGRID, RB, 0, E.s, A, pv, V.v, V.r0, E.S, E.P);
     if constexpr (std::is_same<T, double>::value) {
         if (mg) {
-            launch_pdl(k_bcg_s_agg, RGRID, RB, 0, E.s, mg_fine(E.ctx), V.r, V.v, V.s, E.S, E.P);
+            const MgFine G = mg_fine(E.ctx);
+            launch_pdl(k_bcg_s_agg, std::min<unsigned>(RGRID, agg_blocks(G.n1)), RB, 0, E.s, G, V.r, V.v, V.s, E.S,
+                       E.P);
             mg_apply(E.ctx, V.s, V.sh, E.S, 1, true);
             sv = V.sh;
         }

@@ -44,11 +44,13 @@ struct Sell {
 // The assembled system's SELL copy with FP64 values of A (built on first use).
 Sell<double> sell_a64_view(lsmps_ctx* ctx);
 
-// The multigrid's level-1 aggregates (contiguous row ranges ustart[I] .. ustart[I+1]) and its
-// level-1 right-hand side, for solver kernels that restrict a vector while producing it.
+// The multigrid's level-1 aggregates (contiguous row ranges ustart[I] .. ustart[I+1], and each
+// row's aggregate agg0[i]) and its level-1 right-hand side, for solver kernels that restrict a
+// vector while producing it.
 struct MgFine {
     long long n1;
     const int* ustart;
+    const int* agg0;
     float* r1;
 };
 MgFine mg_fine(lsmps_ctx* ctx);
