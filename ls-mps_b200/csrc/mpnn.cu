@@ -204,7 +204,8 @@ __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ 
 //      staged with h_i as the bf16 A tile [h | m] (16 x 128) in shared memory;
 //   2. z = [h | m] W^T on the tensor cores (8 k-steps x 8 n-tiles of m16n8k16);
 //   3. h_out = h + ReLU(z + b) (bf16), with [h | m] and z kept for the backward pass.
-// 2 NB neighbor-row gathers in flight per warp (a launch-shape parameter: same bits for every NB)
+// 4 NB neighbor-row gathers in flight per warp, 16 bytes per lane (a launch-shape parameter:
+// same bits for every NB)
 template <int NB>
 __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out,
                                                    const bf16* __restrict__ Wl, const float* __restrict__ bl,
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
                 wj = G.ew[e0 + lane];
             }
         };
-        const int half = lane >> 4, sub = lane & 15;  // half-warp per neighbor row, 4 features per lane
+        const int quad = lane >> 3, sub = lane & 7;  // 8 lanes per neighbor row, 8 features (16 B) per lane
         int cj, ne, e0;
         float wj;
         fetch(0, cj, wj, ne, e0);
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
             if (t < 15) fetch(t + 1, cjn, wjn, nen, e0n);  // in flight during node t's gathers
             __nv_bfloat162 own = __floats2bfloat162_rn(0.f, 0.f);
             if (i < G.U) own = *reinterpret_cast<const __nv_bfloat162*>(h_in + i * H + 2 * lane);
-            float m[4] = {0.f, 0.f, 0.f, 0.f};
+            float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             for (int eb = 0; eb < ne; eb += 32) {
                 if (eb) {  // rows of more than 32 edges
                     cj = 0;
@@ -260,38 +261,47 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
                     }
                 }
                 const int nb = min(32, ne - eb);
-                for (int k = 0; k < nb; k += 2 * NB) {
-                    uint2 a[NB];
+                // each lane sums the edges quad, quad + 4, ... of the chunk in ascending order
+                // (the same order for every NB); 4 NB rows in flight per warp
+                for (int k = 0; k < nb; k += 4 * NB) {
+                    uint4 a[NB];
                     float w[NB];
 #pragma unroll
                     for (int q = 0; q < NB; ++q) {
-                        const int edge = k + 2 * q + half;
+                        const int edge = k + 4 * q + quad;
                         const int src = min(edge, nb - 1);
                         const int j = __shfl_sync(0xffffffffu, cj, src);
                         const float wq = __shfl_sync(0xffffffffu, wj, src);
                         w[q] = edge < nb ? wq : 0.f;
-                        a[q] = *reinterpret_cast<const uint2*>(h_in + (long long)j * H + 4 * sub);
+                        a[q] = *reinterpret_cast<const uint4*>(h_in + (long long)j * H + 8 * sub);
                     }
 #pragma unroll
                     for (int q = 0; q < NB; ++q) {
-                        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a[q].x));
-                        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a[q].y));
-                        m[0] += w[q] * lo.x;
-                        m[1] += w[q] * lo.y;
-                        m[2] += w[q] * hi.x;
-                        m[3] += w[q] * hi.y;
+                        const unsigned u[4] = {a[q].x, a[q].y, a[q].z, a[q].w};
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[c]));
+                            m[2 * c] += w[q] * f.x;
+                            m[2 * c + 1] += w[q] * f.y;
+                        }
                     }
                 }
             }
 #pragma unroll
-            for (int c = 0; c < 4; ++c) m[c] += __shfl_xor_sync(0xffffffffu, m[c], 16);  // even + odd edges
+            for (int c = 0; c < 8; ++c) {  // the four edge classes: (0 + 1) + (2 + 3)
+                m[c] += __shfl_xor_sync(0xffffffffu, m[c], 8);
+                m[c] += __shfl_xor_sync(0xffffffffu, m[c], 16);
+            }
             *reinterpret_cast<__nv_bfloat162*>(A + t * LDA + 2 * lane) = own;
-            if (half == 0) {
-                __nv_bfloat162 p0 = __floats2bfloat162_rn(m[0], m[1]), p1 = __floats2bfloat162_rn(m[2], m[3]);
-                uint2 pk;
-                pk.x = *reinterpret_cast<unsigned*>(&p0);
-                pk.y = *reinterpret_cast<unsigned*>(&p1);
-                *reinterpret_cast<uint2*>(A + t * LDA + H + 4 * sub) = pk;
+            if (quad == 0) {
+                uint4 pk;
+                unsigned* pw = reinterpret_cast<unsigned*>(&pk);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    __nv_bfloat162 b2 = __floats2bfloat162_rn(m[2 * c], m[2 * c + 1]);
+                    pw[c] = *reinterpret_cast<unsigned*>(&b2);
+                }
+                *reinterpret_cast<uint4*>(A + t * LDA + H + 8 * sub) = pk;
             }
             cj = cjn;
             wj = wjn;
