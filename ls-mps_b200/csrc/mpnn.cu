@@ -200,19 +200,27 @@ __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ 
 }
 
 // One message-passing layer, one warp per 16-node tile:
-//   1. aggregation m_i = sum_j w_ij h_j (each lane owns two of the 64 features; FP32),
+//   1. aggregation m_i = sum_j w_ij h_j (8 lanes per neighbor row, 8 features per lane; FP32),
 //      staged with h_i as the bf16 A tile [h | m] (16 x 128) in shared memory;
 //   2. z = [h | m] W^T on the tensor cores (8 k-steps x 8 n-tiles of m16n8k16);
 //   3. h_out = h + ReLU(z + b) (bf16), with [h | m] and z kept for the backward pass.
-// 4 NB neighbor-row gathers in flight per warp, 16 bytes per lane (a launch-shape parameter:
-// same bits for every NB)
-template <int NB>
-__global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out,
-                                                   const bf16* __restrict__ Wl, const float* __restrict__ bl,
-                                                   bf16* __restrict__ a_save, float* __restrict__ z_save) {
-    __shared__ __align__(16) bf16 Ws[H * LDA];
-    __shared__ __align__(16) bf16 As[4][16 * LDA];
-    __shared__ float bs[H];
+// Launch shape (the autotuner's choice; every shape gives the same bits, since each node's
+// sums run in the same order and an MMA row depends only on its own A row):
+//   NB     4 NB neighbor-row gathers in flight per warp, 16 bytes per lane;
+//   WARPS  warps per block (dynamic shared memory: W, the bias and one A tile per warp);
+//   LOCAL  false: warp w of block b takes the 16 consecutive nodes of tile 4 b + w (grid-
+//          stride); true: the block takes WARPS * 16 consecutive nodes and warp w the nodes
+//          w, w + WARPS, ..., so the block's warps gather the neighbors of a few consecutive
+//          nodes at a time and those rows (shared by ~3 nodes each in the cell-sorted order)
+//          are re-read from L1 instead of L2.
+template <int NB, int WARPS, bool LOCAL>
+__global__ void __launch_bounds__(WARPS * 32, 24 / WARPS)
+    k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out, const bf16* __restrict__ Wl,
+                const float* __restrict__ bl, bf16* __restrict__ a_save, float* __restrict__ z_save) {
+    extern __shared__ __align__(16) unsigned char layer_smem[];
+    bf16* Ws = reinterpret_cast<bf16*>(layer_smem);          // H x LDA
+    bf16* As = Ws + H * LDA;                                 // WARPS tiles of 16 x LDA
+    float* bs = reinterpret_cast<float*>(As + WARPS * 16 * LDA);  // H
     for (int k = threadIdx.x; k < H * KIN / 8; k += blockDim.x) {
         const int n = k / (KIN / 8), c = (k % (KIN / 8)) * 8;
         *reinterpret_cast<uint4*>(Ws + n * LDA + c) = *reinterpret_cast<const uint4*>(Wl + n * KIN + c);
@@ -221,17 +229,30 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tq = lane & 3;
-    bf16* A = As[warp];
-    const long long ntiles = (G.U + 15) / 16;
-    for (long long tile = blockIdx.x * 4LL + warp; tile < ntiles; tile += gridDim.x * 4LL) {
-        const long long base = tile * 16;
-        // row pointers of the tile's 16 nodes in one load (row has U + 1 entries)
-        const int rp = lane <= 16 ? G.row[min(base + lane, G.U)] : 0;
+    bf16* A = As + warp * 16 * LDA;
+    constexpr long long SPAN = LOCAL ? WARPS * 16 : 16;  // nodes per job
+    const long long njobs = (G.U + SPAN - 1) / SPAN;
+    const long long j0 = LOCAL ? (long long)blockIdx.x : blockIdx.x * (long long)WARPS + warp;
+    const long long js = LOCAL ? (long long)gridDim.x : (long long)gridDim.x * WARPS;
+    // node of row t of this warp's tile in job `job`
+    auto node = [&](long long job, int t) -> long long {
+        return LOCAL ? job * SPAN + warp + (long long)WARPS * t : job * SPAN + t;
+    };
+    for (long long job = j0; job < njobs; job += js) {
+        // first and one-past-last entry of node t's row in lane t (rows have U + 1 pointers)
+        int rs = 0, re = 0;
+        if (lane < 16) {
+            const long long i = node(job, lane);
+            if (i < G.U) {
+                rs = G.row[i];
+                re = G.row[i + 1];
+            }
+        }
         // (col, weight) of up to 32 edges of node t, one per lane; the diagonal (the row's last
         // entry) has no edge
         auto fetch = [&](int t, int& cj, float& wj, int& ne, int& e0) {
-            e0 = __shfl_sync(0xffffffffu, rp, t);
-            ne = max(__shfl_sync(0xffffffffu, rp, t + 1) - 1 - e0, 0);
+            e0 = __shfl_sync(0xffffffffu, rs, t);
+            ne = max(__shfl_sync(0xffffffffu, re, t) - 1 - e0, 0);
             cj = 0;
             wj = 0.f;
             if (lane < min(ne, 32)) {
@@ -244,13 +265,13 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
         float wj;
         fetch(0, cj, wj, ne, e0);
         for (int t = 0; t < 16; ++t) {
-            const long long i = base + t;
+            const long long i = node(job, t);
             int cjn = 0, nen = 0, e0n = 0;
             float wjn = 0.f;
             if (t < 15) fetch(t + 1, cjn, wjn, nen, e0n);  // in flight during node t's gathers
             __nv_bfloat162 own = __floats2bfloat162_rn(0.f, 0.f);
             if (i < G.U) own = *reinterpret_cast<const __nv_bfloat162*>(h_in + i * H + 2 * lane);
-            float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float2 m2[4] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // features (2c, 2c + 1)
             for (int eb = 0; eb < ne; eb += 32) {
                 if (eb) {  // rows of more than 32 edges
                     cj = 0;
@@ -277,15 +298,23 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
                     }
 #pragma unroll
                     for (int q = 0; q < NB; ++q) {
+                        // a bf16 is the upper half of the float it rounds: the low element of a
+                        // pair is u << 16, the high one u with its low half cleared (exact)
                         const unsigned u[4] = {a[q].x, a[q].y, a[q].z, a[q].w};
+                        const float2 ww = make_float2(w[q], w[q]);
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
-                            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[c]));
-                            m[2 * c] += w[q] * f.x;
-                            m[2 * c + 1] += w[q] * f.y;
+                            const float2 f = make_float2(__uint_as_float(u[c] << 16), __uint_as_float(u[c] & 0xffff0000u));
+                            m2[c] = __ffma2_rn(ww, f, m2[c]);  // two FP32 FMAs in one instruction
                         }
                     }
                 }
+            }
+            float m[8];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                m[2 * c] = m2[c].x;
+                m[2 * c + 1] = m2[c].y;
             }
 #pragma unroll
             for (int c = 0; c < 8; ++c) {  // the four edge classes: (0 + 1) + (2 + 3)
@@ -329,7 +358,7 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
                 const int t = g + 8 * half;
-                const long long i = base + t;
+                const long long i = node(job, t);
                 if (i >= G.U) continue;
                 const int c = nt * 8 + 2 * tq;
                 const float z0 = acc[nt][2 * half] + bs[c], z1 = acc[nt][2 * half + 1] + bs[c + 1];
@@ -341,7 +370,7 @@ __global__ void __launch_bounds__(128) k_layer_fwd(GView G, const bf16* __restri
         }
         if (a_save) {
             for (int t = 0; t < 16; ++t) {
-                const long long i = base + t;
+                const long long i = node(job, t);
                 if (i < G.U)
                     *reinterpret_cast<uint2*>(a_save + i * KIN + 4 * lane) =
                         *reinterpret_cast<const uint2*>(A + t * LDA + 4 * lane);
@@ -826,12 +855,31 @@ static void ensure_workspace(MpnnState& S, long long U, bool training) {
     S.cap = cap;
 }
 
-// Launch shapes of the message-passing layer: gathers in flight x blocks per SM (4 warps each).
-constexpr int LAYER_NB[3] = {2, 4, 8};
-constexpr int LAYER_BPS[4] = {2, 3, 4, 6};
+// Launch shapes of the message-passing layer (k_layer_fwd): gathers in flight (4 NB rows per
+// warp), warps per block, node order, blocks per SM.
+struct LayerShape {
+    int nb, warps;
+    bool local;
+    int bps;
+};
+constexpr LayerShape LAYER_SHAPES[] = {{4, 4, false, 4},  {8, 4, false, 4},  {4, 4, false, 6},  {8, 4, false, 6},
+                                       {4, 8, true, 3},   {8, 8, true, 3},   {4, 12, true, 2},  {8, 12, true, 2},
+                                       {4, 24, true, 1},  {8, 24, true, 1}};
+
+template <int NB, int WARPS, bool LOCAL>
+static void launch_layer_kernel(unsigned grid, cudaStream_t s, const GView& G, const bf16* hin, bf16* hout,
+                                const bf16* W, const float* b, bf16* as, float* zs) {
+    const size_t smem = (size_t)(H * LDA + WARPS * 16 * LDA) * sizeof(bf16) + H * sizeof(float);
+    auto k = k_layer_fwd<NB, WARPS, LOCAL>;
+    LSMPS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, WARPS * 32, smem, s>>>(G, hin, hout, W, b, as, zs);
+}
 
 static void launch_layer(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool training, int c, int l) {
-    const unsigned lgrid = std::min<unsigned>((unsigned)((G.U + 63) / 64), 148u * LAYER_BPS[c % 4]);
+    const LayerShape& sh = LAYER_SHAPES[c];
+    const long long span = 16LL * sh.warps;  // nodes per block and round
+    const unsigned lgrid =
+        (unsigned)std::max<long long>(1, std::min<long long>((G.U + span - 1) / span, 148LL * sh.bps));
     const float* w = S.dw.get<float>();
     const bf16* wbf = S.wbf.get<bf16>();
     const bf16* hin = S.h[l].get<bf16>();
@@ -841,12 +889,22 @@ static void launch_layer(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool trai
     bf16* as = training ? S.a[l].get<bf16>() : nullptr;
     float* zs = training ? S.z[l + 1].get<float>() : nullptr;
     cudaStream_t s = ctx->stream;
-    switch (LAYER_NB[c / 4]) {
-        case 2: k_layer_fwd<2><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
-        case 4: k_layer_fwd<4><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
-        default: k_layer_fwd<8><<<lgrid, 128, 0, s>>>(G, hin, hout, W, b, as, zs); break;
+#define LSMPS_LAYER_CASE(NB_, W_, L_)                                                     \
+    if (sh.nb == NB_ && sh.warps == W_ && sh.local == L_) {                               \
+        launch_layer_kernel<NB_, W_, L_>(lgrid, s, G, hin, hout, W, b, as, zs);           \
+        LSMPS_CHECK_LAUNCH();                                                             \
+        return;                                                                           \
     }
-    LSMPS_CHECK_LAUNCH();
+    LSMPS_LAYER_CASE(4, 4, false)
+    LSMPS_LAYER_CASE(8, 4, false)
+    LSMPS_LAYER_CASE(4, 8, true)
+    LSMPS_LAYER_CASE(8, 8, true)
+    LSMPS_LAYER_CASE(4, 12, true)
+    LSMPS_LAYER_CASE(8, 12, true)
+    LSMPS_LAYER_CASE(4, 24, true)
+    LSMPS_LAYER_CASE(8, 24, true)
+#undef LSMPS_LAYER_CASE
+    LSMPS_REQUIRE(false, LSMPS_ERR_STATE, "unknown network layer launch shape");
 }
 
 // The autotuned launch shape of the layer for this graph size (layer 0 is the timed launch:
@@ -854,8 +912,9 @@ static void launch_layer(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool trai
 static int layer_shape(lsmps_ctx* ctx, MpnnState& S, const GView& G, bool training) {
     static const std::vector<std::string> names = [] {
         std::vector<std::string> v;
-        for (int nb : LAYER_NB)
-            for (int bps : LAYER_BPS) v.push_back("gathers" + std::to_string(nb) + "/blocks" + std::to_string(bps) + "xSM");
+        for (const LayerShape& sh : LAYER_SHAPES)
+            v.push_back("gathers" + std::to_string(4 * sh.nb) + "/warps" + std::to_string(sh.warps) +
+                        (sh.local ? "-local" : "") + "/blocks" + std::to_string(sh.bps) + "xSM");
         return v;
     }();
     return autotune(ctx, "mpnn_layer_fwd", G.U, names, 2, [&](int c) { launch_layer(ctx, S, G, training, c, 0); });
