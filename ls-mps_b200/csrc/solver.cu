@@ -465,23 +465,29 @@ __device__ __forceinline__ double warp_agg_sums(const MgFine& G, long long Ia, l
     if (lane < AGG_W) sh[lane] = 0.0;
     __syncwarp();
     const int rb = G.ustart[Ia], re = G.ustart[Ib];
-    for (int base = rb; base < re; base += 32) {
-        const int i = base + lane;
-        double x = 0.0;
-        int a = AGG_W + lane;  // past the last row: a key of its own, never part of a segment
-        if (i < re) {
-            x = f(i);
-            a = G.agg0[i] - (int)Ia;
-        }
+    // segment sums of one step: inclusive scan within runs of equal a, the run's last lane adds
+    auto deliver = [&](double x, int a, bool live) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {  // inclusive scan within runs of equal a
+        for (int o = 1; o < 32; o <<= 1) {
             const double y = __shfl_up_sync(0xffffffffu, x, o);
             const int ay = __shfl_up_sync(0xffffffffu, a, o);
             if (lane >= o && ay == a) x += y;
         }
         const int an = __shfl_down_sync(0xffffffffu, a, 1);
-        if (i < re && (lane == 31 || an != a)) sh[a] += x;
+        if (live && (lane == 31 || an != a)) sh[a] += x;
         __syncwarp();
+    };
+    // two steps per pass: both steps' loads are in flight before either scan
+    for (int base = rb; base < re; base += 64) {
+        const int i0 = base + lane, i1 = base + 32 + lane;
+        const bool l0 = i0 < re, l1 = i1 < re;
+        int a0 = AGG_W + lane, a1 = AGG_W + lane;  // past the last row: a key of its own, in no run
+        if (l0) a0 = G.agg0[i0] - (int)Ia;
+        if (l1) a1 = G.agg0[i1] - (int)Ia;
+        const double x0 = l0 ? f(i0) : 0.0;
+        const double x1 = l1 ? f(i1) : 0.0;
+        deliver(x0, a0, l0);
+        deliver(x1, a1, l1);
     }
     const double sum = lane < AGG_W ? sh[lane] : 0.0;
     __syncwarp();  // before the next task clears the slots
