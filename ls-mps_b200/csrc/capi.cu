@@ -177,6 +177,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
     lsmps_gpu::DevBuf* bufs[] = {&ctx->dflags, &ctx->scratch, &ctx->scan_tmp, &ctx->host_dummy, &ctx->pos,
                                  &ctx->type_in, &ctx->cell_of, &ctx->slot, &ctx->cell_count, &ctx->cell_start,
                                  &ctx->perm, &ctx->iperm, &ctx->sx, &ctx->sy, &ctx->sz, &ctx->stype,
@@ -205,6 +206,9 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (ctx->stage_done) cudaEventDestroy(ctx->stage_done);
     if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
+    if (ctx->side_join) cudaEventDestroy(ctx->side_join);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -49,6 +49,10 @@ struct lsmps_ctx {
     // copy-done and buffer-free events, created at first use
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t stage_done = nullptr, stage_free = nullptr;
+    // the learned solver with the multigrid builds the hierarchy on side_stream (highest priority)
+    // while the network runs on `stream`; fork / join events, all created at first use
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
     size_t stage_n = 0;
     bool have_stage = false;
     double timings[8] = {};

@@ -1640,6 +1640,38 @@ static void solve_mixed_f32(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_pp
     ps->solve_ms = ev_elapsed(ctx, 10, 11);
 }
 
+// The multigrid hierarchy set-up on the context's side stream (created at first use with the
+// device's highest priority), ordered after everything the context stream held when `fork`
+// was recorded; the context stream then waits for it. The set-up reads each level's size back
+// to the host, so work queued on the context stream meanwhile (the network's inference) fills
+// the GPU during those round trips, and the set-up's kernels take the SMs first when both wait.
+static void mg_setup_on_side(lsmps_ctx* ctx) {
+    cudaStream_t main = ctx->stream;
+    LSMPS_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->side_fork, 0));
+    ctx->stream = ctx->side_stream;
+    try {
+        mg_setup(ctx);
+    } catch (...) {
+        ctx->stream = main;
+        cudaStreamSynchronize(ctx->side_stream);
+        throw;
+    }
+    ctx->stream = main;
+    LSMPS_CUDA(cudaEventRecord(ctx->side_join, ctx->side_stream));
+    LSMPS_CUDA(cudaStreamWaitEvent(main, ctx->side_join, 0));
+}
+
+static void side_stream_fork(lsmps_ctx* ctx) {
+    if (!ctx->side_stream) {
+        int least = 0, greatest = 0;
+        LSMPS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        LSMPS_CUDA(cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, greatest));
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->side_fork, cudaEventDisableTiming));
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->side_join, cudaEventDisableTiming));
+    }
+    LSMPS_CUDA(cudaEventRecord(ctx->side_fork, ctx->stream));
+}
+
 // Mixed precision (MIXED, and LEARNED): Jacobi-BiCGStab with FP64 vectors and recurrences
 // whose two SpMVs per iteration read the FP32 copy of A D^-1 (8 bytes per entry instead
 // of 12: the matrix is the bandwidth). The FP32 matrix perturbs each product at ~6e-8
@@ -1669,8 +1701,30 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     const int stall = o->stall_window > 0 ? o->stall_window : 20;
     ev_record(ctx, 10);
     const bool mg = o->precond == LSMPS_PRECOND_MULTIGRID;
+    // y0 = |b| net(b / |b|): launches only (no host round trip)
+    auto net_guess = [&] {
+        float* rhs = ctx->fph.ensure<float>(U + 1);
+        float* yf = ctx->fx.ensure<float>(U + 1);
+        double* scal = engine_scalars(ctx);
+        k_norm2<<<RGRID, RB, 0, s>>>(U, b, scal, E.P, &E.S->counter[5]);
+        k_rhs_unit<<<1184, 256, 0, s>>>(U, b, rhs, scal);  // network input: b / |b| in FP32
+        LSMPS_CHECK_LAUNCH();
+        mpnn_warm_start(ctx, rhs, yf);
+        k_y_from_net<<<1184, 256, 0, s>>>(U, yf, scal, V.x);
+        LSMPS_CHECK_LAUNCH();
+    };
+    // LEARNED with the multigrid from a cold start: the network's guess (context stream) and
+    // the hierarchy set-up (side stream) run at the same time; they read the assembled system
+    // and write disjoint buffers
+    const bool overlap = mg && use_nn && !warm;
     if (mg) {
-        mg_setup(ctx);
+        if (overlap) {
+            side_stream_fork(ctx);
+            net_guess();
+            mg_setup_on_side(ctx);
+        } else {
+            mg_setup(ctx);
+        }
         V.ph = ctx->vph.ensure<double>(U + 1);
         V.sh = ctx->vsh.ensure<double>(U + 1);
     }
@@ -1698,15 +1752,7 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
             warm_rn = std::sqrt(r2);
         }
     } else if (use_nn) {
-        float* rhs = ctx->fph.ensure<float>(U + 1);
-        float* yf = ctx->fx.ensure<float>(U + 1);
-        double* scal = engine_scalars(ctx);
-        k_norm2<<<RGRID, RB, 0, s>>>(U, b, scal, E.P, &E.S->counter[5]);
-        k_rhs_unit<<<1184, 256, 0, s>>>(U, b, rhs, scal);  // network input: b / |b| in FP32
-        LSMPS_CHECK_LAUNCH();
-        mpnn_warm_start(ctx, rhs, yf);
-        k_y_from_net<<<1184, 256, 0, s>>>(U, yf, scal, V.x);  // y0 = |b| net(b / |b|)
-        LSMPS_CHECK_LAUNCH();
+        if (!overlap) net_guess();
         have_start = true;
     } else {
         LSMPS_CUDA(cudaMemsetAsync(V.x, 0, U * sizeof(double), s));
