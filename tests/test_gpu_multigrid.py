@@ -110,6 +110,23 @@ def test_learned_with_multigrid(ctx):
     assert st.converged and st.relative_l2_error <= 1e-8
 
 
+def test_learned_multigrid_setup_beside_network_is_deterministic(ctx):
+    """After each assembly the LEARNED solver with the multigrid builds the hierarchy on a second
+    stream while the network runs; the two read the same system and write disjoint buffers, so
+    every fresh assembly + solve gives the same bits, in every launch form."""
+    _setup(ctx, "mixed", 80_000, 13)
+    ctx.mpnn_load(lib.DEFAULT_WEIGHTS)
+    out = []
+    for g in (0, 1, 2, 0):
+        ctx.ppe_assemble("wls", 10**9, RE, L0, diag_shift=0.0)  # a new hierarchy per solve
+        st = ctx.ppe_solve("learned", 20000, 3e-11, use_graph=g, precond="multigrid")
+        assert st.converged and st.relative_l2_error <= 1e-8
+        out.append((st.iterations, ctx.pressure(st.unknowns)))
+    for it, p in out[1:]:
+        assert it == out[0][0]
+        assert np.array_equal(p, out[0][1])
+
+
 def test_warm_start_with_multigrid(ctx):
     _setup(ctx, "mixed", 60_000, 12)
     cold = ctx.ppe_solve("mixed", 20000, 3e-11, precond="multigrid")
