@@ -1,7 +1,11 @@
 /* LS-MPS per-step path on an sm_100a GPU — C ABI.
  *
  * Plain C types only (pointers, sizes, PODs); no C++ exceptions cross it. One context
- * owns the device buffers and one CUDA stream; calls on one context are not
+ * owns the device buffers and one CUDA stream (lsmps_stream), on which its work is ordered;
+ * two helper streams of its own carry the prefetched uploads (ordered before the context
+ * stream by lsmps_use_prefetched_particles) and, in a LEARNED solve with the multigrid from a
+ * cold start, the hierarchy set-up beside the network (joined back to the context stream
+ * within the solve). Calls on one context are not
  * thread-safe, separate contexts are independent. Every function returns an
  * lsmps_status; lsmps_last_error() gives the message of the last failure.
  *
@@ -251,7 +255,10 @@ enum {
  * which have no cells. Opt-in: cell aggregates ignore connection strength, so systems with
  * weakly coupled particles or strong row contrasts can need more iterations than JACOBI. A
  * multigrid run that stalls (stall_window) or breaks down continues as Jacobi MIXED from its
- * iterate (from zero if that is no longer finite) and reports fallback = 1. */
+ * iterate (from zero if that is no longer finite) and reports fallback = 1. With LEARNED and
+ * no warm start the hierarchy is built on the context's side stream while the network runs
+ * on the context stream (the set-up reads level sizes back to the host; the network fills the
+ * GPU meanwhile); the result is the same bits. */
 enum {
     LSMPS_PRECOND_JACOBI = 0,
     LSMPS_PRECOND_MULTIGRID = 1
