@@ -236,7 +236,10 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
     }
 }
 
-// Moves each row's slot range into the CSR (PPE_G lanes per row, coalesced).
+// Moves each row's slot range into the CSR (PPE_G lanes per row, coalesced). The row's CSR
+// offsets are loaded before its slot base (which needs the sorted index first), and each lane
+// issues up to four entries' loads before their stores, so a row of up to 4 PPE_G entries
+// costs one round trip for the copy instead of one per PPE_G entries.
 __global__ void __launch_bounds__(256) k_ppe_pack(long long U, const int* __restrict__ sorted_of_u,
                                                   const int* __restrict__ nrow, const int* __restrict__ arow,
                                                   const int* __restrict__ scol, const double* __restrict__ sval,
@@ -245,12 +248,28 @@ __global__ void __launch_bounds__(256) k_ppe_pack(long long U, const int* __rest
     const long long u = g / PPE_G;
     const int sub = (int)(g % PPE_G);
     if (u >= U) return;
+    const int o = arow[u], c = arow[u + 1] - o;
     const int k = sorted_of_u[u];
     const long long sb = (long long)nrow[k] + k;
-    const int o = arow[u], c = arow[u + 1] - o;
-    for (int p = sub; p < c; p += PPE_G) {
-        acol[o + p] = __ldcs(scol + sb + p);
-        aval[o + p] = __ldcs(sval + sb + p);
+    for (int p0 = sub; p0 < c; p0 += 4 * PPE_G) {
+        int cc[4];
+        double vv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int p = p0 + j * PPE_G;
+            if (p < c) {
+                cc[j] = __ldcs(scol + sb + p);
+                vv[j] = __ldcs(sval + sb + p);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int p = p0 + j * PPE_G;
+            if (p < c) {
+                acol[o + p] = cc[j];
+                aval[o + p] = vv[j];
+            }
+        }
     }
 }
 
