@@ -158,14 +158,19 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
     const int chunks = __reduce_max_sync(0xffffffffu, (e1 - e0 + PPE_G - 1) / PPE_G);
     double diag = 0.0, bsum = 0.0;
     int written = 0;
+    // the neighbor index of the next chunk is loaded one chunk ahead, so each chunk waits for
+    // one round trip (its gathers) instead of two
+    int mnext = e0 + sub < e1 ? col[e0 + sub] : 0;
     for (int c = 0; c < chunks; ++c) {
         const int e = e0 + c * PPE_G + sub;
+        const int m_cur = mnext;
+        mnext = e + PPE_G < e1 ? col[e + PPE_G] : 0;
         bool contrib = false, keep = false;
         double a = 0.0, xem = 0.0;
         int cj = -1;
         if (e < e1) {
-            // every load of the pair at once (one dependent round trip after col)
-            const int m = col[e];
+            // every load of the pair at once
+            const int m = m_cur;
             cj = uidx[m];
             const double xm = sx[m], ym = sy[m], zm = sz[m];
             const double xpm = xep[m];
