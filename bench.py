@@ -10,8 +10,8 @@ Workload (one "step" = the whole per-step path on one particle set):
   2e-11 (PPE relative L2 against p* <= 1e-8 for every compared solver, checked). Steps
   cycle through --sets seeded particle sets held on the device (a device-to-device copy
   into the library per step): BiCGStab's stopping iteration on one system moves by +-15 %
-  with summation order, so the step time is a mean over systems. Synthetic data, seeded; matrices are larger than L2
-  (126 MB) so no flush is needed.
+  with summation order, so the step time is a mean over systems. Synthetic data, seeded;
+  matrices are larger than L2 (126 MB) so no flush is needed.
 
 `value` = particles x GPUs / (device step time, CUDA events on the library's stream, max
 over ranks) with the metric's solver (--solver, default `learned_multigrid`: the learned +
@@ -19,8 +19,9 @@ mixed-precision solver, i.e. mixed-precision BiCGStab started from the message-p
 network's guess, with the cell-aggregation multigrid V-cycle as its preconditioner; the same
 without the network is `multigrid` in ppe_compare). `e2e` = the same
 through the C ABI with host buffers: the upload from pinned memory (double-buffered: step
-i + 1's copies overlap step i), the step, and the download of the pressure inside the timed
-region. The plain FP64 GPU BiCGStab (the reference iteration),
+i + 1's copies overlap step i), the step, and the download of the pressure into pinned memory
+(asynchronous: step i's result travels while step i + 1 runs; the last download is waited
+for), all inside the timed region. The plain FP64 GPU BiCGStab (the reference iteration),
 Jacobi FP64, MIXED, LEARNED and both with the multigrid preconditioner are timed on the same
 systems beside it (means and per set).
 `--impl reference` times the reference's own CPU implementation of the path.
@@ -295,7 +296,9 @@ def run_mine(args, dist):
         pt[:] = t
         pins.append((px, pt))
     U = max(int(pst.unknowns), 1)
-    pin_p = torch.empty(4 * U, dtype=torch.float64, pin_memory=True).numpy()
+    # two page-locked result buffers, alternated: step i's pressure travels to the host while
+    # step i + 1 runs (lsmps_download_pressure_async); the last one is waited for in the region
+    pin_ps = [torch.empty(4 * U, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
     d2h = []
     ctx.prefetch(*pins[1 % K])  # untimed: allocates the staging buffers once
     ctx.use_prefetched()
@@ -309,8 +312,9 @@ def run_mine(args, dist):
             ctx.prefetch(*pins[(i + 1) % K])
         _, pst_e, _, _ = step(ctx, args.solver, args.tol, args.max_iter, [])
         u = int(pst_e.unknowns)
-        ctx.pressure_into(pin_p[:u])
+        ctx.pressure_into_async(pin_ps[i % 2][:u])
         d2h.append(8 * u)
+    ctx.download_wait()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     e2e_ms_max = dist.reduce(e2e_ms, "max")
 

@@ -307,6 +307,15 @@ int lsmps_download_ppe(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, 
                        double* x_exact, int32_t* unknown_particle);
 /* Solution of the last solve (U, reference numbering). */
 int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+/* The same download without waiting for it: the values are reordered on the context stream
+ * and copied to `p` on the context's copy stream, so a time loop can start its next step while
+ * the result travels. `p` must be page-locked host memory to overlap, and must stay valid and
+ * unread until lsmps_download_wait returns (or the next asynchronous download, which orders
+ * itself after the previous copy, has been waited for). lsmps_download_wait blocks until the
+ * last asynchronous download has landed (at once when none is pending). No reference
+ * counterpart (the reference's solution lives in host memory, src/lsmps.cpp:67). */
+int lsmps_download_pressure_async(lsmps_ctx* ctx, double* p, size_t u);
+int lsmps_download_wait(lsmps_ctx* ctx);
 
 /* Per-particle pressure (n values, caller order) for step series whose unknowns change from
  * step to step. set_initial_pressure: the next lsmps_ppe_solve with warm_start = 1 starts from

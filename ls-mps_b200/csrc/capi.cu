@@ -196,7 +196,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
                                  &ctx->red, &ctx->S_ptr, &ctx->S_len,
                                  &ctx->S_col, &ctx->S_val, &ctx->S_vals, &ctx->S_valf, &ctx->nbr_slots,
                                  &ctx->A_slot_col, &ctx->A_slot_val, &ctx->A_xep, &ctx->stage_pos,
-                                 &ctx->stage_type};
+                                 &ctx->stage_type, &ctx->dl_stage};
     for (auto* b : bufs) b->release();
     mpnn_destroy(ctx);
     mg_destroy(ctx);
@@ -206,6 +206,8 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (ctx->stage_done) cudaEventDestroy(ctx->stage_done);
     if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->dl_ready) cudaEventDestroy(ctx->dl_ready);
+    if (ctx->dl_done) cudaEventDestroy(ctx->dl_done);
     if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
     if (ctx->side_join) cudaEventDestroy(ctx->side_join);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
@@ -404,6 +406,17 @@ int lsmps_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
         ev_record(ctx, 13);
         ctx->timings[6] = ev_elapsed(ctx, 12, 13);
     });
+}
+
+int lsmps_download_pressure_async(lsmps_ctx* ctx, double* p, size_t u) {
+    return guarded(ctx, [&] {
+        LSMPS_REQUIRE(p || u == 0, LSMPS_ERR_ARG, "null pressure buffer");
+        ppe_download_pressure_async(ctx, p, u);
+    });
+}
+
+int lsmps_download_wait(lsmps_ctx* ctx) {
+    return guarded(ctx, [&] { ppe_download_wait(ctx); });
 }
 
 int lsmps_set_initial_pressure(lsmps_ctx* ctx, const double* p, size_t n) {

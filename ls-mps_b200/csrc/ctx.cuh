@@ -53,6 +53,11 @@ struct lsmps_ctx {
     // while the network runs on `stream`; fork / join events, all created at first use
     cudaStream_t side_stream = nullptr;
     cudaEvent_t side_fork = nullptr, side_join = nullptr;
+    // asynchronous result download (lsmps_download_pressure_async): staging buffer on the
+    // device, reordered-result-ready and copy-done events, a copy in flight
+    lsmps_gpu::DevBuf dl_stage;
+    cudaEvent_t dl_ready = nullptr, dl_done = nullptr;
+    bool dl_pending = false;
     size_t stage_n = 0;
     bool have_stage = false;
     double timings[8] = {};

@@ -49,6 +49,8 @@ void ppe_download(lsmps_ctx* ctx, int32_t* row, int32_t* col, double* val, doubl
 // solver.cu
 void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_stats* out);
 void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u);
+void ppe_download_pressure_async(lsmps_ctx* ctx, double* p, size_t u);
+void ppe_download_wait(lsmps_ctx* ctx);
 void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool device);
 void ppe_pressure_particles(lsmps_ctx* ctx, double* pp, size_t n, double fill, bool device);
 

@@ -2085,4 +2085,42 @@ void ppe_download_pressure(lsmps_ctx* ctx, double* p, size_t u) {
     LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+// The same values without waiting: reordered into a staging buffer on the context stream,
+// then copied to the host on the context's copy stream, so the next step's kernels run while
+// the copy is in flight. The staging buffer is reused by the next call, which therefore first
+// orders the context stream after the previous copy.
+void ppe_download_pressure_async(lsmps_ctx* ctx, double* p, size_t u) {
+    LSMPS_REQUIRE(ctx->have_solution, LSMPS_ERR_STATE, "no PPE solution");
+    LSMPS_REQUIRE((long long)u == ctx->U, LSMPS_ERR_ARG, "pressure buffer size differs from the unknown count");
+    if (!u) return;
+    if (!ctx->copy_stream) LSMPS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (!ctx->dl_ready) {
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->dl_ready, cudaEventDisableTiming));
+        LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->dl_done, cudaEventDisableTiming));
+    }
+    if (ctx->dl_pending) {
+        if (ctx->dl_stage.bytes < (u + 1) * sizeof(double)) {  // growing frees the copy's source
+            LSMPS_CUDA(cudaEventSynchronize(ctx->dl_done));
+            ctx->dl_pending = false;
+        } else {
+            LSMPS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->dl_done, 0));
+        }
+    }
+    double* st = ctx->dl_stage.ensure<double>(u + 1);
+    k_to_ref<<<blocks_for(u, 256), 256, 0, ctx->stream>>>(ctx->vx.get<double>(), ctx->u_of_ref.get<int>(),
+                                                          (long long)u, st);
+    LSMPS_CHECK_LAUNCH();
+    LSMPS_CUDA(cudaEventRecord(ctx->dl_ready, ctx->stream));
+    LSMPS_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->dl_ready, 0));
+    LSMPS_CUDA(cudaMemcpyAsync(p, st, u * sizeof(double), cudaMemcpyDeviceToHost, ctx->copy_stream));
+    LSMPS_CUDA(cudaEventRecord(ctx->dl_done, ctx->copy_stream));
+    ctx->dl_pending = true;
+}
+
+void ppe_download_wait(lsmps_ctx* ctx) {
+    if (!ctx->dl_pending) return;
+    LSMPS_CUDA(cudaEventSynchronize(ctx->dl_done));
+    ctx->dl_pending = false;
+}
+
 }  // namespace lsmps_gpu

@@ -184,6 +184,8 @@ SIGNATURES = {
     "lsmps_download_wls": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "lsmps_download_ppe": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "lsmps_download_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_download_pressure_async": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "lsmps_download_wait": (C.c_int, [_vp]),
     "lsmps_ppe_manufacture": (C.c_int, [_vp, _vp, C.c_int]),
     "lsmps_ppe_residual_static": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int, _vp]),
     "lsmps_set_initial_pressure": (C.c_int, [_vp, _vp, C.c_size_t]),
@@ -527,6 +529,17 @@ class Context:
         assert out.dtype == np.float64 and out.flags.c_contiguous
         self._check(self.L.lsmps_download_pressure(self.h, _p(out), len(out)))
         return out
+
+    def pressure_into_async(self, out):
+        """lsmps_download_pressure_async: start the download into `out` (page-locked host memory
+        to overlap; keep it alive and unread until download_wait)."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        self._check(self.L.lsmps_download_pressure_async(self.h, _p(out), len(out)))
+        return out
+
+    def download_wait(self):
+        """lsmps_download_wait: block until the last asynchronous download has landed."""
+        self._check(self.L.lsmps_download_wait(self.h))
 
     def ppe_reference_numbering(self):
         """The assembled system in the reference's numbering (row, col, val, b, p*, particle)."""

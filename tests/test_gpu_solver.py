@@ -114,6 +114,39 @@ def test_warm_start(ctx, lattice_system):
     assert c.converged and c.iterations <= 2
 
 
+def test_async_download_matches_blocking(ctx, lattice_system):
+    """lsmps_download_pressure_async lands the same values as the blocking download, also with
+    the next step's work queued before the wait, with two downloads in flight into alternating
+    page-locked buffers, and after the unknown count changes."""
+    import torch
+
+    xyz, t = lattice_system
+    ctx.upload(xyz, t)
+    ctx.build_neighbors(2.1, 128, 1.0)
+    st = ctx.ppe_assemble("shifted", 10**9, 2.1, 1.0)
+    u = int(st.unknowns)
+    bufs = [torch.empty(u + 1000, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    ctx.download_wait()  # nothing pending: returns at once
+    ctx.ppe_solve("mixed", 5000, 1e-10)
+    want0 = ctx.pressure(u)
+    ctx.pressure_into_async(bufs[0][:u])
+    ctx.ppe_solve("jacobi", 5000, 1e-10)  # queued while the first download is in flight
+    want1 = ctx.pressure(u)
+    ctx.pressure_into_async(bufs[1][:u])
+    ctx.download_wait()
+    assert np.array_equal(bufs[0][:u], want0)
+    assert np.array_equal(bufs[1][:u], want1)
+    # fewer unknowns (the PPE capped at half the particles), then the same count again
+    st2 = ctx.ppe_assemble("shifted", u // 2, 2.1, 1.0)
+    u2 = int(st2.unknowns)
+    ctx.ppe_solve("mixed", 5000, 1e-10)
+    ctx.pressure_into_async(bufs[0][:u2])
+    ctx.download_wait()
+    assert np.array_equal(bufs[0][:u2], ctx.pressure(u2))
+    with pytest.raises(lib.LsmpsError):
+        ctx.pressure_into_async(bufs[1][: u2 + 1])  # wrong size: rejected before any copy
+
+
 @pytest.fixture(scope="module")
 def plate_system(built):
     c = lib.Context(0)
