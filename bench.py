@@ -217,7 +217,7 @@ def step(ctx, solver, tol, max_iter, timings):
 
     re = RE_RATIO * L0
     nst = ctx.build_neighbors(re, MAXN, L0)
-    ctx.wls(re, L0, mode=1)
+    ctx.wls(re, L0, mode=1, stats=False)  # no statistics read-back: the host does not wait here
     pst = ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
     sv, pc, ug = SOLVER_SPECS[solver]
     s = ctx.ppe_solve(sv, max_iter, tol, precond=pc, use_graph=ug)

@@ -52,7 +52,8 @@ const char* lsmps_last_error(const lsmps_ctx* ctx);
 int lsmps_abi_version(void);
 /* Device time (ms, CUDA events on the context stream) of the phases of the last calls:
  * [0] upload, [1] neighbor build (+classification when fused), [2] classification,
- * [3] WLS, [4] PPE assembly, [5] PPE solve, [6] last download. */
+ * [3] WLS, [4] PPE assembly, [5] PPE solve, [6] last download. A WLS call without
+ * statistics did not wait for its events; this call reads them (and waits for them). */
 int lsmps_get_timings(lsmps_ctx* ctx, double out[8]);
 /* Block until all work queued on the context stream has finished. */
 int lsmps_sync(lsmps_ctx* ctx);
@@ -188,7 +189,9 @@ typedef struct lsmps_wls_stats {
 } lsmps_wls_stats;
 
 /* wls_test (mode 0) or the all-particle batched WLS (mode 1). Mode 1 also keeps each
- * particle's Laplacian vector z = M^-1 (e3+e4+e5) and sum of weights for the WLS PPE. */
+ * particle's Laplacian vector z = M^-1 (e3+e4+e5) and sum of weights for the WLS PPE; with
+ * out == NULL it returns without reading its statistics back, so the host does not wait for
+ * the device (the next call is ordered after it on the context stream). */
 int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out);
 
 /* ---- PPE assembly ----------------------------------------------------------------- */

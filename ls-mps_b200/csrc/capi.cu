@@ -83,8 +83,9 @@ void particles_upload(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, si
 void particles_prefetch(lsmps_ctx* ctx, const double* xyz, const uint8_t* type, size_t n) {
     LSMPS_REQUIRE(n == 0 || (xyz && type), LSMPS_ERR_ARG, "null particle buffers");
     LSMPS_REQUIRE(n < (size_t)(1u << 31) - 1, LSMPS_ERR_OVERFLOW, "particle count beyond int32");
-    if (!ctx->copy_stream) {
+    if (!ctx->copy_stream)  // also created by an asynchronous download
         LSMPS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (!ctx->stage_done) {
         LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->stage_done, cudaEventDisableTiming));
         LSMPS_CUDA(cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming));
     }
@@ -219,6 +220,11 @@ const char* lsmps_last_error(const lsmps_ctx* ctx) { return ctx ? ctx->last_erro
 
 int lsmps_get_timings(lsmps_ctx* ctx, double out[8]) {
     if (!ctx || !out) return LSMPS_ERR_ARG;
+    if (ctx->wls_timing_pending) {  // a WLS call that did not wait: its events are read now
+        const int rc = guarded(ctx, [&] { ctx->timings[3] = ev_elapsed(ctx, 6, 7); });
+        if (rc != LSMPS_OK) return rc;
+        ctx->wls_timing_pending = false;
+    }
     std::memcpy(out, ctx->timings, sizeof(ctx->timings));
     return LSMPS_OK;
 }
@@ -347,7 +353,9 @@ int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out) 
         ev_record(ctx, 6);
         wls_run(ctx, opts, out);
         ev_record(ctx, 7);
-        ctx->timings[3] = ev_elapsed(ctx, 6, 7);
+        // without statistics the call does not wait; its time is read by lsmps_get_timings
+        ctx->wls_timing_pending = out == nullptr;
+        if (out) ctx->timings[3] = ev_elapsed(ctx, 6, 7);
     });
 }
 

@@ -61,6 +61,7 @@ struct lsmps_ctx {
     size_t stage_n = 0;
     bool have_stage = false;
     double timings[8] = {};
+    bool wls_timing_pending = false;  // timings[3] of a WLS call without statistics, not yet read
 
     lsmps_gpu::DevBuf dflags;      // int device error flags
     lsmps_gpu::DevBuf scratch;     // general reduction scratch

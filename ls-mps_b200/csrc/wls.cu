@@ -657,6 +657,11 @@ void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* o, lsmps_wls_stats* out) {
         else if (P.nrhs == 2) launch_all<2, 1>(ctx, P, gcnt, gsum);
         else launch_all<3, 1>(ctx, P, gcnt, gsum);
     }
+    ctx->have_wls = true;
+    ctx->wls_nrhs = o->nrhs;
+    ctx->wls_stored = P.store != 0;
+    ctx->have_ppe = ctx->have_solution = false;
+    if (!out) return;  // no statistics wanted: no read-back, the host does not wait
     unsigned long long hc[8];
     double hs[4];
     LSMPS_CUDA(cudaMemcpyAsync(hc, gcnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
@@ -674,11 +679,7 @@ void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* o, lsmps_wls_stats* out) {
     st.rms_laplacian_error = nsol > 0 ? std::sqrt(hs[1] / nsol) : 0;
     st.max_gradient_error = hs[2];
     st.max_laplacian_error = hs[3];
-    ctx->have_wls = true;
-    ctx->wls_nrhs = o->nrhs;
-    ctx->wls_stored = P.store != 0;
-    ctx->have_ppe = ctx->have_solution = false;
-    if (out) *out = st;
+    *out = st;
 }
 
 namespace {

@@ -384,13 +384,18 @@ class Context:
         self._check(self.L.lsmps_max_displacement(self.h, C.byref(d)))
         return d.value
 
-    def wls(self, re, l0, mode=1, wls_samples=4096, coef=None, precision=0, store=False, reg=1e-8):
+    def wls(self, re, l0, mode=1, wls_samples=4096, coef=None, precision=0, store=False, reg=1e-8,
+            stats=True):
+        """lsmps_wls; stats=False (mode 1) skips the statistics read-back and returns None."""
         coef = REF_QUADRATIC[None, :] if coef is None else np.atleast_2d(coef)
         self._coef = np.ascontiguousarray(coef, dtype=np.float64)
         o = WlsOpts(re=re, l0=l0, regularization=reg, mode=mode, wls_samples=wls_samples,
                     nrhs=self._coef.shape[0], precision=precision,
                     quad_coef=self._coef.ctypes.data_as(C.POINTER(C.c_double)),
                     store_solutions=1 if store else 0)
+        if not stats and mode == 1:
+            self._check(self.L.lsmps_wls(self.h, C.byref(o), None))
+            return None
         st = WlsStats()
         self._check(self.L.lsmps_wls(self.h, C.byref(o), C.byref(st)))
         return st

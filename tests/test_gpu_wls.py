@@ -67,6 +67,22 @@ def test_all_particle_wls_matches_oracle(ctx, case):
     assert st.rms_gradient_error < 1e-8 and st.rms_laplacian_error < 1e-6
 
 
+def test_all_particle_wls_without_statistics(ctx):
+    """A mode-1 WLS call without statistics (out = NULL) returns without waiting, leaves the
+    same results, and its phase time is read by lsmps_get_timings."""
+    xyz, t, _ = lib.generate(None, case="rain_plate", particles=40_000, l0=1.0, seed=6)
+    _setup(ctx, xyz, t, 2.1, 1.0)
+    ctx.wls(2.1, 1.0, mode=1, store=True)
+    ref = ctx.wls_result(nrhs=1, with_x=True)
+    assert ctx.wls(2.1, 1.0, mode=1, store=True, stats=False) is None
+    assert ctx.timings()[3] > 0.0
+    got = ctx.wls_result(nrhs=1, with_x=True)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+    st = ctx.ppe_assemble("wls", 10**9, 2.1, 1.0, diag_shift=0.0)  # the WLS state is set
+    assert st.unknowns > 0
+
+
 def test_mixed_precision_wls_refines_to_fp64(ctx):
     xyz = jittered_lattice(24, 0.1, seed=2)
     t = np.zeros(len(xyz), np.uint8)
