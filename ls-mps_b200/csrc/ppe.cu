@@ -241,38 +241,70 @@ __global__ void __launch_bounds__(128) k_ppe_rows(PpeParams P, long long U, cons
     }
 }
 
-// Moves each row's slot range into the CSR (PPE_G lanes per row, coalesced). The row's CSR
-// offsets are loaded before its slot base (which needs the sorted index first), and each lane
-// issues up to four entries' loads before their stores, so a row of up to 4 PPE_G entries
-// costs one round trip for the copy instead of one per PPE_G entries.
-__global__ void __launch_bounds__(256) k_ppe_pack(long long U, const int* __restrict__ sorted_of_u,
-                                                  const int* __restrict__ nrow, const int* __restrict__ arow,
-                                                  const int* __restrict__ scol, const double* __restrict__ sval,
-                                                  int* __restrict__ acol, double* __restrict__ aval) {
-    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long u = g / PPE_G;
-    const int sub = (int)(g % PPE_G);
-    if (u >= U) return;
-    const int o = arow[u], c = arow[u + 1] - o;
-    const int k = sorted_of_u[u];
-    const long long sb = (long long)nrow[k] + k;
-    for (int p0 = sub; p0 < c; p0 += 4 * PPE_G) {
-        int cc[4];
-        double vv[4];
+// Moves each row's slot range into the CSR. A block takes PACK_ROWS consecutive rows, whose
+// entries are one contiguous range of the CSR: each warp loads the first 32 entries of four
+// rows at once (the rest of a longer row after them) into shared memory at their CSR offsets,
+// then the block writes the range with consecutive stores. A block whose range exceeds
+// PACK_CAP entries copies its rows directly.
+constexpr int PACK_ROWS = 32, PACK_CAP = 2048, PACK_THREADS = 256;
+__global__ void __launch_bounds__(PACK_THREADS) k_ppe_pack(long long U, const int* __restrict__ sorted_of_u,
+                                                           const int* __restrict__ nrow, const int* __restrict__ arow,
+                                                           const int* __restrict__ scol,
+                                                           const double* __restrict__ sval, int* __restrict__ acol,
+                                                           double* __restrict__ aval) {
+    __shared__ double bval[PACK_CAP];
+    __shared__ int bcol[PACK_CAP];
+    __shared__ int roff[PACK_ROWS + 1];
+    __shared__ long long rsrc[PACK_ROWS];
+    const long long u0 = blockIdx.x * (long long)PACK_ROWS;
+    const int nr = (int)min((long long)PACK_ROWS, U - u0);
+    if (threadIdx.x <= nr) roff[threadIdx.x] = arow[u0 + threadIdx.x];
+    if (threadIdx.x < nr) {
+        const int k = sorted_of_u[u0 + threadIdx.x];
+        rsrc[threadIdx.x] = (long long)nrow[k] + k;
+    }
+    __syncthreads();
+    const int base = roff[0], total = roff[nr] - base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int RPW = PACK_ROWS / (PACK_THREADS / 32);  // rows per warp
+    if (total <= PACK_CAP) {
+        int cc[RPW];
+        double vv[RPW];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int p = p0 + j * PPE_G;
-            if (p < c) {
-                cc[j] = __ldcs(scol + sb + p);
-                vv[j] = __ldcs(sval + sb + p);
-            }
+        for (int j = 0; j < RPW; ++j) {
+            const int r = warp + j * (PACK_THREADS / 32);
+            const bool on = r < nr && lane < roff[r + 1] - roff[r];
+            cc[j] = on ? __ldcs(scol + rsrc[r] + lane) : 0;
+            vv[j] = on ? __ldcs(sval + rsrc[r] + lane) : 0.0;
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int p = p0 + j * PPE_G;
-            if (p < c) {
-                acol[o + p] = cc[j];
-                aval[o + p] = vv[j];
+        for (int j = 0; j < RPW; ++j) {
+            const int r = warp + j * (PACK_THREADS / 32);
+            if (r < nr && lane < roff[r + 1] - roff[r]) {
+                bcol[roff[r] - base + lane] = cc[j];
+                bval[roff[r] - base + lane] = vv[j];
+            }
+        }
+        for (int j = 0; j < RPW; ++j) {  // rows longer than 32 entries
+            const int r = warp + j * (PACK_THREADS / 32);
+            if (r >= nr) break;
+            const int o = roff[r] - base, c = roff[r + 1] - roff[r];
+            for (int p = 32 + lane; p < c; p += 32) {
+                bcol[o + p] = __ldcs(scol + rsrc[r] + p);
+                bval[o + p] = __ldcs(sval + rsrc[r] + p);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < total; i += PACK_THREADS) {
+            acol[base + i] = bcol[i];
+            aval[base + i] = bval[i];
+        }
+    } else {
+        for (int r = warp; r < nr; r += PACK_THREADS / 32) {
+            const int o = roff[r], c = roff[r + 1] - o;
+            for (int p = lane; p < c; p += 32) {
+                acol[o + p] = __ldcs(scol + rsrc[r] + p);
+                aval[o + p] = __ldcs(sval + rsrc[r] + p);
             }
         }
     }
@@ -386,8 +418,8 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     int* acol = ctx->A_col.ensure<int>(nnz + 1);
     double* aval = ctx->A_val.ensure<double>(nnz + 1);
     if (U) {
-        k_ppe_pack<<<blocks_for((size_t)U * PPE_G, 256), 256, 0, s>>>(U, sorted_of_u, ctx->nbr_row.get<int>(), arow,
-                                                                      scol, sval, acol, aval);
+        k_ppe_pack<<<blocks_for((size_t)U, PACK_ROWS), PACK_THREADS, 0, s>>>(U, sorted_of_u, ctx->nbr_row.get<int>(),
+                                                                             arow, scol, sval, acol, aval);
         LSMPS_CHECK_LAUNCH();
     }
     ev_record(ctx, 9);

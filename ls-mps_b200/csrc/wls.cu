@@ -204,24 +204,60 @@ struct WlsParams {
     double coef[30];  // nrhs x 10
 };
 
-__device__ __forceinline__ void basis_fast(double dx, double dy, double dz, double ir, double l0inv,
-                                           double* q) {
-    q[0] = dx * ir;
-    q[1] = dy * ir;
-    q[2] = dz * ir;
-    double s = ir * l0inv;
-    double hs = 0.5 * s;
-    q[3] = dx * dx * hs;
-    q[4] = dy * dy * hs;
-    q[5] = dz * dz * hs;
-    q[6] = dx * dy * s;
-    q[7] = dx * dz * s;
-    q[8] = dy * dz * s;
-}
-
 __device__ __forceinline__ double quad_fast(const double* c, double x, double y, double z) {
     return c[0] + c[1] * x + c[2] * y + c[3] * z + c[4] * x * x + c[5] * y * y + c[6] * z * z + c[7] * x * y +
            c[8] * x * z + c[9] * y * z;
+}
+
+// Every basis function of the reference (src/lsmps.cpp:23) is one power of 1/r times a monomial
+// of (dx, dy, dz) times a constant: q_a = c_a mono_a(d) / r with mono = x, y, z, xx, yy, zz,
+// xy, xz, yz and c = 1, 1, 1, 1/(2 l0) x 3, 1/l0 x 3. So M_ac = sum w q_a q_c = c_a c_c
+// sum (w / r^2) mono_a mono_c, and the 45 moments are 31 distinct sums T over the monomials of
+// degree 2 to 4 of W d, W = w / r^2 (degree 2 xx xy xz yy yz zz, then degree 3 and 4 in the
+// same order: descending x exponent, then descending y exponent). A neighbor costs 43 FP64
+// operations for the moments instead of 9 basis products, 9 weight products and 45 FMAs.
+constexpr int NMONO = 31;
+__host__ __device__ constexpr int basis_exp(int a, int axis) {  // exponent of axis in mono_a
+    return a < 3 ? (a == axis) : a < 6 ? 2 * (a - 3 == axis) : (a == 6 ? axis != 2 : a == 7 ? axis != 1 : axis != 0);
+}
+__host__ __device__ constexpr int mono_index(int ex, int ey, int ez) {  // position among T
+    const int d = ex + ey + ez;
+    int pos = d == 2 ? 0 : d == 3 ? 6 : 16;
+    for (int e = d; e > ex; --e) pos += d - e + 1;  // monomials with a larger x exponent
+    return pos + (d - ex - ey);
+}
+__host__ __device__ constexpr int moment_mono(int a, int c) {
+    return mono_index(basis_exp(a, 0) + basis_exp(c, 0), basis_exp(a, 1) + basis_exp(c, 1),
+                      basis_exp(a, 2) + basis_exp(c, 2));
+}
+static_assert(moment_mono(0, 0) == 0 && moment_mono(1, 2) == 4 && moment_mono(5, 5) == 30 &&
+                  moment_mono(3, 4) == 19 && moment_mono(6, 6) == 19 && moment_mono(8, 0) == 10 &&
+                  moment_mono(7, 2) == 11 && moment_mono(4, 8) == 27,
+              "monomial numbering");
+__device__ __forceinline__ double basis_const(int a, double l0inv) {
+    return a < 3 ? 1.0 : a < 6 ? 0.5 * l0inv : l0inv;
+}
+
+// Adds one neighbor's W d-monomials to T; p = (xx, xy, xz, yy, yz, zz) of d.
+__device__ __forceinline__ void add_monomials(double W, double dx, double dy, double dz, const double* p,
+                                              double* T) {
+    const double bxx = W * p[0], bxy = W * p[1], bxz = W * p[2], byy = W * p[3], byz = W * p[4], bzz = W * p[5];
+    T[0] += bxx, T[1] += bxy, T[2] += bxz, T[3] += byy, T[4] += byz, T[5] += bzz;
+    T[6] += bxx * dx, T[7] += bxx * dy, T[8] += bxx * dz, T[9] += byy * dx, T[10] += bxy * dz;
+    T[11] += bzz * dx, T[12] += byy * dy, T[13] += byy * dz, T[14] += bzz * dy, T[15] += bzz * dz;
+    T[16] += bxx * p[0], T[17] += bxx * p[1], T[18] += bxx * p[2], T[19] += bxx * p[3], T[20] += bxx * p[4];
+    T[21] += bxx * p[5], T[22] += byy * p[1], T[23] += byy * p[2], T[24] += bzz * p[1], T[25] += bzz * p[2];
+    T[26] += byy * p[3], T[27] += byy * p[4], T[28] += byy * p[5], T[29] += bzz * p[4], T[30] += bzz * p[5];
+}
+
+// The packed normalised moments from the monomial sums (M = 0 where sum w is 0).
+__device__ __forceinline__ void moments_from_sums(const double* T, double ws, double l0inv, double* M) {
+    const double inv = ws > 0 ? 1.0 / ws : 0.0;
+#pragma unroll
+    for (int a = 0; a < K; ++a)
+#pragma unroll
+        for (int c = 0; c <= a; ++c)
+            M[tri(a, c)] = basis_const(a, l0inv) * basis_const(c, l0inv) * inv * T[moment_mono(a, c)];
 }
 
 // Accumulates the normalised packed moment matrix of particle k; returns sum w.
@@ -231,39 +267,30 @@ __device__ __forceinline__ double accumulate_moments(int k, const double* __rest
                                                      const int* __restrict__ row,
                                                      const int* __restrict__ col, double re, double l0inv,
                                                      double* M) {
+    double T[NMONO];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) M[t] = 0;
-    double xi = sx[k], yi = sy[k], zi = sz[k];
+    for (int t = 0; t < NMONO; ++t) T[t] = 0;
+    const double xi = sx[k], yi = sy[k], zi = sz[k];
     double ws = 0;
     for (int e = row[k]; e < row[k + 1]; ++e) {
-        int m = col[e];
-        double dx = sx[m] - xi, dy = sy[m] - yi, dz = sz[m] - zi;
-        double r2 = dx * dx + dy * dy + dz * dz;
+        const int m = col[e];
+        const double dx = sx[m] - xi, dy = sy[m] - yi, dz = sz[m] - zi;
+        const double r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 > 1e-24) || r2 >= re * re) continue;  // r <= 1e-12 or r >= re: weight 0
-        double ir = rsqrt(r2);                           // 1 / r without a square root and a division
-        double qq = re * ir - 1.0;
-        double w = qq * qq;
-        double q[K];
-        basis_fast(dx, dy, dz, ir, l0inv, q);
+        const double ir = rsqrt(r2);                     // 1 / r without a square root and a division
+        const double qq = re * ir - 1.0;
+        const double w = qq * qq;
+        const double p[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
         ws += w;
-#pragma unroll
-        for (int a = 0; a < K; ++a) {
-            double wq = w * q[a];
-#pragma unroll
-            for (int c = 0; c <= a; ++c) M[tri(a, c)] += wq * q[c];
-        }
+        add_monomials(w * (ir * ir), dx, dy, dz, p, T);
     }
-    if (ws > 0) {
-        double inv = 1.0 / ws;
-#pragma unroll
-        for (int t = 0; t < NT; ++t) M[t] *= inv;
-    }
+    moments_from_sums(T, ws, l0inv, M);
     return ws;
 }
 
 // One pass over the neighbors for both the moments (as accumulate_moments) and the
-// right-hand sides B[f] = sum w q (f_m - f_k) / r (the same expressions as the separate
-// right-hand-side pass of k_wls_all, in the same neighbor order). Returns sum w.
+// right-hand sides B[f]_a = sum w q_a (f_m - f_k) / r = c_a sum W (f_m - f_k) mono_a, in the
+// neighbor order. Returns sum w.
 template <int NRHS>
 __device__ __forceinline__ double accumulate_moments_rhs(int k, const double* __restrict__ sx,
                                                          const double* __restrict__ sy,
@@ -272,8 +299,9 @@ __device__ __forceinline__ double accumulate_moments_rhs(int k, const double* __
                                                          const uint8_t* __restrict__ cls, const WlsParams& P,
                                                          double l0inv, const double* __restrict__ fvals,
                                                          const double* fi, double* M, double (*B)[K]) {
+    double T[NMONO];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) M[t] = 0;
+    for (int t = 0; t < NMONO; ++t) T[t] = 0;
 #pragma unroll
     for (int f = 0; f < NRHS; ++f)
 #pragma unroll
@@ -289,29 +317,25 @@ __device__ __forceinline__ double accumulate_moments_rhs(int k, const double* __
         const double ir = rsqrt(r2);                         // 1 / r without a square root and a division
         const double qq = P.re * ir - 1.0;
         const double w = qq * qq;
-        double q[K];
-        basis_fast(dx, dy, dz, ir, l0inv, q);
+        const double W = w * (ir * ir);
+        const double p[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
         ws += w;
-#pragma unroll
-        for (int a = 0; a < K; ++a) {
-            const double wq = w * q[a];
-#pragma unroll
-            for (int c = 0; c <= a; ++c) M[tri(a, c)] += wq * q[c];
-        }
+        add_monomials(W, dx, dy, dz, p, T);
         if (P.mirror_walls && cls[m] == LSMPS_WALL) continue;  // f_m = f_k: no right-hand-side term
 #pragma unroll
         for (int f = 0; f < NRHS; ++f) {
             const double fm = fvals ? fvals[(size_t)m * NRHS + f] : quad_fast(P.coef + 10 * f, xm, ym, zm);
-            const double df = (fm - fi[f]) * w * ir;
-#pragma unroll
-            for (int a = 0; a < K; ++a) B[f][a] += q[a] * df;
+            const double g = (fm - fi[f]) * W;
+            B[f][0] += g * dx, B[f][1] += g * dy, B[f][2] += g * dz;
+            B[f][3] += g * p[0], B[f][4] += g * p[3], B[f][5] += g * p[5];
+            B[f][6] += g * p[1], B[f][7] += g * p[2], B[f][8] += g * p[4];
         }
     }
-    if (ws > 0) {
-        const double inv = 1.0 / ws;
 #pragma unroll
-        for (int t = 0; t < NT; ++t) M[t] *= inv;
-    }
+    for (int f = 0; f < NRHS; ++f)
+#pragma unroll
+        for (int a = 0; a < K; ++a) B[f][a] *= basis_const(a, l0inv);
+    moments_from_sums(T, ws, l0inv, M);
     return ws;
 }
 
@@ -368,8 +392,10 @@ __device__ void atomic_max_nonneg(double* addr, double v) {
 
 // The right-hand sides accumulate in the moments' neighbor pass (one pass over the neighbors;
 // measured 22 % faster at 1M particles than a second right-hand-side pass, for 2 more registers).
-template <int NRHS, int PREC>
-__global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8_t* __restrict__ cls,
+// MINB > 1 caps the registers so that MINB blocks of 128 threads fit an SM (the Cholesky's
+// values spill to L1; the neighbor pass stays in registers).
+template <int NRHS, int PREC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_wls_all(WlsParams P, int n, const uint8_t* __restrict__ cls,
                                                  const double* __restrict__ sx, const double* __restrict__ sy,
                                                  const double* __restrict__ sz, const int* __restrict__ row,
                                                  const int* __restrict__ col, int* __restrict__ status,
@@ -548,8 +574,10 @@ __global__ void __launch_bounds__(128) k_wls_all(WlsParams P, int n, const uint8
     }
 }
 
-// Block sizes the autotuner chooses from (one particle per thread: same bits for each).
-constexpr int WLS_BLOCK[3] = {32, 64, 128};
+// Launch shapes the autotuner chooses from (one particle per thread: same bits for each):
+// blocks of 32, 64 or 128 threads with the compiler's register count, and (single field) 128
+// threads capped at 128 registers for four blocks per SM.
+constexpr int WLS_BLOCK[4] = {32, 64, 128, 128};
 
 // Outputs of one all-particle WLS launch (sorted order).
 struct WlsOut {
@@ -565,17 +593,24 @@ void launch_all(lsmps_ctx* ctx, const WlsParams& P, unsigned long long* gcnt, do
     const WlsOut o = dst ? *dst
                          : WlsOut{ctx->wls_status.get<int>(), ctx->wls_z.get<double>(), ctx->wls_wsum.get<double>(),
                                   ctx->wls_x.get<double>()};
+    constexpr bool capped = NRHS == 1;  // the register-capped shape exists for one field
     auto go = [&](int c) {
         const int t = WLS_BLOCK[c];
-        k_wls_all<NRHS, PREC><<<blocks_for(n, t), t, 0, ctx->stream>>>(
-            P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
-            ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), o.status, o.z, o.wsum, o.x, gcnt, gsum, fvals);
+        if (capped && c == 3)
+            k_wls_all<NRHS, PREC, capped ? 4 : 1><<<blocks_for(n, t), t, 0, ctx->stream>>>(
+                P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
+                ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), o.status, o.z, o.wsum, o.x, gcnt, gsum, fvals);
+        else
+            k_wls_all<NRHS, PREC, 1><<<blocks_for(n, t), t, 0, ctx->stream>>>(
+                P, n, ctx->cls.get<uint8_t>(), ctx->sx.get<double>(), ctx->sy.get<double>(), ctx->sz.get<double>(),
+                ctx->nbr_row.get<int>(), ctx->nbr_col.get<int>(), o.status, o.z, o.wsum, o.x, gcnt, gsum, fvals);
         LSMPS_CHECK_LAUNCH();
     };
-    static const std::vector<std::string> names = {"block32", "block64", "block128"};
+    static const std::vector<std::string> names3 = {"block32", "block64", "block128"};
+    static const std::vector<std::string> names4 = {"block32", "block64", "block128", "block128 regs128"};
     const std::string key = "wls_all nrhs" + std::to_string(NRHS) + (PREC ? " mixed" : " fp64");
     const size_t tuned_before = ctx->tuner.table.size();
-    const int c = autotune(ctx, key.c_str(), n, names, 2, go);
+    const int c = autotune(ctx, key.c_str(), n, capped ? names4 : names3, 2, go);
     if (ctx->tuner.table.size() != tuned_before)  // the timed launches added to the statistics
         LSMPS_CUDA(cudaMemsetAsync(gcnt, 0, 16 * sizeof(double), ctx->stream));
     go(c);
