@@ -339,7 +339,11 @@ __device__ __forceinline__ double accumulate_moments_rhs(int k, const double* __
     return ws;
 }
 
-// In-place packed Cholesky (reference pivot rule: > 1e-14 and finite) with diagonal add.
+// In-place packed Cholesky (reference pivot rule: > 1e-14 and finite) with diagonal add. The
+// diagonal slots receive the reciprocals 1 / L_ii (one reciprocal square root per pivot), so
+// the factor and both triangular solves multiply instead of dividing.
+__device__ __forceinline__ double recip_sqrt(double s) { return rsqrt(s); }
+__device__ __forceinline__ float recip_sqrt(float s) { return rsqrtf(s); }
 template <class T>
 __device__ __forceinline__ bool chol_packed(T* L, T add) {
 #pragma unroll
@@ -352,9 +356,9 @@ __device__ __forceinline__ bool chol_packed(T* L, T add) {
             for (int k = 0; k < j; ++k) s -= L[tri(i, k)] * L[tri(j, k)];
             if (i == j) {
                 if (!(s > (T)1e-14) || !isfinite(s)) return false;
-                L[tri(i, i)] = sqrt(s);
+                L[tri(i, i)] = recip_sqrt(s);
             } else {
-                L[tri(i, j)] = s / L[tri(j, j)];
+                L[tri(i, j)] = s * L[tri(j, j)];
             }
         }
     }
@@ -368,14 +372,14 @@ __device__ __forceinline__ void solve_packed(const T* L, T* x) {  // x holds b o
         T s = x[i];
 #pragma unroll
         for (int k = 0; k < i; ++k) s -= L[tri(i, k)] * x[k];
-        x[i] = s / L[tri(i, i)];
+        x[i] = s * L[tri(i, i)];
     }
 #pragma unroll
     for (int i = K - 1; i >= 0; --i) {
         T s = x[i];
 #pragma unroll
         for (int k = i + 1; k < K; ++k) s -= L[tri(k, i)] * x[k];
-        x[i] = s / L[tri(i, i)];
+        x[i] = s * L[tri(i, i)];
     }
 }
 
@@ -445,13 +449,15 @@ __global__ void __launch_bounds__(128, MINB) k_wls_all(WlsParams P, int n, const
                     fp32 = chol_packed<float>(Lf, 0.0f);
                     if (fp32) {
                         // ill-conditioned systems go to FP64: squared pivot ratio below 1e-3
-                        float dmin = Lf[0], dmax = Lf[0];
+                        // (the factor holds the pivots' reciprocals: the smallest pivot is the
+                        // reciprocal of the largest one stored)
+                        float rmin = Lf[0], rmax = Lf[0];
 #pragma unroll
                         for (int a = 1; a < K; ++a) {
-                            dmin = fminf(dmin, Lf[tri(a, a)]);
-                            dmax = fmaxf(dmax, Lf[tri(a, a)]);
+                            rmin = fminf(rmin, Lf[tri(a, a)]);
+                            rmax = fmaxf(rmax, Lf[tri(a, a)]);
                         }
-                        if (dmin * dmin < 1e-3f * dmax * dmax) fp32 = false;
+                        if (rmin * rmin < 1e-3f * rmax * rmax) fp32 = false;
                     }
                 }
                 if (fp32) {
@@ -610,7 +616,8 @@ void launch_all(lsmps_ctx* ctx, const WlsParams& P, unsigned long long* gcnt, do
     static const std::vector<std::string> names4 = {"block32", "block64", "block128", "block128 regs128"};
     const std::string key = "wls_all nrhs" + std::to_string(NRHS) + (PREC ? " mixed" : " fp64");
     const size_t tuned_before = ctx->tuner.table.size();
-    const int c = autotune(ctx, key.c_str(), n, capped ? names4 : names3, 2, go);
+    // without tuning: the capped shape for one field (fastest at 1M), else 128 threads
+    const int c = autotune(ctx, key.c_str(), n, capped ? names4 : names3, capped ? 3 : 2, go);
     if (ctx->tuner.table.size() != tuned_before)  // the timed launches added to the statistics
         LSMPS_CUDA(cudaMemsetAsync(gcnt, 0, 16 * sizeof(double), ctx->stream));
     go(c);
