@@ -213,8 +213,13 @@ __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ 
 //          w, w + WARPS, ..., so the block's warps gather the neighbors of a few consecutive
 //          nodes at a time and those rows (shared by ~3 nodes each in the cell-sorted order)
 //          are re-read from L1 instead of L2.
+// At most 72 registers (80 uncapped): the tuned shapes hold 24 warps per SM, which then leave
+// 10,240 registers free, so the multigrid set-up's kernels on the LEARNED solve's side stream
+// (blocks of at most 256 threads at 40 registers) run on the SMs beside the layer instead of
+// waiting for it (step 14.01 against 14.12-14.23 ms at 1M particles; the layer's own time is
+// unchanged, 503-511 us).
 template <int NB, int WARPS, bool LOCAL>
-__global__ void __launch_bounds__(WARPS * 32, 24 / WARPS)
+__global__ void __maxnreg__(72)
     k_layer_fwd(GView G, const bf16* __restrict__ h_in, bf16* __restrict__ h_out, const bf16* __restrict__ Wl,
                 const float* __restrict__ bl, bf16* __restrict__ a_save, float* __restrict__ z_save) {
     extern __shared__ __align__(16) unsigned char layer_smem[];

@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_tile_sums(const InT* __restric
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x < 32) {
-        long long v = ws[threadIdx.x];
+        long long v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0;
         v = warp_sum(v);
         if (threadIdx.x == 0) tile_sum[blockIdx.x] = v;
     }
