@@ -26,11 +26,8 @@ void* pinned_ensure(lsmps_ctx* ctx, size_t bytes) {
     return ctx->pinned;
 }
 
-void check_device_flags(lsmps_ctx* ctx, const char* where) {
-    int f = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&f, ctx->dflags.get<int>(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (!f) return;
+// Clears the device error flags and throws the error that set flag f names.
+static void raise_device_flags(lsmps_ctx* ctx, int f, const char* where) {
     LSMPS_CUDA(cudaMemsetAsync(ctx->dflags.get<int>(), 0, sizeof(int), ctx->stream));
     std::string w(where);
     if (f & DFLAG_NONFINITE) throw Error{LSMPS_ERR_NONFINITE, w + ": non-finite particle position"};
@@ -39,6 +36,32 @@ void check_device_flags(lsmps_ctx* ctx, const char* where) {
     if (f & DFLAG_TIMEOUT) throw Error{LSMPS_ERR_TIMEOUT, w + ": a bounded device wait expired"};
     if (f & DFLAG_STENCIL) throw Error{LSMPS_ERR_GRID, w + ": a coupling spans more than one neighbor cell"};
     throw Error{LSMPS_ERR_CUDA, w + ": device error flag " + std::to_string(f)};
+}
+
+void check_device_flags(lsmps_ctx* ctx, const char* where) { read_back(ctx, {}, where); }
+
+void read_back(lsmps_ctx* ctx, std::initializer_list<ReadBack> items, const char* where) {
+    auto span = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    size_t total = 16;
+    for (const ReadBack& r : items) total += span(r.bytes);
+    char* pin = static_cast<char*>(pinned_ensure(ctx, total));
+    cudaStream_t s = ctx->stream;
+    if (where) LSMPS_CUDA(cudaMemcpyAsync(pin, ctx->dflags.get<int>(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    size_t off = 16;
+    for (const ReadBack& r : items) {
+        if (r.bytes) LSMPS_CUDA(cudaMemcpyAsync(pin + off, r.src, r.bytes, cudaMemcpyDeviceToHost, s));
+        off += span(r.bytes);
+    }
+    LSMPS_CUDA(cudaStreamSynchronize(s));
+    off = 16;
+    for (const ReadBack& r : items) {
+        if (r.bytes) std::memcpy(r.dst, pin + off, r.bytes);
+        off += span(r.bytes);
+    }
+    if (!where) return;
+    int f = 0;
+    std::memcpy(&f, pin, sizeof(int));
+    if (f) raise_device_flags(ctx, f, where);
 }
 
 void ev_record(lsmps_ctx* ctx, int slot) { LSMPS_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream)); }

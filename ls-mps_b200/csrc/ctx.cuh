@@ -15,6 +15,7 @@
 //                              S_vals (A D^-1): E x f64, S_valf (A D^-1): E x f32, with
 //                              E = Z + padding (each slice padded to its longest row)
 #pragma once
+#include <initializer_list>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -147,4 +148,14 @@ namespace lsmps_gpu {
 void* pinned_ensure(lsmps_ctx* ctx, size_t bytes);
 // Read device int flags, clear them, and throw on any set flag.
 void check_device_flags(lsmps_ctx* ctx, const char* where);
+// A device value to read back to the host: bytes from src (device) to dst (host).
+struct ReadBack {
+    const void* src;
+    void* dst;
+    size_t bytes;
+};
+// Reads the values, and the device error flags unless where is null, in one synchronisation of
+// the context stream (copies into the context's pinned staging buffer), then throws on a set
+// flag as check_device_flags does.
+void read_back(lsmps_ctx* ctx, std::initializer_list<ReadBack> items, const char* where);
 }  // namespace lsmps_gpu

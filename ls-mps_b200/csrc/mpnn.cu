@@ -99,15 +99,19 @@ __device__ __forceinline__ unsigned a_addr(const bf16* tile, int ld, int k0, int
 }
 
 // ---- graph construction from the assembled PPE ---------------------------------------
-// warp per row (grid-stride), lanes over the row's entries
+// Four rows per warp step (grid-stride), eight lanes over each row's entries, so a warp has
+// four rows' loads in flight
 __global__ void k_graph_ew(long long U, const int* __restrict__ row, const double* __restrict__ val,
                            const double* __restrict__ dinv, float* __restrict__ ew) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, g = lane >> 3, sub = lane & 7;
     const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long u = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; u < U; u += nw) {
+    for (long long u0 = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) * 4; u0 < U; u0 += 4 * nw) {
+        const long long u = u0 + g;
+        if (u >= U) continue;
         const int e0 = row[u], e1 = row[u + 1];
         const double di = dinv[u];
-        for (int e = e0 + lane; e < e1; e += 32) ew[e] = e < e1 - 1 ? (float)(-val[e] * di) : 0.f;  // diagonal last
+#pragma unroll 4
+        for (int e = e0 + sub; e < e1; e += 8) ew[e] = e < e1 - 1 ? (float)(-val[e] * di) : 0.f;  // diagonal last
     }
 }
 
@@ -175,27 +179,40 @@ __device__ __forceinline__ void features(const GView& G, const float* __restrict
     x[3] = G.feat[3 * i + 2];
 }
 
-// h0 = ReLU(W_enc x + b_enc) (CUDA cores: K = 4)
+// h0 = ReLU(W_enc x + b_enc) (CUDA cores: K = 4). Four nodes per warp step, eight lanes per
+// node and eight features per lane (whose weights stay in registers), so each node's
+// 128-byte row is one coalesced store.
 __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ r, const float* __restrict__ w,
                                              bf16* __restrict__ h0, float* __restrict__ z0) {
-    __shared__ float sw[OFF_L0];
-    for (int k = threadIdx.x; k < (int)OFF_L0; k += blockDim.x) sw[k] = w[k];
-    __syncthreads();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < G.U; i += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, g = lane >> 3, c8 = (lane & 7) * 8;
+    float we[8][NF], be[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        be[q] = w[OFF_BE + c8 + q];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) we[q][f] = w[OFF_WE + (c8 + q) * NF + f];
+    }
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long i0 = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) * 4; i0 < G.U; i0 += 4 * nw) {
+        const long long i = i0 + g;
+        if (i >= G.U) continue;
         float x[NF];
         features(G, r, i, x);
-        for (int c8 = 0; c8 < H; c8 += 8) {
-            __align__(16) bf16 hv[8];
-            for (int q = 0; q < 8; ++q) {
-                const int c = c8 + q;
-                float zz = sw[OFF_BE + c];
+        __align__(16) bf16 hv[8];
+        __align__(16) float zv[8];
 #pragma unroll
-                for (int f = 0; f < NF; ++f) zz += sw[OFF_WE + c * NF + f] * x[f];
-                if (z0) z0[i * H + c] = zz;
-                hv[q] = __float2bfloat16(fmaxf(zz, 0.f));
-            }
-            *reinterpret_cast<uint4*>(h0 + i * H + c8) = *reinterpret_cast<const uint4*>(hv);
+        for (int q = 0; q < 8; ++q) {
+            float zz = be[q];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) zz += we[q][f] * x[f];
+            zv[q] = zz;
+            hv[q] = __float2bfloat16(fmaxf(zz, 0.f));
         }
+        if (z0) {
+            *reinterpret_cast<float4*>(z0 + i * H + c8) = *reinterpret_cast<const float4*>(zv);
+            *reinterpret_cast<float4*>(z0 + i * H + c8 + 4) = *reinterpret_cast<const float4*>(zv + 4);
+        }
+        *reinterpret_cast<uint4*>(h0 + i * H + c8) = *reinterpret_cast<const uint4*>(hv);
     }
 }
 

@@ -579,9 +579,7 @@ void mg_setup(lsmps_ctx* ctx) {
     LSMPS_CHECK_LAUNCH();
     scan_exclusive<int>(head, hscan, U, s, ctx->scan_tmp, dflag);
     int hn = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hn, hscan + U, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "multigrid aggregates");
+    read_back(ctx, {{hscan + U, &hn, sizeof(int)}}, "multigrid aggregates");
     long long n1 = hn;
     MgLevel& L1 = M.L[1];
     L1.n = n1;
@@ -621,8 +619,7 @@ void mg_setup(lsmps_ctx* ctx) {
         LSMPS_CHECK_LAUNCH();
         scan_exclusive<int>(flags, pos, nb, s, ctx->scan_tmp, dflag);
         int hc = 0;
-        LSMPS_CUDA(cudaMemcpyAsync(&hc, pos + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
-        LSMPS_CUDA(cudaStreamSynchronize(s));
+        read_back(ctx, {{pos + nb, &hc, sizeof(int)}}, nullptr);
         C.n = hc;
         int3* cc = C.coord.ensure<int3>(C.n);
         k_mg_assign<<<grid_for(nb, 256), 256, 0, s>>>(nb, flags, pos, C.dims[0], C.dims[1], cc, map);

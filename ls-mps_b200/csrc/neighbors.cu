@@ -856,9 +856,7 @@ void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out) {
         LSMPS_CHECK_LAUNCH();
     }
     std::vector<unsigned long long> h(8 + maxn + 1);
-    LSMPS_CUDA(cudaMemcpyAsync(h.data(), st, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                               ctx->stream));
-    LSMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+    read_back(ctx, {{st, h.data(), h.size() * sizeof(unsigned long long)}}, nullptr);
     h[5] = ctx->truncated;
     h[7] = (unsigned long long)ctx->max_cell_occupancy;
     fill_stats(ctx, h, out);
@@ -890,9 +888,7 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
         LSMPS_CHECK_LAUNCH();
     }
     int hb[6];
-    LSMPS_CUDA(cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "cell coordinates");
+    read_back(ctx, {{bounds, hb, sizeof(hb)}}, "cell coordinates");
     if (n == 0) { hb[0] = hb[1] = hb[2] = 0; hb[3] = hb[4] = hb[5] = 0; }
     for (int a = 0; a < 3; ++a) {
         ctx->gmin[a] = hb[a];
@@ -959,8 +955,7 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     k_list_segments<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(sg, nseg, seg_list, seg_count);
     LSMPS_CHECK_LAUNCH();
     int hsegs = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hsegs, seg_count, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
+    read_back(ctx, {{seg_count, &hsegs, sizeof(int)}}, nullptr);
     ctx->nsegs = hsegs;
     const unsigned seg_grid = (unsigned)std::max(hsegs, 1);
     const int do_cls = (flags & LSMPS_NBR_CLASSIFY) ? 1 : 0;
@@ -981,14 +976,10 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
         LSMPS_CHECK_LAUNCH();
     }
     scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
-    int hpairs = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hpairs, row + n, sizeof(int), cudaMemcpyDeviceToHost, s));
-    int hocc = 0;
+    int hpairs = 0, hocc = 0;
     unsigned long long htr = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hocc, big + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaMemcpyAsync(&htr, trunc_d, sizeof(htr), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "neighbor count");
+    read_back(ctx, {{row + n, &hpairs, sizeof(int)}, {big + 1, &hocc, sizeof(int)}, {trunc_d, &htr, sizeof(htr)}},
+              "neighbor count");
     ctx->pairs = (uint64_t)hpairs;
     ctx->truncated = htr;
     ctx->max_cell_occupancy = hocc;
@@ -1032,10 +1023,7 @@ bool nb_filter_single(lsmps_ctx* ctx, int classify) {
     scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
     int hpairs = 0;
     unsigned long long htr = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hpairs, row + n, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaMemcpyAsync(&htr, trunc_d, sizeof(htr), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "neighbor filter");
+    read_back(ctx, {{row + n, &hpairs, sizeof(int)}, {trunc_d, &htr, sizeof(htr)}}, "neighbor filter");
     ctx->pairs = (uint64_t)hpairs;
     ctx->truncated = htr;
     int* col = ctx->nbr_col.ensure<int>((size_t)hpairs + 1);

@@ -370,8 +370,7 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     }
     scan_exclusive<uint8_t>(isu, uidx, (long long)n, s, ctx->scan_tmp, dflag);
     int hU = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hU, uidx + n, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
+    read_back(ctx, {{uidx + n, &hU, sizeof(int)}}, nullptr);
     const long long U = hU;
     int* sorted_of_u = ctx->sorted_of_u.ensure<int>(U + 1);
     int* ref_of_u = ctx->ref_of_u.ensure<int>(U + 1);
@@ -412,9 +411,8 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     }
     scan_exclusive<int>(cnt, arow, U, s, ctx->scan_tmp, dflag);
     int hnnz = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hnnz, arow + U, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "PPE rows");
+    unsigned long long hs[2];  // the rows' statistics are final here
+    read_back(ctx, {{arow + U, &hnnz, sizeof(int)}, {st, hs, sizeof(hs)}}, "PPE rows");
     const long long nnz = hnnz;
     int* acol = ctx->A_col.ensure<int>(nnz + 1);
     double* aval = ctx->A_val.ensure<double>(nnz + 1);
@@ -424,9 +422,6 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
         LSMPS_CHECK_LAUNCH();
     }
     ev_record(ctx, 9);
-    unsigned long long hs[2];
-    LSMPS_CUDA(cudaMemcpyAsync(hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
     lsmps_ppe_stats ps{};
     ps.unknowns = (uint64_t)U;
     ps.nnz = (uint64_t)nnz;

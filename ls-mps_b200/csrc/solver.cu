@@ -1526,9 +1526,7 @@ static void sell_structure(lsmps_ctx* ctx) {
     }
     scan_exclusive<int>(ssize, sptr, ns, s, ctx->scan_tmp, ctx->dflags.get<int>());
     int total = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&total, sptr + ns, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "SELL layout");
+    read_back(ctx, {{sptr + ns, &total, sizeof(int)}}, "SELL layout");
     ctx->sell_nslices = ns;
     ctx->sell_entries = total;
     int* col = ctx->S_col.ensure<int>((size_t)total + 8);
@@ -1546,8 +1544,7 @@ static void sell_structure(lsmps_ctx* ctx) {
                                                               slen, col, val, dcol, rbase, vals, valf, bad);
         LSMPS_CHECK_LAUNCH();
         int hbad = 1;
-        LSMPS_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
-        LSMPS_CUDA(cudaStreamSynchronize(s));
+        read_back(ctx, {{bad, &hbad, sizeof(int)}}, nullptr);
         ctx->have_steps = hbad == 0 && ctx->sell_steps_enabled;
     }
     ctx->have_sell_s = ctx->have_sell_f = true;  // the scaled copies come with the structure

@@ -166,10 +166,7 @@ void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out) {
     scan_exclusive<int>(cnt, row, (long long)n, s, ctx->scan_tmp, dflag);
     int hpairs = 0;
     unsigned long long htr = 0;
-    LSMPS_CUDA(cudaMemcpyAsync(&hpairs, row + n, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaMemcpyAsync(&htr, trunc_d, sizeof(htr), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "neighbor filter count");
+    read_back(ctx, {{row + n, &hpairs, sizeof(int)}, {trunc_d, &htr, sizeof(htr)}}, "neighbor filter count");
     ctx->pairs = (uint64_t)hpairs;
     ctx->truncated = htr;
     int* col = ctx->nbr_col.ensure<int>((size_t)hpairs + 1);

@@ -706,9 +706,7 @@ void wls_run(lsmps_ctx* ctx, const lsmps_wls_opts* o, lsmps_wls_stats* out) {
     if (!out) return;  // no statistics wanted: no read-back, the host does not wait
     unsigned long long hc[8];
     double hs[4];
-    LSMPS_CUDA(cudaMemcpyAsync(hc, gcnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaMemcpyAsync(hs, gsum, sizeof(hs), cudaMemcpyDeviceToHost, s));
-    LSMPS_CUDA(cudaStreamSynchronize(s));
+    read_back(ctx, {{gcnt, hc, sizeof(hc)}, {gsum, hs, sizeof(hs)}}, nullptr);
     st.ok = hc[W_OK];
     st.regularized = hc[W_REG];
     st.skipped = hc[W_SKIP];
