@@ -211,14 +211,16 @@ def committed_traffic():
         return {}
 
 
-def step(ctx, solver, tol, max_iter, timings):
-    """One pass of the per-step path on the resident particle set."""
+def step(ctx, solver, tol, max_iter, timings, stats=True):
+    """One pass of the per-step path on the resident particle set. stats=False (the timed
+    steps): the neighbor build, WLS and assembly return no statistics, so the host does not
+    wait at the end of each phase (their times come from lsmps_get_timings)."""
     import lsmps_b200 as lib
 
     re = RE_RATIO * L0
-    nst = ctx.build_neighbors(re, MAXN, L0)
+    nst = ctx.build_neighbors(re, MAXN, L0, stats=stats)
     ctx.wls(re, L0, mode=1, stats=False)  # no statistics read-back: the host does not wait here
-    pst = ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0)
+    pst = ctx.ppe_assemble("wls", 10**12, re, L0, diag_shift=0.0, stats=stats)
     sv, pc, ug = SOLVER_SPECS[solver]
     s = ctx.ppe_solve(sv, max_iter, tol, precond=pc, use_graph=ug)
     t = ctx.timings()
@@ -274,7 +276,7 @@ def run_mine(args, dist):
     l2s = []
     for i in range(args.steps):
         put(i % K)
-        nst, pst, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings)
+        _, _, s, _ = step(ctx, args.solver, args.tol, args.max_iter, timings, stats=False)
         l2s.append(s.relative_l2_error)
     ev1.record(stream)
     ev1.synchronize()
@@ -310,8 +312,8 @@ def run_mine(args, dist):
         ctx.use_prefetched()
         if i + 1 < args.steps:
             ctx.prefetch(*pins[(i + 1) % K])
-        _, pst_e, _, _ = step(ctx, args.solver, args.tol, args.max_iter, [])
-        u = int(pst_e.unknowns)
+        _, _, s_e, _ = step(ctx, args.solver, args.tol, args.max_iter, [], stats=False)
+        u = int(s_e.unknowns)
         ctx.pressure_into_async(pin_ps[i % 2][:u])
         d2h.append(8 * u)
     ctx.download_wait()

@@ -141,7 +141,10 @@ typedef struct lsmps_neighbor_stats {
  * (src/lsmps.cpp:16-18,26): cell = floor(r / re) per axis, 27 cells dz, dy, dx from -1
  * to 1, ascending index within a cell, |rj - ri|^2 < re^2 without FMA contraction, first
  * max_neighbors kept. With LSMPS_NBR_CLASSIFY also classify() (src/lsmps.cpp:27) with l0.
- * re must be the caller's re_ratio * l0 product, as run_benchmark (src/lsmps.cpp:73). */
+ * re must be the caller's re_ratio * l0 product, as run_benchmark (src/lsmps.cpp:73). With
+ * out == NULL the statistics are neither computed nor read back, and the call returns once the
+ * lists' last kernels are queued (the host waits only for the pair count, which sizes the
+ * lists); its phase time is read later by lsmps_get_timings. */
 int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l0, int flags,
                           lsmps_neighbor_stats* out);
 /* classify() (src/lsmps.cpp:27) over the current neighbor lists, standalone. */
@@ -222,7 +225,10 @@ typedef struct lsmps_ppe_stats {
     double relative_residual;   /* |b - Ax| / |b| at exit (FP64) */
 } lsmps_ppe_stats;
 
-/* assemble_ppe (src/lsmps.cpp:30-64) and its variants; keeps A, b = A p*, p* on the device. */
+/* assemble_ppe (src/lsmps.cpp:30-64) and its variants; keeps A, b = A p*, p* on the device.
+ * With out == NULL the call returns once the matrix's last kernel is queued (the host waits
+ * only for the unknown and nonzero counts); its phase time is read by lsmps_get_timings or
+ * reported by the next lsmps_ppe_solve. */
 int lsmps_ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_stats* out);
 
 /* A caller's sparse system in place of an assembled PPE, for the solvers and kernel benches

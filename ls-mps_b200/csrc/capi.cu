@@ -66,6 +66,15 @@ void read_back(lsmps_ctx* ctx, std::initializer_list<ReadBack> items, const char
 
 void ev_record(lsmps_ctx* ctx, int slot) { LSMPS_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream)); }
 
+void resolve_timings(lsmps_ctx* ctx) {
+    if (ctx->timing_pending & 2u) ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+    if (ctx->timing_pending & 8u) ctx->timings[3] = ev_elapsed(ctx, 6, 7);
+    if (ctx->timing_pending & 16u) {
+        ctx->timings[4] = ctx->ppe_assembly.assembly_ms = ev_elapsed(ctx, 8, 9);
+    }
+    ctx->timing_pending = 0;
+}
+
 double ev_elapsed(lsmps_ctx* ctx, int a, int b) {
     LSMPS_CUDA(cudaEventSynchronize(ctx->ev[b]));
     float ms = 0;
@@ -243,10 +252,9 @@ const char* lsmps_last_error(const lsmps_ctx* ctx) { return ctx ? ctx->last_erro
 
 int lsmps_get_timings(lsmps_ctx* ctx, double out[8]) {
     if (!ctx || !out) return LSMPS_ERR_ARG;
-    if (ctx->wls_timing_pending) {  // a WLS call that did not wait: its events are read now
-        const int rc = guarded(ctx, [&] { ctx->timings[3] = ev_elapsed(ctx, 6, 7); });
+    if (ctx->timing_pending) {  // calls that did not wait: their events are read now
+        const int rc = guarded(ctx, [&] { resolve_timings(ctx); });
         if (rc != LSMPS_OK) return rc;
-        ctx->wls_timing_pending = false;
     }
     std::memcpy(out, ctx->timings, sizeof(ctx->timings));
     return LSMPS_OK;
@@ -323,7 +331,13 @@ int lsmps_build_neighbors(lsmps_ctx* ctx, double re, int max_neighbors, double l
         ev_record(ctx, 2);
         nb_build(ctx, re, max_neighbors, l0, flags, out);
         ev_record(ctx, 3);
-        ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+        // without statistics the call does not wait for its last kernels; its time is read later
+        if (out) {
+            ctx->timing_pending &= ~2u;
+            ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+        } else {
+            ctx->timing_pending |= 2u;
+        }
     });
 }
 
@@ -334,6 +348,7 @@ int lsmps_build_neighbors_skin(lsmps_ctx* ctx, double re, double skin, int max_n
         nb_build_skin(ctx, re, skin, max_neighbors, max_candidates, l0, flags, out);
         ev_record(ctx, 3);
         ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+        ctx->timing_pending &= ~2u;
     });
 }
 
@@ -351,6 +366,7 @@ int lsmps_refresh_neighbors(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out
         nb_refresh(ctx, flags, out);
         ev_record(ctx, 3);
         ctx->timings[1] = ev_elapsed(ctx, 2, 3);
+        ctx->timing_pending &= ~2u;
     });
 }
 
@@ -377,8 +393,12 @@ int lsmps_wls(lsmps_ctx* ctx, const lsmps_wls_opts* opts, lsmps_wls_stats* out) 
         wls_run(ctx, opts, out);
         ev_record(ctx, 7);
         // without statistics the call does not wait; its time is read by lsmps_get_timings
-        ctx->wls_timing_pending = out == nullptr;
-        if (out) ctx->timings[3] = ev_elapsed(ctx, 6, 7);
+        if (out) {
+            ctx->timing_pending &= ~8u;
+            ctx->timings[3] = ev_elapsed(ctx, 6, 7);
+        } else {
+            ctx->timing_pending |= 8u;
+        }
     });
 }
 
@@ -386,7 +406,13 @@ int lsmps_ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* opts, lsmps_ppe_sta
     return guarded(ctx, [&] {
         LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null PPE options");
         ppe_assemble(ctx, opts, out);
-        ctx->timings[4] = ctx->ppe_assembly.assembly_ms;
+        // without statistics the call does not wait for its last kernels; its time is read later
+        if (out) {
+            ctx->timing_pending &= ~16u;
+            ctx->timings[4] = ctx->ppe_assembly.assembly_ms;
+        } else {
+            ctx->timing_pending |= 16u;
+        }
     });
 }
 
@@ -394,6 +420,11 @@ int lsmps_ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* opts, lsmps_ppe_sta
     return guarded(ctx, [&] {
         LSMPS_REQUIRE(opts, LSMPS_ERR_ARG, "null solver options");
         ppe_solve(ctx, opts, out);
+        // an assembly that did not wait: its events are complete once the solve has returned
+        if (ctx->timing_pending & 16u) {
+            resolve_timings(ctx);
+            if (out) out->assembly_ms = ctx->ppe_assembly.assembly_ms;
+        }
     });
 }
 

@@ -62,7 +62,9 @@ struct lsmps_ctx {
     size_t stage_n = 0;
     bool have_stage = false;
     double timings[8] = {};
-    bool wls_timing_pending = false;  // timings[3] of a WLS call without statistics, not yet read
+    // phase times of calls made without statistics, which do not wait: their events are read
+    // later (bit 1: neighbors, events 2-3; bit 3: WLS, 6-7; bit 4: assembly, 8-9)
+    unsigned timing_pending = 0;
 
     lsmps_gpu::DevBuf dflags;      // int device error flags
     lsmps_gpu::DevBuf scratch;     // general reduction scratch

@@ -59,11 +59,25 @@ __global__ void k_cell_coords(const double* __restrict__ pos, size_t n, double r
             mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
         }
     }
+    // the block's bounds, then six atomics per block (per-warp atomics on the same six words
+    // serialise in L2: ~9.5k per word at 1M particles)
+    __shared__ int sb[6][32];
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            if (mn[a] != INT_MAX) atomicMin(&bounds[a], mn[a]);
-            if (mx[a] != INT_MIN) atomicMax(&bounds[3 + a], mx[a]);
+            sb[a][warp] = mn[a];
+            sb[3 + a][warp] = mx[a];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        int v = sb[a][0];
+        for (int w = 1; w < nwarps; ++w) v = a < 3 ? min(v, sb[a][w]) : max(v, sb[a][w]);
+        if (a < 3 ? v != INT_MAX : v != INT_MIN) {
+            if (a < 3) atomicMin(&bounds[a], v);
+            else atomicMax(&bounds[a], v);
         }
     }
     if (bad) atomicOr(dflag, DFLAG_NONFINITE);
@@ -87,7 +101,41 @@ __global__ void k_scatter(const int* __restrict__ lin, const int* __restrict__ s
     perm[cell_start[lin[i]] + slot[i]] = (int)i;
 }
 
-// Atomic slots leave a cell's members in arbitrary order; restore ascending index.
+// Atomic slots leave a cell's members in arbitrary order; restore ascending index (cells of up
+// to 32 members sorted in registers, up to SMALL_CELL in place).
+// Ascending bitonic sort of N (a power of two) values held in registers (the loops unroll to
+// fixed indices).
+template <int N>
+__device__ __forceinline__ void bitonic_sort_regs(int (&v)[N]) {
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int a = v[i], c = v[l];
+                    const bool asc = (i & k) == 0;
+                    v[i] = asc ? min(a, c) : max(a, c);
+                    v[l] = asc ? max(a, c) : min(a, c);
+                }
+            }
+}
+
+// A cell's members (occ <= N, distinct indices) sorted ascending in registers: all loads in
+// flight at once, padding INT_MAX sorts last.
+template <int N>
+__device__ __forceinline__ void sort_cell_regs(int* __restrict__ perm, int b, int occ) {
+    int v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = i < occ ? perm[b + i] : INT_MAX;
+    bitonic_sort_regs<N>(v);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (i < occ) perm[b + i] = v[i];
+}
+
 __global__ void k_sort_small_cells(const int* __restrict__ cell_start, long long ncells,
                                    int* __restrict__ perm, int* big_list, int* big_count,
                                    int* max_occ) {
@@ -99,6 +147,10 @@ __global__ void k_sort_small_cells(const int* __restrict__ cell_start, long long
         if (occ > SMALL_CELL) {
             int slot = atomicAdd(big_count, 1);
             big_list[slot] = (int)c;
+        } else if (occ > 1 && occ <= 16) {
+            sort_cell_regs<16>(perm, b, occ);
+        } else if (occ > 1 && occ <= 32) {
+            sort_cell_regs<32>(perm, b, occ);
         } else if (occ > 1) {
             for (int a = b + 1; a < e; ++a) {
                 int v = perm[a];
@@ -113,7 +165,15 @@ __global__ void k_sort_small_cells(const int* __restrict__ cell_start, long long
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) occ = max(occ, __shfl_xor_sync(0xffffffffu, occ, o));
-    if ((threadIdx.x & 31) == 0 && occ > 0) atomicMax(max_occ, occ);
+    // one atomic per block (per-warp atomics on one word serialise in L2)
+    __shared__ int socc[32];
+    if ((threadIdx.x & 31) == 0) socc[threadIdx.x >> 5] = occ;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = max(m, socc[w]);
+        if (m > 0) atomicMax(max_occ, m);
+    }
 }
 
 // One block per crowded cell: bitonic sort in shared memory (padding with INT_MAX).
@@ -844,7 +904,7 @@ static void fill_stats(lsmps_ctx* ctx, const std::vector<unsigned long long>& st
     if (out) *out = s;
 }
 
-void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out) {
+void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out, const char* where) {
     int n = (int)ctx->n;
     int maxn = ctx->maxn;
     auto* st = ctx->nbr_stats.ensure<unsigned long long>(8 + maxn + 1);
@@ -856,7 +916,7 @@ void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out) {
         LSMPS_CHECK_LAUNCH();
     }
     std::vector<unsigned long long> h(8 + maxn + 1);
-    read_back(ctx, {{st, h.data(), h.size() * sizeof(unsigned long long)}}, nullptr);
+    read_back(ctx, {{st, h.data(), h.size() * sizeof(unsigned long long)}}, where);
     h[5] = ctx->truncated;
     h[7] = (unsigned long long)ctx->max_cell_occupancy;
     fill_stats(ctx, h, out);
@@ -995,9 +1055,9 @@ void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_n
     }
     ctx->have_neighbors = true;
     ctx->have_classes = do_cls != 0;
-    nb_stats(ctx, out);
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "neighbor fill");
+    // without statistics nothing is read back here (no device flag is set after the count's
+    // read-back), so the host does not wait for the compaction
+    if (out) nb_stats(ctx, out, "neighbor fill");
 }
 
 bool nb_filter_single(lsmps_ctx* ctx, int classify) {

@@ -18,7 +18,8 @@ void series_rain_outputs(lsmps_series* s, lsmps_rain_outputs* out);
 lsmps_ctx* series_context(lsmps_series* s);
 void nb_build(lsmps_ctx* ctx, double re, int maxn, double l0, int flags, lsmps_neighbor_stats* out);
 void nb_classify(lsmps_ctx* ctx, double l0, lsmps_neighbor_stats* out);
-void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out);
+// Neighbor statistics (one read-back; with `where`, the device error flags in the same one).
+void nb_stats(lsmps_ctx* ctx, lsmps_neighbor_stats* out, const char* where = nullptr);
 void nb_download(lsmps_ctx* ctx, int32_t* row_ptr, int32_t* col, size_t col_cap);
 void nb_download_types(lsmps_ctx* ctx, uint8_t* type, size_t n);
 void nb_build_skin(lsmps_ctx* ctx, double re, double skin, int maxn, int maxc, double l0, int flags,
@@ -106,5 +107,7 @@ std::string autotune_report(lsmps_ctx* ctx);
 
 void ev_record(lsmps_ctx* ctx, int slot);
 double ev_elapsed(lsmps_ctx* ctx, int a, int b);
+// Reads the phase times of calls that did not wait (statistics not requested).
+void resolve_timings(lsmps_ctx* ctx);
 
 }  // namespace lsmps_gpu

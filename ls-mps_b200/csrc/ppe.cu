@@ -429,7 +429,7 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     // the reference counts NearWall rows except the pinned row 0 (src/lsmps.cpp:45,56)
     ps.neumann = hs[0];
     ps.failed_rows = hs[1];
-    ps.assembly_ms = ev_elapsed(ctx, 8, 9);
+    ps.assembly_ms = out ? ev_elapsed(ctx, 8, 9) : 0.0;  // without statistics: read later
     ctx->U = U;
     ctx->nnz = nnz;
     ctx->ppe_variant = o->variant;
@@ -522,6 +522,7 @@ void ppe_load_csr(lsmps_ctx* ctx, const int64_t* row_ptr, const int32_t* col, co
     ctx->assembly_gen += 1;
     ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = false;
     ctx->ppe_assembly = ps;
+    ctx->timing_pending &= ~16u;  // a loaded system has no pending assembly time
     if (out) *out = ps;
 }
 

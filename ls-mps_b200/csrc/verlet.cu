@@ -144,8 +144,7 @@ void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out) {
         ctx->have_neighbors = true;
         ctx->have_classes = classify != 0;
         ctx->have_wls = ctx->have_ppe = ctx->have_solution = false;
-        nb_stats(ctx, out);
-        check_device_flags(ctx, "neighbor filter");
+        nb_stats(ctx, out, "neighbor filter");
         return;
     }
     cudaStream_t s = ctx->stream;
@@ -183,7 +182,8 @@ void nb_refresh(lsmps_ctx* ctx, int flags, lsmps_neighbor_stats* out) {
         nb_classify(ctx, ctx->l0, out);
     } else {
         ctx->cls.ensure<uint8_t>(ctx->n + 1);
-        nb_stats(ctx, out);
+        nb_stats(ctx, out, "neighbor filter");
+        return;
     }
     check_device_flags(ctx, "neighbor filter");
 }

@@ -350,9 +350,14 @@ class Context:
         self._xyz, self._types = self._staged
         self.n = len(self._types)
 
-    def build_neighbors(self, re, max_neighbors, l0, classify=True, two_pass=False):
-        st = NeighborStats()
+    def build_neighbors(self, re, max_neighbors, l0, classify=True, two_pass=False, stats=True):
+        """lsmps_build_neighbors; stats=False skips the statistics (and the wait for the lists'
+        last kernels) and returns None."""
         flags = (NBR_CLASSIFY if classify else 0) | (NBR_TWO_PASS if two_pass else 0)
+        if not stats:
+            self._check(self.L.lsmps_build_neighbors(self.h, re, max_neighbors, l0, flags, None))
+            return None
+        st = NeighborStats()
         self._check(self.L.lsmps_build_neighbors(self.h, re, max_neighbors, l0, flags, C.byref(st)))
         return st
 
@@ -400,9 +405,14 @@ class Context:
         self._check(self.L.lsmps_wls(self.h, C.byref(o), C.byref(st)))
         return st
 
-    def ppe_assemble(self, variant, max_unknowns, re, l0, diag_shift=1e-3, wall_neumann=False):
+    def ppe_assemble(self, variant, max_unknowns, re, l0, diag_shift=1e-3, wall_neumann=False, stats=True):
+        """lsmps_ppe_assemble; stats=False does not wait for the matrix's last kernel and returns
+        None (its time comes with the next solve's statistics)."""
         o = PpeOpts(variant=VARIANTS.get(variant, variant), max_unknowns=int(max_unknowns), re=re,
                     l0=l0, diag_shift=diag_shift, flags=PPE_WALL_NEUMANN if wall_neumann else 0)
+        if not stats:
+            self._check(self.L.lsmps_ppe_assemble(self.h, C.byref(o), None))
+            return None
         st = PpeStats()
         self._check(self.L.lsmps_ppe_assemble(self.h, C.byref(o), C.byref(st)))
         self._last_ppe = st

@@ -93,3 +93,30 @@ def test_cap_and_empty(ctx):
     assert st.unknowns == 0 and st.nnz == 0
     s = ctx.ppe_solve("reference", 10, 1e-7)
     assert s.iterations == 0 and s.converged == 0
+
+
+def test_neighbors_and_assembly_without_statistics(ctx):
+    """A neighbor build and an assembly called without statistics (out = NULL) return without
+    waiting for their last kernels, leave the same lists and system as with statistics, and
+    their phase times are read by lsmps_get_timings (the assembly's also by the next solve)."""
+    xyz, t, _ = lib.generate(None, case="mixed", particles=50_000, l0=1.0, seed=4)
+    ctx.upload(xyz, t)
+    nst = ctx.build_neighbors(2.1, 128, 1.0)
+    row, col = ctx.neighbors(nst.pairs)
+    ctx.wls(2.1, 1.0, mode=1)
+    pst = ctx.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0)
+    ref = ctx.ppe(pst.unknowns, pst.nnz)
+    assert ctx.build_neighbors(2.1, 128, 1.0, stats=False) is None
+    tm = ctx.timings()
+    assert tm[1] > 0.0
+    row2, col2 = ctx.neighbors(nst.pairs)
+    assert np.array_equal(row, row2) and np.array_equal(col, col2)
+    ctx.wls(2.1, 1.0, mode=1, stats=False)
+    assert ctx.ppe_assemble("wls", 10**12, 2.1, 1.0, diag_shift=0.0, stats=False) is None
+    s = ctx.ppe_solve("mixed", 5000, 1e-10, precond="multigrid")
+    assert s.converged and s.assembly_ms > 0.0
+    assert s.unknowns == pst.unknowns and s.nnz == pst.nnz
+    assert ctx.timings()[4] == s.assembly_ms
+    got = ctx.ppe(pst.unknowns, pst.nnz)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
