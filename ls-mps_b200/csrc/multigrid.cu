@@ -46,7 +46,7 @@
 namespace lsmps_gpu {
 
 constexpr int MG_MAX_LEVELS = 40;
-constexpr int MG_COARSE_MAX = 256;       // rows of the coarsest level
+constexpr int MG_COARSE_MAX = 640;       // rows of the coarsest level (one block)
 constexpr int MG_SWEEPS = 10;            // Jacobi sweeps on the coarsest level
 constexpr float MG_OMEGA = 1.0f;         // smoother damping
 constexpr float MG_ALPHA = 1.5f;         // coarse-correction scaling
@@ -410,9 +410,14 @@ __global__ void k_mg_down(long long nc, const int* __restrict__ child, const flo
     if (lane == 0) rc[B] = res;
 }
 
-// Coarsest level (n <= MG_COARSE_MAX rows): Jacobi sweeps from 0 in one block, one thread
-// per row, stencil and iterate in shared memory. A single block pays each dependent L2 round
-// trip in series, so only this level runs in one (the levels above it get grid-wide kernels).
+// Coarsest level (n <= MG_COARSE_MAX rows): Jacobi sweeps from 0 in one block of nb >= n
+// threads (a multiple of 32), one thread per row with its 27 stencil values and neighbor rows
+// in registers, the iterate in shared memory (no large shared-memory carve-out, which would
+// make the SM reconfigure between the V-cycle's kernels). A single block pays each dependent
+// L2 round trip in series, so only this level runs in one (the levels above it get grid-wide
+// kernels). At 1M particles a coarsest level of up to 640 rows ends the hierarchy one level
+// earlier (537 rows instead of a further level of 82): the restatement's iterations stay the
+// same (26-28 against 28), and each V-cycle saves a down and an up step.
 __global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarsest(int n, const float* __restrict__ val,
                                                                const int* __restrict__ nbr,
                                                                const float* __restrict__ dinv,
@@ -421,14 +426,14 @@ __global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarsest(int n, const floa
     pdl_begin();
     if (gated(S, need_s)) return;
     __shared__ float cur[2][MG_COARSE_MAX];
-    __shared__ float cv[MG_SLOTS][MG_COARSE_MAX];
-    __shared__ short cn[MG_SLOTS][MG_COARSE_MAX];
     const int I = threadIdx.x;
     const bool own = I < n;
+    float cv[MG_SLOTS];
+    int cn[MG_SLOTS];
 #pragma unroll
     for (int t = 0; t < MG_SLOTS; ++t) {
-        cv[t][I] = own ? val[slot_index(I, t)] : 0.0f;
-        cn[t][I] = (short)(own ? max(nbr[slot_index(I, t)], 0) : 0);  // empty slots hold 0
+        cv[t] = own ? val[slot_index(I, t)] : 0.0f;
+        cn[t] = own ? max(nbr[slot_index(I, t)], 0) : 0;  // empty slots hold 0
     }
     const float ri = own ? r[I] : 0.0f, di = own ? dinv[I] : 0.0f;
     float x = MG_OMEGA * ri * di;  // first sweep from 0
@@ -438,7 +443,7 @@ __global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarsest(int n, const floa
     for (int it = 1; it < MG_SWEEPS; ++it) {
         float s = 0.0f;
 #pragma unroll
-        for (int t = 0; t < MG_SLOTS; ++t) s += cv[t][I] * cur[b][cn[t][I]];
+        for (int t = 0; t < MG_SLOTS; ++t) s += cv[t] * cur[b][cn[t]];
         x = x + MG_OMEGA * di * (ri - s);
         cur[b ^ 1][I] = x;
         __syncthreads();
@@ -692,7 +697,8 @@ void mg_apply(lsmps_ctx* ctx, const double* z, double* out, const BcgScalars* S,
                        L[l].x.get<float>(), L[l + 1].r.get<float>(), S, need_s);
         }
     }
-    launch_pdl(k_mg_coarsest, 1, MG_COARSE_MAX, 0, s, (int)L[Lc].n, L[Lc].val.get<float>(), L[Lc].nbr.get<int>(),
+    const int nbc = (int)std::max<long long>(32, (L[Lc].n + 31) / 32 * 32);
+    launch_pdl(k_mg_coarsest, 1, nbc, 0, s, (int)L[Lc].n, L[Lc].val.get<float>(), L[Lc].nbr.get<int>(),
                L[Lc].dinv.get<float>(), L[Lc].r.get<float>(), L[Lc].e.get<float>(), S, need_s);
     for (int l = Lc - 1; l >= 1; --l)
         launch_pdl(k_mg_up, grid_for(4 * L[l].n, 256), 256, 0, s, L[l].n, L[l].val.get<float>(), L[l].nbr.get<int>(),

@@ -22,7 +22,7 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
-COARSE_MAX = 256
+COARSE_MAX = 640
 SWEEPS = 10
 OMEGA = 1.0
 ALPHA = 1.5
