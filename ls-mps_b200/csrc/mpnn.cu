@@ -181,7 +181,7 @@ __device__ __forceinline__ void features(const GView& G, const float* __restrict
 
 // h0 = ReLU(W_enc x + b_enc) (CUDA cores: K = 4). Four nodes per warp step, eight lanes per
 // node and eight features per lane (whose weights stay in registers), so each node's
-// 128-byte row is one coalesced store.
+// 128-byte row is one coalesced store; four steps' inputs are loaded before their sums.
 __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ r, const float* __restrict__ w,
                                              bf16* __restrict__ h0, float* __restrict__ z0) {
     const int lane = threadIdx.x & 31, g = lane >> 3, c8 = (lane & 7) * 8;
@@ -193,26 +193,35 @@ __global__ void __launch_bounds__(256) k_enc(GView G, const float* __restrict__ 
         for (int f = 0; f < NF; ++f) we[q][f] = w[OFF_WE + (c8 + q) * NF + f];
     }
     const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long i0 = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) * 4; i0 < G.U; i0 += 4 * nw) {
-        const long long i = i0 + g;
-        if (i >= G.U) continue;
-        float x[NF];
-        features(G, r, i, x);
-        __align__(16) bf16 hv[8];
-        __align__(16) float zv[8];
+    constexpr int STEPS = 4;
+    for (long long i0 = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) * 4; i0 < G.U;
+         i0 += 4 * STEPS * nw) {
+        float x[STEPS][NF];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            float zz = be[q];
+        for (int k = 0; k < STEPS; ++k) {
+            const long long i = i0 + 4 * k * nw + g;
+            if (i < G.U) features(G, r, i, x[k]);
+        }
 #pragma unroll
-            for (int f = 0; f < NF; ++f) zz += we[q][f] * x[f];
-            zv[q] = zz;
-            hv[q] = __float2bfloat16(fmaxf(zz, 0.f));
+        for (int k = 0; k < STEPS; ++k) {
+            const long long i = i0 + 4 * k * nw + g;
+            if (i >= G.U) continue;
+            __align__(16) bf16 hv[8];
+            __align__(16) float zv[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                float zz = be[q];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zz += we[q][f] * x[k][f];
+                zv[q] = zz;
+                hv[q] = __float2bfloat16(fmaxf(zz, 0.f));
+            }
+            if (z0) {
+                *reinterpret_cast<float4*>(z0 + i * H + c8) = *reinterpret_cast<const float4*>(zv);
+                *reinterpret_cast<float4*>(z0 + i * H + c8 + 4) = *reinterpret_cast<const float4*>(zv + 4);
+            }
+            *reinterpret_cast<uint4*>(h0 + i * H + c8) = *reinterpret_cast<const uint4*>(hv);
         }
-        if (z0) {
-            *reinterpret_cast<float4*>(z0 + i * H + c8) = *reinterpret_cast<const float4*>(zv);
-            *reinterpret_cast<float4*>(z0 + i * H + c8 + 4) = *reinterpret_cast<const float4*>(zv + 4);
-        }
-        *reinterpret_cast<uint4*>(h0 + i * H + c8) = *reinterpret_cast<const uint4*>(hv);
     }
 }
 
