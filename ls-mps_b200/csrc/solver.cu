@@ -1775,7 +1775,10 @@ static void side_stream_fork(lsmps_ctx* ctx) {
 // Jacobi-BiCGStab (fallback). With the multigrid preconditioner a stall (no 1 % progress in
 // `stall_window` iterations) or a breakdown ends the multigrid phase, and the solve continues
 // as Jacobi MIXED from the current iterate (from zero when it is no longer finite; fallback).
-static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned) {
+// exit_res (optional): {|b - A D^-1 y|, |b|} of the returned iterate when the solve converged
+// (the convergence test's own FP64 residual), else {-1, -1}.
+static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool learned,
+                        double* exit_res = nullptr) {
     cudaStream_t s = ctx->stream;
     const long long U = ctx->U;
     Engine E = make_engine(ctx);
@@ -2009,6 +2012,14 @@ static void solve_mixed(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
     ps->converged = converged;
     ps->fallback = fallback;
     ps->solve_ms = ev_elapsed(ctx, 10, 11);
+    if (exit_res) {
+        // convergence is only declared right after a residual replacement or a (re)start (in
+        // the device-driven loop too, which runs the same kernels in the same order), whose
+        // FP64 residual b - A D^-1 y of the final iterate h holds
+        const bool exact = converged && std::isfinite(h.rn);
+        exit_res[0] = exact ? h.rn : -1.0;
+        exit_res[1] = exact ? h.bnorm : -1.0;
+    }
 }
 
 void ppe_set_initial_particles(lsmps_ctx* ctx, const double* pp, size_t n, bool device) {
@@ -2078,17 +2089,20 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
     if (o->solver == LSMPS_SOLVER_REFERENCE) {
         solve_exact(ctx, o, &ps);
     } else {
+        double exit_res[2] = {-1.0, -1.0};
         if (o->solver == LSMPS_SOLVER_FP64) solve_fast64(ctx, o, &ps, false);
         else if (o->solver == LSMPS_SOLVER_JACOBI) solve_fast64(ctx, o, &ps, true);
         else if (o->solver == LSMPS_SOLVER_MIXED_F32) solve_mixed_f32(ctx, o, &ps, false);
-        else solve_mixed(ctx, o, &ps, o->solver == LSMPS_SOLVER_LEARNED);
-        // final statistics in FP64: |Ax - b|, |b|, error against p*
+        else solve_mixed(ctx, o, &ps, o->solver == LSMPS_SOLVER_LEARNED, exit_res);
+        // final statistics in FP64: |Ax - b|, |b| (for a converged MIXED / LEARNED solve the
+        // convergence test's own FP64 residual of the final iterate, |b - A D^-1 y| with
+        // y = D x), error against p*
         cudaStream_t s = ctx->stream;
         Engine E = make_engine(ctx);
         double* scal = engine_scalars(ctx);
         double* x = ctx->vx.get<double>();
         double* tmp = ctx->vt.ensure<double>(U + 1);
-        residual64(E, sell_a64(ctx), ctx->A_b.get<double>(), x, tmp, scal);
+        if (exit_res[0] < 0) residual64(E, sell_a64(ctx), ctx->A_b.get<double>(), x, tmp, scal);
         auto* maxbits = reinterpret_cast<unsigned long long*>(scal + 4);
         LSMPS_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), s));
         k_error_stats<<<RGRID, RB, 0, s>>>(U, x, ctx->A_xexact.get<double>(), scal + 2, E.P, &E.S->counter[6],
@@ -2097,8 +2111,8 @@ void ppe_solve(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* out)
         double h[5];
         LSMPS_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, s));
         LSMPS_CUDA(cudaStreamSynchronize(s));
-        ps.initial_residual = std::sqrt(h[1]);
-        ps.final_residual = std::sqrt(h[0]);
+        ps.initial_residual = exit_res[0] < 0 ? std::sqrt(h[1]) : exit_res[1];
+        ps.final_residual = exit_res[0] < 0 ? std::sqrt(h[0]) : exit_res[0];
         ps.relative_residual = ps.final_residual / std::max(ps.initial_residual, 1e-300);
         ps.relative_l2_error = std::sqrt(h[2] / std::max(h[3], 1e-30));
         unsigned long long mb;
