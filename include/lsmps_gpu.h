@@ -218,6 +218,9 @@ typedef struct lsmps_ppe_stats {
     uint64_t unknowns, nnz, dirichlet, neumann, failed_rows;
     int32_t iterations, converged;
     double initial_residual, final_residual, relative_l2_error, max_error, assembly_ms, solve_ms;
+    /* final_residual is |b - A x| in FP64; for a converged MIXED or LEARNED solve it is the
+     * convergence test's own FP64 residual of the final iterate, |b - (A D^-1)(D x)|, the same
+     * quantity up to rounding (no further SpMV) */
     /* extensions */
     int32_t outer_iterations;   /* FP64 refinement sweeps (mixed / learned) */
     int32_t fallback;           /* 1 when the solve continued as Jacobi MIXED: LEARNED after a stall or a
