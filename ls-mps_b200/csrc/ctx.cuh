@@ -121,6 +121,7 @@ struct lsmps_ctx {
     lsmps_gpu::DevBuf ld_ident;     // identity map standing in for the particle permutation
     // SELL-32 copies of A for the fast solvers (built on first use after an assembly)
     bool have_sell = false, have_sell_s = false, have_sell_f = false;
+    bool have_sell_raw = false;  // the unscaled FP64 values and 32-bit columns of the SELL copy
     long long sell_nslices = 0, sell_entries = 0;
     lsmps_gpu::DevBuf S_ptr, S_len, S_col, S_val, S_vals, S_valf;
     // 16-bit column steps of the SELL copies (used when every row ascends in steps < 65536)

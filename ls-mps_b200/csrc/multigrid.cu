@@ -147,12 +147,14 @@ __global__ void k_mg_nbr(long long n, const int3* __restrict__ coord, int gx, in
 
 // AP[i][t]: row i's entries summed per neighbor aggregate, in FP32 slice-major (for level 1)
 // and as AP / a_ii in FP16 row-major, MG_APH_STRIDE halves per row (for the V-cycle). One warp
-// per SELL slice of the FP64 matrix, one lane per row, four entries per load (coalesced). Each
-// lane adds its entries, in entry order, into its own column of a shared-memory table of 27
-// slots; the table is then written out with coalesced stores. AP is deterministic.
+// per SELL slice, one lane per row, four entries per load (coalesced), read from the solver's
+// FP32 copy of A D^-1 (a_ij = (a_ij / a_jj) a_jj, the column's diagonal from D^-1; the copy's
+// 16-bit column steps or 32-bit columns), so the set-up needs no unscaled FP64 copy. Each lane
+// adds its entries, in entry order, into its own column of a shared-memory table of 27 slots;
+// the table is then written out with coalesced stores. AP is deterministic.
 constexpr int MG_APH_STRIDE = 28;  // 27 slots + 1 zero pad: 56 B rows, read as seven 8-byte loads
 constexpr int AP_WARPS = 4;
-__global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<double> A, const unsigned* __restrict__ upack,
+__global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<float> A, const unsigned* __restrict__ upack,
                                                               Pack pk, const double* __restrict__ dinv,
                                                               float* __restrict__ ap, __half* __restrict__ aph,
                                                               int* __restrict__ dflag) {
@@ -167,22 +169,39 @@ __global__ void __launch_bounds__(AP_WARPS * 32) k_mg_fine_ap(Sell<double> A, co
     const int3 ci = unpack(live ? upack[i] : 0u, pk);
     const long long base = (long long)A.sptr[sl] + 4 * lane;
     const int chunks = A.slen[sl] >> 2;
+    int cur = A.dcol ? A.rbase[i] : 0;  // the row's first column (16-bit steps)
     for (int c = 0; c < chunks; ++c) {
-        const double2 v01 = __ldcs(reinterpret_cast<const double2*>(A.val + base + 128 * c));
-        const double2 v23 = __ldcs(reinterpret_cast<const double2*>(A.val + base + 128 * c + 2));
-        const int4 cc = __ldcs(reinterpret_cast<const int4*>(A.col + base + 128 * c));
-        const double v[4] = {v01.x, v01.y, v23.x, v23.y};
-        const int col[4] = {cc.x, cc.y, cc.z, cc.w};
+        const float4 v4 = __ldcs(reinterpret_cast<const float4*>(A.val + base + 128 * c));
+        int col[4];
+        if (A.dcol) {
+            const uint2 q = __ldcs(reinterpret_cast<const uint2*>(A.dcol + base + 128 * c));
+            cur += (int)(q.x & 0xffffu);
+            col[0] = cur;
+            cur += (int)(q.x >> 16);
+            col[1] = cur;
+            cur += (int)(q.y & 0xffffu);
+            col[2] = cur;
+            cur += (int)(q.y >> 16);
+            col[3] = cur;
+        } else {
+            const int4 cc = __ldcs(reinterpret_cast<const int4*>(A.col + base + 128 * c));
+            col[0] = cc.x, col[1] = cc.y, col[2] = cc.z, col[3] = cc.w;
+        }
+        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
         unsigned pj[4];
+        double dj[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) pj[k] = live ? upack[col[k]] : 0u;
+        for (int k = 0; k < 4; ++k) {
+            pj[k] = live ? upack[col[k]] : 0u;
+            dj[k] = live ? dinv[col[k]] : 1.0;
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int3 cj = unpack(pj[k], pk);
             // a coupling beyond the adjacent cells has no slot: flag it (clamped slot, no write
             // out of bounds; the setup then fails with LSMPS_ERR_GRID)
             if (abs(cj.x - ci.x) > 1 || abs(cj.y - ci.y) > 1 || abs(cj.z - ci.z) > 1) atomicOr(dflag, DFLAG_STENCIL);
-            acc[w][slot_of(ci, cj)][lane] += (float)v[k];
+            acc[w][slot_of(ci, cj)][lane] += v[k] / (float)dj[k];  // padding: v = 0
         }
     }
     __syncwarp();
@@ -602,9 +621,9 @@ void mg_setup(lsmps_ctx* ctx) {
     k_mg_nbr<<<grid_for(n1, 256), 256, 0, s>>>(n1, coord1, gx, gy, gz, map, nbr1);
     LSMPS_CHECK_LAUNCH();
     float* ap = M.ap.ensure<float>(padded(U) * MG_SLOTS);
-    const Sell<double> A64 = sell_a64_view(ctx);
-    k_mg_fine_ap<<<grid_for(A64.nslices, AP_WARPS), AP_WARPS * 32, 0, s>>>(
-        A64, upack, pk, ctx->A_dinv.get<double>(), ap, M.aph.ensure<__half>(U * MG_APH_STRIDE + 8), dflag);
+    const Sell<float> Af = sell_scaled32_view(ctx);
+    k_mg_fine_ap<<<grid_for(Af.nslices, AP_WARPS), AP_WARPS * 32, 0, s>>>(
+        Af, upack, pk, ctx->A_dinv.get<double>(), ap, M.aph.ensure<__half>(U * MG_APH_STRIDE + 8), dflag);
     LSMPS_CHECK_LAUNCH();
     k_mg_level1<<<grid_for(32 * n1, 256), 256, 0, s>>>(n1, ustart, ap, L1.val.ensure<float>(padded(n1) * MG_SLOTS),
                                                        L1.dinv.ensure<float>(n1));

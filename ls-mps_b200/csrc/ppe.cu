@@ -438,7 +438,7 @@ void ppe_assemble(lsmps_ctx* ctx, const lsmps_ppe_opts* o, lsmps_ppe_stats* out)
     ctx->have_ppe = true;
     ctx->have_solution = false;
     ctx->assembly_gen += 1;
-    ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = false;
+    ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = ctx->have_sell_raw = false;
     ctx->ppe_assembly = ps;
     if (out) *out = ps;
 }
@@ -520,7 +520,7 @@ void ppe_load_csr(lsmps_ctx* ctx, const int64_t* row_ptr, const int32_t* col, co
     ctx->have_ppe = true;
     ctx->have_solution = false;
     ctx->assembly_gen += 1;
-    ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = false;
+    ctx->have_sell = ctx->have_sell_s = ctx->have_sell_f = ctx->have_sell_raw = false;
     ctx->ppe_assembly = ps;
     ctx->timing_pending &= ~16u;  // a loaded system has no pending assembly time
     if (out) *out = ps;

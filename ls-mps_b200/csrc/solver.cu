@@ -854,7 +854,7 @@ __global__ void __launch_bounds__(128) k_sell_build(long long n, long long nslic
                                                     const int* __restrict__ slen, int* __restrict__ col,
                                                     double* __restrict__ val, unsigned short* __restrict__ dcol,
                                                     int* __restrict__ rbase, double* __restrict__ vals,
-                                                    float* __restrict__ valf, int* bad) {
+                                                    float* __restrict__ valf, int* bad, int raw) {
     __shared__ int scol[4][SB_CAP];
     __shared__ double sval[4][SB_CAP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -916,9 +916,11 @@ __global__ void __launch_bounds__(128) k_sell_build(long long n, long long nslic
             sv[j] = vv[j] * dinv[cc[j]];
         }
         const long long e = base + 128LL * (k4 >> 2);
-        *reinterpret_cast<int4*>(col + e) = make_int4(cc[0], cc[1], cc[2], cc[3]);
-        *reinterpret_cast<double2*>(val + e) = make_double2(vv[0], vv[1]);
-        *reinterpret_cast<double2*>(val + e + 2) = make_double2(vv[2], vv[3]);
+        if (raw) {  // unscaled values and 32-bit columns: only the plain FP64 solver reads them
+            *reinterpret_cast<int4*>(col + e) = make_int4(cc[0], cc[1], cc[2], cc[3]);
+            *reinterpret_cast<double2*>(val + e) = make_double2(vv[0], vv[1]);
+            *reinterpret_cast<double2*>(val + e + 2) = make_double2(vv[2], vv[3]);
+        }
         *reinterpret_cast<ushort4*>(dcol + e) = make_ushort4(dd[0], dd[1], dd[2], dd[3]);
         *reinterpret_cast<double2*>(vals + e) = make_double2(sv[0], sv[1]);
         *reinterpret_cast<double2*>(vals + e + 2) = make_double2(sv[2], sv[3]);
@@ -1511,6 +1513,7 @@ static void solve_exact(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_st
 
 
 // ---- SELL-32 copies of the assembled matrix (built on first use after an assembly) ----
+static void sell_raw(lsmps_ctx* ctx);
 // kind 0: A (FP64), 1: A D^-1 (FP64), 2: A D^-1 (FP32)
 static void sell_structure(lsmps_ctx* ctx) {
     if (ctx->have_sell) return;
@@ -1541,7 +1544,7 @@ static void sell_structure(lsmps_ctx* ctx) {
         LSMPS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
         k_sell_build<<<(unsigned)((ns + 3) / 4), 128, 0, s>>>(U, ns, ctx->A_row.get<int>(), ctx->A_col.get<int>(),
                                                               ctx->A_val.get<double>(), ctx->A_dinv.get<double>(), sptr,
-                                                              slen, col, val, dcol, rbase, vals, valf, bad);
+                                                              slen, col, val, dcol, rbase, vals, valf, bad, 0);
         LSMPS_CHECK_LAUNCH();
         int hbad = 1;
         read_back(ctx, {{bad, &hbad, sizeof(int)}}, nullptr);
@@ -1549,6 +1552,25 @@ static void sell_structure(lsmps_ctx* ctx) {
     }
     ctx->have_sell_s = ctx->have_sell_f = true;  // the scaled copies come with the structure
     ctx->have_sell = true;
+    ctx->have_sell_raw = ns == 0;
+    if (!ctx->have_steps) sell_raw(ctx);  // every view then reads the 32-bit columns
+}
+
+// The unscaled FP64 values and 32-bit columns (the plain FP64 solver's matrix, and the columns
+// of every view when the copies have no 16-bit steps): the same build again, writing them too.
+static void sell_raw(lsmps_ctx* ctx) {
+    if (ctx->have_sell_raw) return;
+    const long long U = ctx->U, ns = ctx->sell_nslices;
+    if (ns) {
+        int* bad = ctx->scratch.get<int>() + 46;
+        k_sell_build<<<(unsigned)((ns + 3) / 4), 128, 0, ctx->stream>>>(
+            U, ns, ctx->A_row.get<int>(), ctx->A_col.get<int>(), ctx->A_val.get<double>(), ctx->A_dinv.get<double>(),
+            ctx->S_ptr.get<int>(), ctx->S_len.get<int>(), ctx->S_col.get<int>(), ctx->S_val.get<double>(),
+            ctx->S_dcol.get<unsigned short>(), ctx->S_rbase.get<int>(), ctx->S_vals.get<double>(),
+            ctx->S_valf.get<float>(), bad, 1);
+        LSMPS_CHECK_LAUNCH();
+    }
+    ctx->have_sell_raw = true;
 }
 
 template <class T>
@@ -1563,6 +1585,7 @@ static Sell<T> sell_view(lsmps_ctx* ctx, const T* val) {
 
 static Sell<double> sell_a64(lsmps_ctx* ctx) {
     sell_structure(ctx);
+    sell_raw(ctx);
     return sell_view<double>(ctx, ctx->S_val.get<double>());
 }
 
@@ -1577,6 +1600,8 @@ static Sell<float> sell_scaled32(lsmps_ctx* ctx) {  // A D^-1 in FP32 (built wit
     sell_structure(ctx);
     return sell_view<float>(ctx, ctx->S_valf.get<float>());
 }
+
+Sell<float> sell_scaled32_view(lsmps_ctx* ctx) { return sell_scaled32(ctx); }
 
 // Fast FP64 / Jacobi: BiCGStab on A (or A D^-1) in FP64.
 static void solve_fast64(lsmps_ctx* ctx, const lsmps_solver_opts* o, lsmps_ppe_stats* ps, bool jacobi) {

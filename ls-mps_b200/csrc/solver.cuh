@@ -43,6 +43,8 @@ struct Sell {
 
 // The assembled system's SELL copy with FP64 values of A (built on first use).
 Sell<double> sell_a64_view(lsmps_ctx* ctx);
+// The SELL copy of A D^-1 with FP32 values (built with the structure).
+Sell<float> sell_scaled32_view(lsmps_ctx* ctx);
 
 // The multigrid's level-1 aggregates (contiguous row ranges ustart[I] .. ustart[I+1], and each
 // row's aggregate agg0[i]) and its level-1 right-hand side, for solver kernels that restrict a
