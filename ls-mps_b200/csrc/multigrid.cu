@@ -72,6 +72,7 @@ struct MgState {
     double setup_ms = 0;
     MgLevel L[MG_MAX_LEVELS + 1];
     DevBuf agg0, ustart, ucell, upack, head, hscan, ap, aph, map, flags, pos;
+    DevBuf nsz;  // int: size of level l at [l] (levels >= 2, written on the device)
 };
 
 namespace {
@@ -130,10 +131,14 @@ __global__ void k_mg_aggregates(long long U, const int* __restrict__ ucell, cons
 }
 
 // nbr[I][t]: the row at offset t of row I's block, through the dense map of its grid
-__global__ void k_mg_nbr(long long n, const int3* __restrict__ coord, int gx, int gy, int gz,
+// Set-up kernels of a coarse level run before the host knows its size: they take an upper
+// bound n for the grid and, when nd is set, the level's size from the device (*nd <= n).
+__device__ __forceinline__ long long dev_size(long long n, const int* nd) { return nd ? (long long)*nd : n; }
+
+__global__ void k_mg_nbr(long long n, const int* nd, const int3* __restrict__ coord, int gx, int gy, int gz,
                          const int* __restrict__ map, int* __restrict__ nbr) {
     long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (I >= n) return;
+    if (I >= dev_size(n, nd)) return;
     int3 c = coord[I];
 #pragma unroll
     for (int t = 0; t < MG_SLOTS; ++t) {
@@ -249,9 +254,10 @@ __global__ void k_mg_level1(long long n1, const int* __restrict__ ustart, const 
     if (t == MG_CENTER) dinv1[I] = safe_inv(a);
 }
 
-__global__ void k_mg_mark(long long n, const int3* __restrict__ coord, int gx, int gy, int* __restrict__ flags) {
+__global__ void k_mg_mark(long long n, const int* nd, const int3* __restrict__ coord, int gx, int gy,
+                          int* __restrict__ flags) {
     long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (I >= n) return;
+    if (I >= dev_size(n, nd)) return;
     int3 c = coord[I];
     flags[((long long)(c.z >> 1) * gy + (c.y >> 1)) * gx + (c.x >> 1)] = 1;
 }
@@ -269,10 +275,10 @@ __global__ void k_mg_assign(long long nb, const int* __restrict__ flags, const i
     }
 }
 
-__global__ void k_mg_parent(long long n, const int3* __restrict__ coord, int gx, int gy,
+__global__ void k_mg_parent(long long n, const int* nd, const int3* __restrict__ coord, int gx, int gy,
                             const int* __restrict__ map, int* __restrict__ parent, int* __restrict__ child) {
     long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (I >= n) return;
+    if (I >= dev_size(n, nd)) return;
     int3 c = coord[I];
     int B = map[((long long)(c.z >> 1) * gy + (c.y >> 1)) * gx + (c.x >> 1)];
     parent[I] = B;
@@ -280,9 +286,10 @@ __global__ void k_mg_parent(long long n, const int3* __restrict__ coord, int gx,
 }
 
 // pn[I][t] = parent of row I's neighbor in slot t (or -1)
-__global__ void k_mg_pn(long long n, const int* __restrict__ nbr, const int* __restrict__ parent,
+__global__ void k_mg_pn(long long ncap, const int* nd, const int* __restrict__ nbr, const int* __restrict__ parent,
                         int* __restrict__ pn) {
     long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long n = dev_size(ncap, nd);
     if (q >= padded(n) * MG_SLOTS) return;
     const long long I = ((q >> 5) / MG_SLOTS) * 32 + (q & 31);  // padding rows hold no neighbors
     const int J = I < n ? nbr[q] : -1;
@@ -293,10 +300,10 @@ __global__ void k_mg_pn(long long n, const int* __restrict__ nbr, const int* __r
 // through its slot offset d to the block at offset (o + d) >> 1 (per axis) of B, so slot t'
 // = e collects, per axis, the offsets d in [2e - o, 2e - o + 1] within [-1, 1] of every
 // child (children in octant order, offsets in slot order).
-__global__ void k_mg_coarsen(long long n, const int* __restrict__ child, const float* __restrict__ val,
-                             float* __restrict__ valc, float* __restrict__ dinvc) {
+__global__ void k_mg_coarsen(long long ncap, const int* nd, const int* __restrict__ child,
+                             const float* __restrict__ val, float* __restrict__ valc, float* __restrict__ dinvc) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q >= n * MG_SLOTS) return;
+    if (q >= dev_size(ncap, nd) * MG_SLOTS) return;
     const long long B = q / MG_SLOTS;
     const int tp = (int)(q - B * MG_SLOTS);
     const int ex = tp % 3 - 1, ey = (tp / 3) % 3 - 1, ez = tp / 9 - 1;
@@ -565,7 +572,7 @@ void mg_destroy(lsmps_ctx* ctx) {
         for (DevBuf* d : {&l.coord, &l.val, &l.nbr, &l.dinv, &l.parent, &l.pn, &l.child, &l.r, &l.x, &l.e})
             d->release();
     for (DevBuf* d : {&m->agg0, &m->ustart, &m->ucell, &m->upack, &m->head, &m->hscan, &m->ap, &m->aph, &m->map,
-                      &m->flags, &m->pos})
+                      &m->flags, &m->pos, &m->nsz})
         d->release();
     delete m;
     ctx->mg = nullptr;
@@ -618,7 +625,7 @@ void mg_setup(lsmps_ctx* ctx) {
     k_mg_aggregates<<<grid_for(U, 256), 256, 0, s>>>(U, ucell, head, hscan, gx, gy, agg0, ustart, coord1, map, n1);
     LSMPS_CHECK_LAUNCH();
     int* nbr1 = L1.nbr.ensure<int>(padded(n1) * MG_SLOTS);
-    k_mg_nbr<<<grid_for(n1, 256), 256, 0, s>>>(n1, coord1, gx, gy, gz, map, nbr1);
+    k_mg_nbr<<<grid_for(n1, 256), 256, 0, s>>>(n1, nullptr, coord1, gx, gy, gz, map, nbr1);
     LSMPS_CHECK_LAUNCH();
     float* ap = M.ap.ensure<float>(padded(U) * MG_SLOTS);
     const Sell<float> Af = sell_scaled32_view(ctx);
@@ -628,53 +635,72 @@ void mg_setup(lsmps_ctx* ctx) {
     k_mg_level1<<<grid_for(32 * n1, 256), 256, 0, s>>>(n1, ustart, ap, L1.val.ensure<float>(padded(n1) * MG_SLOTS),
                                                        L1.dinv.ensure<float>(n1));
     LSMPS_CHECK_LAUNCH();
-    // levels 2..: 2x2x2 blocks of the level below, until the coarsest is small enough
+    // levels 2..: 2x2x2 blocks of the level below, until the coarsest is small enough. The
+    // coarse levels are built before the host knows their sizes: arrays and grids take upper
+    // bounds (a level has at most as many rows as the level below and as its block grid has
+    // blocks), and the kernels read the sizes from the device. Once a level's bound is within
+    // 8x of MG_COARSE_MAX the sizes so far are read back (with the device flags) in one
+    // synchronisation, so the loop stops at the first level of at most MG_COARSE_MAX rows.
+    int* nsz = M.nsz.ensure<int>(MG_MAX_LEVELS + 2);
     int lv = 1;
-    while (M.L[lv].n > MG_COARSE_MAX) {
+    long long ub = n1;  // upper bound of level lv's size (its size, for level 1)
+    int hsz[MG_MAX_LEVELS + 2] = {};
+    while (ub > MG_COARSE_MAX) {
         LSMPS_REQUIRE(lv < MG_MAX_LEVELS, LSMPS_ERR_STATE, "multigrid coarsening did not converge");
         MgLevel& F = M.L[lv];
         MgLevel& C = M.L[lv + 1];
+        const int* fn = lv == 1 ? nullptr : nsz + lv;  // F's size on the device (level 1: n1)
         for (int a = 0; a < 3; ++a) C.dims[a] = (F.dims[a] + 1) >> 1;
         const long long nb = (long long)C.dims[0] * C.dims[1] * C.dims[2];
+        const long long cub = std::min(nb, ub);
         int* flags = M.flags.ensure<int>(nb + 1);
         int* pos = M.pos.ensure<int>(nb + 1);
         LSMPS_CUDA(cudaMemsetAsync(flags, 0, (nb + 1) * sizeof(int), s));
-        k_mg_mark<<<grid_for(F.n, 256), 256, 0, s>>>(F.n, F.coord.get<int3>(), C.dims[0], C.dims[1], flags);
+        k_mg_mark<<<grid_for(ub, 256), 256, 0, s>>>(ub, fn, F.coord.get<int3>(), C.dims[0], C.dims[1], flags);
         LSMPS_CHECK_LAUNCH();
         scan_exclusive<int>(flags, pos, nb, s, ctx->scan_tmp, dflag);
-        int hc = 0;
-        read_back(ctx, {{pos + nb, &hc, sizeof(int)}}, nullptr);
-        C.n = hc;
-        int3* cc = C.coord.ensure<int3>(C.n);
+        LSMPS_CUDA(cudaMemcpyAsync(nsz + lv + 1, pos + nb, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        const int* cn = nsz + lv + 1;
+        C.n = cub;  // the bound until the read-back
+        int3* cc = C.coord.ensure<int3>(cub);
         k_mg_assign<<<grid_for(nb, 256), 256, 0, s>>>(nb, flags, pos, C.dims[0], C.dims[1], cc, map);
         LSMPS_CHECK_LAUNCH();
-        int* child = C.child.ensure<int>(8 * C.n);
-        LSMPS_CUDA(cudaMemsetAsync(child, 0xff, 8 * C.n * sizeof(int), s));
-        k_mg_parent<<<grid_for(F.n, 256), 256, 0, s>>>(F.n, F.coord.get<int3>(), C.dims[0], C.dims[1], map,
-                                                       F.parent.ensure<int>(F.n), child);
+        int* child = C.child.ensure<int>(8 * cub);
+        LSMPS_CUDA(cudaMemsetAsync(child, 0xff, 8 * cub * sizeof(int), s));
+        k_mg_parent<<<grid_for(ub, 256), 256, 0, s>>>(ub, fn, F.coord.get<int3>(), C.dims[0], C.dims[1], map,
+                                                     F.parent.ensure<int>(ub), child);
         LSMPS_CHECK_LAUNCH();
-        k_mg_pn<<<grid_for(padded(F.n) * MG_SLOTS, 256), 256, 0, s>>>(F.n, F.nbr.get<int>(), F.parent.get<int>(),
-                                                                       F.pn.ensure<int>(padded(F.n) * MG_SLOTS));
+        k_mg_pn<<<grid_for(padded(ub) * MG_SLOTS, 256), 256, 0, s>>>(ub, fn, F.nbr.get<int>(), F.parent.get<int>(),
+                                                                      F.pn.ensure<int>(padded(ub) * MG_SLOTS));
         LSMPS_CHECK_LAUNCH();
-        k_mg_nbr<<<grid_for(C.n, 256), 256, 0, s>>>(C.n, cc, C.dims[0], C.dims[1], C.dims[2], map,
-                                                    C.nbr.ensure<int>(padded(C.n) * MG_SLOTS));
+        k_mg_nbr<<<grid_for(cub, 256), 256, 0, s>>>(cub, cn, cc, C.dims[0], C.dims[1], C.dims[2], map,
+                                                    C.nbr.ensure<int>(padded(cub) * MG_SLOTS));
         LSMPS_CHECK_LAUNCH();
-        k_mg_coarsen<<<grid_for(MG_SLOTS * C.n, 256), 256, 0, s>>>(C.n, child, F.val.get<float>(),
-                                                                   C.val.ensure<float>(padded(C.n) * MG_SLOTS),
-                                                                   C.dinv.ensure<float>(C.n));
+        k_mg_coarsen<<<grid_for(MG_SLOTS * cub, 256), 256, 0, s>>>(cub, cn, child, F.val.get<float>(),
+                                                                   C.val.ensure<float>(padded(cub) * MG_SLOTS),
+                                                                   C.dinv.ensure<float>(cub));
         LSMPS_CHECK_LAUNCH();
+        ub = cub;
         ++lv;
+        if (ub <= 8 * MG_COARSE_MAX) {
+            read_back(ctx, {{nsz + 2, hsz + 2, (size_t)(lv - 1) * sizeof(int)}}, "multigrid setup");
+            for (int l = 2; l <= lv; ++l) M.L[l].n = hsz[l];
+            ub = M.L[lv].n;
+        }
     }
-    M.levels = lv;
-    for (int l = 1; l <= lv; ++l) {
+    ev_record(ctx, 17);
+    // the loop ends on a size read back (a bound of at most MG_COARSE_MAX is within 8x), which
+    // checked the device flags; a single-level hierarchy checks them here
+    if (lv == 1) check_device_flags(ctx, "multigrid setup");
+    int levels = 1;
+    while (levels < lv && M.L[levels].n > MG_COARSE_MAX) ++levels;
+    M.levels = levels;
+    for (int l = 1; l <= levels; ++l) {
         MgLevel& Ll = M.L[l];
         Ll.r.ensure<float>(Ll.n + 1);
         Ll.x.ensure<float>(Ll.n + 1);
         Ll.e.ensure<float>(Ll.n + 1);
     }
-    ev_record(ctx, 17);
-    LSMPS_CUDA(cudaStreamSynchronize(s));
-    check_device_flags(ctx, "multigrid setup");
     M.setup_ms = ev_elapsed(ctx, 16, 17);
     M.gen = ctx->assembly_gen;
 }
