@@ -8,7 +8,8 @@
 //             Unknowns are numbered in cell-sorted order, so an aggregate is a contiguous
 //             range of rows [ustart[I], ustart[I+1]).
 //   level l+1 one aggregate per 2x2x2 block of level-l aggregates.
-//   coarsest  the first level with at most MG_COARSE_MAX rows.
+//   coarsest  the first level of at most MG_COARSE_SMALL rows, or of at most MG_COARSE_MAX rows
+//             from level MG_COARSE_DEEP on (is_coarsest).
 // Coarse operators are Galerkin products with piecewise-constant prolongation,
 // A_{l+1} = P^T A_l P. An unknown's neighbors lie within re, so every coupling of an
 // aggregate reaches only the 27 aggregates around it. Every coarse operator is therefore a
@@ -47,6 +48,14 @@ namespace lsmps_gpu {
 
 constexpr int MG_MAX_LEVELS = 40;
 constexpr int MG_COARSE_MAX = 640;       // rows of the coarsest level (one block)
+constexpr int MG_COARSE_SMALL = 256;     // ... of a hierarchy of fewer than MG_COARSE_DEEP levels
+constexpr int MG_COARSE_DEEP = 3;
+// The coarsest level's 10 Jacobi sweeps: enough for a level of up to 640 rows at the bottom of
+// a deep hierarchy (at 1M particles, level 4 of 537 rows), not for level 1 or 2 of a small
+// system, which keep the 256-row limit (4,000 particles: 18 iterations against 27 with 640).
+__host__ __device__ constexpr bool is_coarsest(long long n, int level) {
+    return n <= MG_COARSE_SMALL || (n <= MG_COARSE_MAX && level >= MG_COARSE_DEEP);
+}
 constexpr int MG_SWEEPS = 10;            // Jacobi sweeps on the coarsest level
 constexpr float MG_OMEGA = 1.0f;         // smoother damping
 constexpr float MG_ALPHA = 1.5f;         // coarse-correction scaling
@@ -640,12 +649,12 @@ void mg_setup(lsmps_ctx* ctx) {
     // bounds (a level has at most as many rows as the level below and as its block grid has
     // blocks), and the kernels read the sizes from the device. Once a level's bound is within
     // 8x of MG_COARSE_MAX the sizes so far are read back (with the device flags) in one
-    // synchronisation, so the loop stops at the first level of at most MG_COARSE_MAX rows.
+    // synchronisation, so the loop stops at the first level is_coarsest accepts.
     int* nsz = M.nsz.ensure<int>(MG_MAX_LEVELS + 2);
     int lv = 1;
     long long ub = n1;  // upper bound of level lv's size (its size, for level 1)
     int hsz[MG_MAX_LEVELS + 2] = {};
-    while (ub > MG_COARSE_MAX) {
+    while (!is_coarsest(ub, lv)) {
         LSMPS_REQUIRE(lv < MG_MAX_LEVELS, LSMPS_ERR_STATE, "multigrid coarsening did not converge");
         MgLevel& F = M.L[lv];
         MgLevel& C = M.L[lv + 1];
@@ -689,11 +698,11 @@ void mg_setup(lsmps_ctx* ctx) {
         }
     }
     ev_record(ctx, 17);
-    // the loop ends on a size read back (a bound of at most MG_COARSE_MAX is within 8x), which
+    // the loop ends on a size read back (is_coarsest needs at most MG_COARSE_MAX, within 8x), which
     // checked the device flags; a single-level hierarchy checks them here
     if (lv == 1) check_device_flags(ctx, "multigrid setup");
     int levels = 1;
-    while (levels < lv && M.L[levels].n > MG_COARSE_MAX) ++levels;
+    while (levels < lv && !is_coarsest(M.L[levels].n, levels)) ++levels;
     M.levels = levels;
     for (int l = 1; l <= levels; ++l) {
         MgLevel& Ll = M.L[l];

@@ -9,7 +9,8 @@ reference's.
 The hierarchy is built from the unknowns' cells, floor(x / re) per axis, offset by the
 minimum over all particles. That is the neighbor grid of ``src/lsmps.cpp:16-18,26``.
 Level 1 has one aggregate per cell; level l + 1 groups the 2x2x2 blocks of level l
-((c - cmin) >> l). Coarsening stops at the first level with at most ``COARSE_MAX`` rows.
+((c - cmin) >> l). Coarsening stops at the first level that ``is_coarsest`` accepts: at most
+``COARSE_SMALL`` rows, or at most ``COARSE_MAX`` rows from level ``COARSE_DEEP`` on.
 Each coarse operator is the Galerkin product P^T A P with piecewise-constant P. The V-cycle
 (OMEGA, ALPHA, SWEEPS) is documented in ``multigrid.cu``. ``apply`` returns D M z, the
 operator the solvers apply while iterating on y = D x. Its fine-level sweep uses the same
@@ -23,6 +24,14 @@ import numpy as np
 import scipy.sparse as sp
 
 COARSE_MAX = 640
+COARSE_SMALL = 256
+COARSE_DEEP = 3
+
+
+def is_coarsest(n, level):
+    """The multigrid.cu rule: a level of at most COARSE_SMALL rows, or of at most COARSE_MAX
+    rows at level COARSE_DEEP or deeper, is the coarsest."""
+    return n <= COARSE_SMALL or (n <= COARSE_MAX and level >= COARSE_DEEP)
 SWEEPS = 10
 OMEGA = 1.0
 ALPHA = 1.5
@@ -65,7 +74,7 @@ class Hierarchy:
             Acur = sp.csr_matrix(P.T @ Acur @ P)
             self.Al.append(Acur)
             self.sizes.append(nc)
-            if nc <= COARSE_MAX:
+            if is_coarsest(nc, len(self.Al)):
                 break
             coord = coord >> 1
             key = (coord[:, 2] << 42) | (coord[:, 1] << 21) | coord[:, 0]

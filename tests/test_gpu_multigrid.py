@@ -54,7 +54,7 @@ def test_vcycle_matches_restatement(ctx, case):
 
 
 def test_single_level_hierarchy(ctx):
-    """A system with at most 640 cells: level 1 is the coarsest (one block solves it)."""
+    """A system with at most 256 cells: level 1 is the coarsest (one block solves it)."""
     import scipy.sparse as sp
     from _util import jittered_lattice
 

@@ -27,7 +27,7 @@ def system(built):
 
 def test_coarse_operators_are_27_slot_stencils(system):
     A, _, _, H = system
-    assert H.sizes[0] == A.shape[0] and H.sizes[-1] <= mgo.COARSE_MAX
+    assert H.sizes[0] == A.shape[0] and mgo.is_coarsest(H.sizes[-1], H.levels)
     assert all(a > b for a, b in zip(H.sizes, H.sizes[1:]))
     for M in H.Al:
         assert np.diff(M.indptr).max() <= 27
