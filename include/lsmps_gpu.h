@@ -261,8 +261,9 @@ enum {
  * only JACOBI). MULTIGRID: a cell-aggregation multigrid V-cycle in FP32. Level 1 has one
  * aggregate per neighbor-grid cell; each coarser level groups 2x2x2 blocks of the level below.
  * Coarse operators are the Galerkin products, stored as 27-slot stencils. One Jacobi sweep
- * smooths each level; the coarsest level (at most 256 rows, or 640 from level 3 on) gets 10 sweeps. It is rebuilt
- * after each assembly (its setup time is in solve_ms). No reference counterpart: the
+ * smooths each level; the coarsest level (at most 256 rows, or 640 from level 3 on) gets 10
+ * sweeps. It is rebuilt after each assembly (its setup time is in solve_ms). No reference
+ * counterpart: the
  * reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for loaded CSR systems,
  * which have no cells. Opt-in: cell aggregates ignore connection strength, so systems with
  * weakly coupled particles or strong row contrasts can need more iterations than JACOBI. A
