@@ -263,14 +263,14 @@ enum {
  * Coarse operators are the Galerkin products, stored as 27-slot stencils. One Jacobi sweep
  * smooths each level; the coarsest level (at most 256 rows, or 640 from level 3 on) gets 10
  * sweeps. It is rebuilt after each assembly (its setup time is in solve_ms). No reference
- * counterpart: the reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for
- * loaded CSR systems, which have no cells. Opt-in: cell aggregates ignore connection
- * strength, so systems with weakly coupled particles or strong row contrasts can need more
- * iterations than JACOBI. A multigrid run that stalls (stall_window) or breaks down continues
- * as Jacobi MIXED from its iterate (from zero if that is no longer finite) and reports fallback = 1. With LEARNED and
- * no warm start the hierarchy is built on the context's side stream while the network runs
- * on the context stream (the set-up reads level sizes back to the host; the network fills the
- * GPU meanwhile); the result is the same bits. */
+ * counterpart: the reference's BiCGStab (src/lsmps.cpp:67) is unpreconditioned. Not for loaded
+ * CSR systems, which have no cells. Opt-in: cell aggregates ignore connection strength, so
+ * systems with weakly coupled particles or strong row contrasts can need more iterations than
+ * JACOBI. A multigrid run that stalls (stall_window) or breaks down continues as Jacobi MIXED
+ * from its iterate (from zero if that is no longer finite) and reports fallback = 1. With
+ * LEARNED and no warm start the hierarchy is built on the context's side stream while the
+ * network runs on the context stream (the set-up reads level sizes back to the host; the
+ * network fills the GPU meanwhile); the result is the same bits. */
 enum {
     LSMPS_PRECOND_JACOBI = 0,
     LSMPS_PRECOND_MULTIGRID = 1
